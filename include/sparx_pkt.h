@@ -1,0 +1,166 @@
+/*
+ * sparx_pkt.h — C ABI of the B200 PKT k-truss engine (libsparx_pkt.so).
+ *
+ * Drop-in for the PKT path of alexfaisca/sparkx.  The reference computes an
+ * edge's truss number with `AlgoPKT` (src/k_truss/pkt.rs) over a
+ * memory-mapped CSR `GraphMemoryMap` (src/graph/mod.rs:365-378) whose
+ * offsets are u64[n+1] and whose neighbour ids are u64[width]
+ * (graph/mod.rs:482-489).  The result is one truss number per CSR slot, u8,
+ * in slot order (pkt.rs:33,104-114,524-526).  The entry points below take
+ * exactly those arrays and fill that result; every call returns a status
+ * code (0 = SPARX_OK), never aborts, and never falls back to the CPU.
+ *
+ * Input contract (as produced by the reference's cache builders, minus
+ * multi-edges): rows sorted strictly ascending, both directions of every
+ * edge present, ids < n.  Self-loop slots are accepted and get truss 2
+ * (triangles.rs:194-195, impl_csc.rs:148-153).  Parallel edges return
+ * SPARX_E_MULTIGRAPH.
+ */
+#ifndef SPARX_PKT_H
+#define SPARX_PKT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define SPARX_OK              0
+#define SPARX_E_INVALID_CSR   1  /* unsorted row, asymmetric, id >= n, bad offsets */
+#define SPARX_E_MULTIGRAPH    2  /* duplicate slot in a row */
+#define SPARX_E_OVERFLOW_U8   3  /* truss > 255 with 8-bit output (pkt.rs:508-516) */
+#define SPARX_E_OOM           4  /* device memory or HBM budget exhausted */
+#define SPARX_E_TIMEOUT       5  /* device-side peel exceeded its time budget */
+#define SPARX_E_CUDA          6  /* CUDA runtime error (see sparx_last_error) */
+#define SPARX_E_TOO_LARGE     7  /* width >= 2^32 or m >= 2^28 per graph */
+#define SPARX_E_ARG           8  /* bad argument */
+#define SPARX_E_NOT_FOUND     9  /* unknown ticket */
+#define SPARX_E_CANCELLED    10  /* request cancelled before completion */
+
+/* ---- options ---------------------------------------------------------- */
+#define SPARX_SUPPORT_WIDE 0u  /* u32 triangle counters: the defined truss */
+#define SPARX_SUPPORT_U8   1u  /* the reference's AtomicU8 counters (support mod 256) */
+
+#define SPARX_LOOP_GRAPH 0u    /* level loop on the device: CUDA graph WHILE node */
+#define SPARX_LOOP_HOST  1u    /* host re-launches batches of waves (debugging) */
+
+typedef struct sparx_pkt_opts {
+  uint32_t struct_size;    /* sizeof(sparx_pkt_opts) */
+  uint32_t support_mode;   /* SPARX_SUPPORT_WIDE | SPARX_SUPPORT_U8 */
+  uint32_t out_bits;       /* 8 (reference layout) or 32 */
+  int32_t device;          /* CUDA ordinal; -1 = current device */
+  uint32_t loop;           /* SPARX_LOOP_GRAPH | SPARX_LOOP_HOST */
+  uint32_t support_kernel; /* 0 = auto, 1 = balanced binary search, 2 = vertex hash */
+  uint64_t timeout_ms;     /* device budget for the peel; 0 = 600000 */
+} sparx_pkt_opts;
+
+typedef struct sparx_pkt_stats {
+  uint64_t n, width, m, self_loops;
+  uint64_t triangles;      /* sum of support / 3 (wide counters) */
+  uint64_t max_support;    /* before the peel, after the u8 wrap in u8 mode */
+  uint32_t k_max;          /* largest truss number */
+  uint32_t levels;         /* non-empty peel levels */
+  uint32_t waves;          /* device peel waves (sub-levels + level scans) */
+  uint32_t reserved;
+  double ms_upload, ms_orient, ms_support, ms_peel, ms_finalize, ms_download, ms_total;
+} sparx_pkt_stats;
+
+/* Fill `opts` with defaults (wide support, u8 output, device loop). */
+int sparx_pkt_default_opts(sparx_pkt_opts* opts);
+
+/* Human-readable status text. */
+const char* sparx_strerror(int status);
+
+/* Detail of the last failing call on this thread (CUDA error text etc.). */
+const char* sparx_last_error(void);
+
+/*
+ * Full PKT decomposition of one graph from HOST memory in the reference's
+ * layout.  Replaces AlgoPKT::new / new_with_conf (pkt.rs:45-52,85-95), whose
+ * work is compute_with_proc_mem_impl (pkt.rs:216-563).
+ *   offsets    u64[n_plus_1]  (graph/mod.rs:482-485, offsets_ptr)
+ *   neighbours u64[width]     (graph/mod.rs:487-489, neighbours_ptr)
+ *   truss_out  u8[width] (out_bits 8) or u32[width] (out_bits 32), caller-owned
+ */
+int sparx_pkt_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours,
+                  uint64_t width, void* truss_out, const sparx_pkt_opts* opts,
+                  sparx_pkt_stats* stats);
+
+/* Same, with u32 neighbour ids in host memory. */
+int sparx_pkt_run_u32(const uint64_t* offsets, uint64_t n_plus_1, const uint32_t* neighbours,
+                      uint64_t width, void* truss_out, const sparx_pkt_opts* opts,
+                      sparx_pkt_stats* stats);
+
+/*
+ * Same, with every array already in DEVICE memory of opts->device; runs on
+ * `cuda_stream` (a cudaStream_t, or NULL for the library's own stream) and
+ * returns after the stream has finished the result.
+ */
+int sparx_pkt_run_device(const uint64_t* d_offsets, uint64_t n_plus_1,
+                         const uint32_t* d_neighbours, uint64_t width, void* d_truss_out,
+                         const sparx_pkt_opts* opts, sparx_pkt_stats* stats, void* cuda_stream);
+
+/*
+ * Triangle support per CSR slot, host memory in / out.  Replaces
+ * Triangles::new (triangles.rs:27-32), i.e. compute_with_proc_mem_impl
+ * (triangles.rs:144-243).  support_out is u32[width]; in SPARX_SUPPORT_U8 mode
+ * the values are reduced mod 256 like the reference's AtomicU8 counters.
+ */
+int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours,
+                        uint64_t width, uint32_t* support_out, const sparx_pkt_opts* opts,
+                        sparx_pkt_stats* stats);
+
+/* ---- batched decomposition -------------------------------------------- */
+/* One member of a batch: host arrays in the reference's layout (u64 ids) or
+ * u32 ids (neighbour_bits 32).  truss_out follows opts->out_bits. */
+typedef struct sparx_graph_view {
+  const uint64_t* offsets;
+  uint64_t n_plus_1;
+  const void* neighbours;
+  uint64_t width;
+  uint32_t neighbour_bits; /* 64 or 32 */
+  uint32_t reserved;
+  void* truss_out;
+} sparx_graph_view;
+
+/*
+ * Decompose `count` independent graphs.  Graphs are packed into waves under
+ * `hbm_budget_bytes` (0 = 150 GB); each wave is one concatenated CSR whose
+ * peel advances every member with one launch per device wave.  Per-graph
+ * status goes to status_out[count] (may be NULL), per-graph stats to
+ * stats_out[count] (may be NULL); the return value is the first failure.
+ */
+int sparx_pkt_run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
+                        const sparx_pkt_opts* opts, int* status_out, sparx_pkt_stats* stats_out);
+
+/* ---- serving: continuous batching ------------------------------------ */
+typedef struct sparx_server sparx_server;
+
+/* Create a server on opts->device with an HBM budget (0 = 150 GB). */
+int sparx_server_create(sparx_server** out, uint64_t hbm_budget_bytes, const sparx_pkt_opts* opts);
+
+/* Queue a decomposition; the arrays must stay valid until sparx_server_poll
+ * reports it done.  *ticket identifies the request. */
+int sparx_server_submit(sparx_server* s, const sparx_graph_view* graph, uint64_t* ticket);
+
+/* Non-blocking: *done = 1 once finished; *status is that request's status. */
+int sparx_server_poll(sparx_server* s, uint64_t ticket, int* done, int* status,
+                      sparx_pkt_stats* stats);
+
+/* Block until the request finishes (timeout_ms 0 = forever). */
+int sparx_server_wait(sparx_server* s, uint64_t ticket, uint64_t timeout_ms, int* status,
+                      sparx_pkt_stats* stats);
+
+/* Cancel a queued (not yet admitted) request. */
+int sparx_server_cancel(sparx_server* s, uint64_t ticket);
+
+/* Drain and free. */
+int sparx_server_destroy(sparx_server* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARX_PKT_H */

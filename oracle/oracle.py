@@ -1,0 +1,188 @@
+"""ORACLE — test infrastructure only (the checker, never the product path).
+
+Python side of the CPU restatement in ``pkt_oracle.cpp`` plus a brute-force
+truss decomposition straight from the definition.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py`` may
+import this module.
+
+Parity is unpinned by the reference: the Rust reference cannot be built here
+and ships no truss/support golden vectors (see ``pkt_oracle.cpp``).  The
+restatements are pinned by hand-derived known answers and by agreement with
+``brute_force_truss`` (below) on random graphs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+MODE_WIDE = 0
+MODE_U8 = 1
+
+ERRORS = {0: "ok", 1: "invalid CSR", 2: "multigraph", 3: "level overflow (u8)", 4: "queue full"}
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def build(force: bool = False) -> str:
+    path = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "pkt_oracle.cpp")
+    if force or not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+    return path
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+        L.orc_validate.restype = i32
+        L.orc_validate.argtypes = [u64, vp, vp]
+        L.orc_edge_index.restype = i32
+        L.orc_edge_index.argtypes = [u64, vp, vp, vp, vp, i32]
+        L.orc_triangles.restype = i32
+        L.orc_triangles.argtypes = [u64, vp, vp, vp, vp, i32, i32, i32, vp]
+        L.orc_pkt.restype = i32
+        L.orc_pkt.argtypes = [u64, vp, vp, vp, vp, i32, i32, i32, vp, vp]
+        L.orc_burkhardt.restype = i32
+        L.orc_burkhardt.argtypes = [u64, vp, vp, vp, vp, i32, i32, vp]
+        L.orc_verify.restype = u64
+        L.orc_verify.argtypes = [u64, vp, vp, vp, vp, i32]
+        L.orc_fast_truss.restype = i32
+        L.orc_fast_truss.argtypes = [u64, vp, vp, i32, i32, vp, vp, vp]
+        _LIB = L
+    return _LIB
+
+
+def _csr(off, nbr):
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    nbr = np.ascontiguousarray(nbr, dtype=np.uint32)
+    return off, nbr, len(off) - 1
+
+
+def _check(rc):
+    if rc:
+        raise OracleError(ERRORS.get(rc, f"error {rc}"))
+
+
+def edge_index(off, nbr, threads=1):
+    """(eo, er) as in graph/impl_csc.rs:87-263."""
+    off, nbr, n = _csr(off, nbr)
+    eo = np.zeros(n, dtype=np.uint64)
+    er = np.zeros(len(nbr), dtype=np.uint64)
+    _check(lib().orc_edge_index(n, off.ctypes.data, nbr.ctypes.data, eo.ctypes.data,
+                                er.ctypes.data, threads))
+    return eo, er
+
+
+def triangles(off, nbr, mode=MODE_WIDE, threads=1, hash_map=False, eo_er=None):
+    """Per-slot triangle support as in k_truss/triangles.rs:144-243."""
+    off, nbr, n = _csr(off, nbr)
+    eo, er = eo_er if eo_er is not None else edge_index(off, nbr, threads)
+    sup = np.zeros(len(nbr), dtype=np.uint32)
+    _check(lib().orc_triangles(n, off.ctypes.data, nbr.ctypes.data, eo.ctypes.data,
+                               er.ctypes.data, threads, mode, int(hash_map), sup.ctypes.data))
+    return sup
+
+
+def pkt(off, nbr, mode=MODE_WIDE, threads=1, hash_map=False, return_stats=False):
+    """Truss per slot (u32) by the PKT restatement of k_truss/pkt.rs:216-563."""
+    off, nbr, n = _csr(off, nbr)
+    eo, er = edge_index(off, nbr, threads)
+    sup = triangles(off, nbr, mode, threads, hash_map, (eo, er))
+    truss = np.zeros(len(nbr), dtype=np.uint32)
+    st = np.zeros(3, dtype=np.uint64)
+    _check(lib().orc_pkt(n, off.ctypes.data, nbr.ctypes.data, er.ctypes.data, sup.ctypes.data,
+                         threads, mode, int(hash_map), truss.ctypes.data, st.ctypes.data))
+    if return_stats:
+        return truss, {"levels": int(st[0]), "sublevels": int(st[1]), "max_level": int(st[2])}
+    return truss
+
+
+def burkhardt(off, nbr, mode=MODE_WIDE, hash_map=False):
+    """Truss per slot by the restatement of k_truss/burkhardt_et_al.rs:186-380."""
+    off, nbr, n = _csr(off, nbr)
+    eo, er = edge_index(off, nbr)
+    sup = triangles(off, nbr, mode, 1, hash_map, (eo, er))
+    truss = np.zeros(len(nbr), dtype=np.uint32)
+    _check(lib().orc_burkhardt(n, off.ctypes.data, nbr.ctypes.data, er.ctypes.data,
+                               sup.ctypes.data, mode, int(hash_map), truss.ctypes.data))
+    return truss
+
+
+def verify(off, nbr, truss, threads=1):
+    """Corrected k_truss/mod.rs:30-216; returns -1 if the assignment passes,
+    else the first failing slot."""
+    off, nbr, n = _csr(off, nbr)
+    _, er = edge_index(off, nbr, threads)
+    t = np.ascontiguousarray(truss, dtype=np.uint32)
+    r = lib().orc_verify(n, off.ctypes.data, nbr.ctypes.data, er.ctypes.data, t.ctypes.data,
+                         threads)
+    return int(r) - 1
+
+
+def fast_truss(off, nbr, mode=MODE_WIDE, threads=None):
+    """Independent exact peel for large graphs: (truss per slot, triangles, levels)."""
+    off, nbr, n = _csr(off, nbr)
+    threads = threads or os.cpu_count() or 1
+    truss = np.zeros(len(nbr), dtype=np.uint32)
+    tri = ctypes.c_uint64()
+    lev = ctypes.c_uint64()
+    _check(lib().orc_fast_truss(n, off.ctypes.data, nbr.ctypes.data, threads, mode,
+                                truss.ctypes.data, ctypes.byref(tri), ctypes.byref(lev)))
+    return truss, int(tri.value), int(lev.value)
+
+
+def brute_force_truss(off, nbr):
+    """Truss per slot straight from the definition: the k-truss is the largest
+    subgraph in which every edge lies in >= k-2 triangles; an edge's truss is
+    the largest such k.  Pure Python: small graphs only."""
+    off = np.asarray(off, dtype=np.int64)
+    nbr = np.asarray(nbr, dtype=np.int64)
+    n = len(off) - 1
+    adj = [set() for _ in range(n)]
+    edges = set()
+    for u in range(n):
+        for s in range(off[u], off[u + 1]):
+            v = int(nbr[s])
+            if v != u:
+                adj[u].add(v)
+                edges.add((min(u, v), max(u, v)))
+    truss = {e: 2 for e in edges}
+    live = set(edges)
+    k = 3
+    while live:
+        # peel to the k-truss of the current live graph
+        ladj = {}
+        for (u, v) in live:
+            ladj.setdefault(u, set()).add(v)
+            ladj.setdefault(v, set()).add(u)
+        changed = True
+        while changed:
+            changed = False
+            for (u, v) in list(live):
+                if len(ladj[u] & ladj[v]) < k - 2:
+                    live.discard((u, v))
+                    ladj[u].discard(v)
+                    ladj[v].discard(u)
+                    changed = True
+        for e in live:
+            truss[e] = k
+        k += 1
+    out = np.zeros(len(nbr), dtype=np.uint32)
+    for u in range(n):
+        for s in range(off[u], off[u + 1]):
+            v = int(nbr[s])
+            out[s] = 2 if v == u else truss[(min(u, v), max(u, v))]
+    return out

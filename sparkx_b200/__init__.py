@@ -1,0 +1,10 @@
+"""B200-native PKT k-truss decomposition (drop-in for SparX's ``k_truss`` PKT path).
+
+Public surface mirrors the reference's ``AlgoPKT`` (``src/k_truss/pkt.rs:29-123``):
+``AlgoPKT.new(graph)``, ``trussness(e)``, ``k_trusses()``, ``drop_cache()``; the
+graph is a memory-mapped CSR like ``GraphMemoryMap`` (``src/graph/mod.rs:365-378``).
+"""
+from .graph import GraphMemoryMap  # noqa: F401
+from .pkt import AlgoPKT, PktError, PktOptions, PktStats, Triangles  # noqa: F401
+
+__all__ = ["GraphMemoryMap", "AlgoPKT", "Triangles", "PktOptions", "PktStats", "PktError"]

@@ -1,0 +1,997 @@
+// Device kernels of the B200 PKT k-truss engine (sm_100a).
+//
+// One "union" CSR holds every graph of a launch as a disjoint union (vertex
+// ids, slots and edge ids offset per member), so the preparation kernels
+// (narrowing, orientation, support, finalize) see a single graph.  The peel
+// runs a per-member state machine: each member has its own level, phase and
+// frontier, and one device "wave" advances every member by one step (a level
+// scan or one PKT sub-level).  A single graph is a union of one.
+//
+// Layout in HBM (u32 everywhere: width < 2^32, m < 2^28 per member):
+//   off[n+1], nbr[width]        narrowed CSR, rows sorted ascending
+//   eid[width]                  slot -> undirected edge id (0xFFFFFFFF: self-loop)
+//   dplus[n], opos[n+1]         degree-ordered out-degree and its prefix
+//   ocol[m], osrc[m]            oriented edge e = (osrc[e] -> ocol[e]); e is the
+//                               undirected edge id; rank(osrc) < rank(ocol)
+//   sup[m] (i32), tag[m]        support / PKT level, and the wave at which the
+//                               edge is processed (0xFFFFFFFF: not yet queued)
+//   act[2][m], q[2][m] (u64)    per-member active lists and frontier queues,
+//                               segment [eb_g, eb_g + m_g) for member g
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sparx {
+
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+constexpr uint32_t kTagActive = 0xFFFFFFFFu;
+constexpr int kWorkBits = 36;  // packed queue counter: (count << 36) | work
+constexpr unsigned long long kWorkMask = (1ull << kWorkBits) - 1;
+constexpr int kEidBits = 28;   // queue entry: (wstart << 28) | local eid
+constexpr uint32_t kEidMask = (1u << kEidBits) - 1;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// error flags (device bitmask)
+enum : uint32_t {
+  kErrRange = 1u,       // neighbour id >= n
+  kErrUnsorted = 2u,    // row not ascending
+  kErrMulti = 4u,       // duplicate slot
+  kErrAsym = 8u,        // reverse slot missing
+  kErrOverflowU8 = 16u, // truss > 255 with 8-bit output / level 255 in u8 mode
+  kErrCapacity = 32u,   // packed counter or queue capacity exceeded
+  kErrTimeout = 64u,    // device time budget exhausted
+  kErrOffsets = 128u,   // offsets not monotone / wrong total
+  kErrWaves = 256u,     // wave bound exceeded (no progress)
+};
+
+enum : uint32_t { kPhaseScan0 = 0, kPhaseScan = 1, kPhaseProc = 2, kPhaseDone = 3 };
+
+struct Union {  // the prepared concatenated graph
+  const uint32_t* off;
+  const uint32_t* nbr;
+  const uint32_t* eid;
+  const uint32_t* opos;
+  const uint32_t* ocol;
+  const uint32_t* osrc;
+  int32_t* sup;
+  uint32_t* tag;
+  uint32_t* act[2];
+  unsigned long long* q[2];
+  uint32_t n;
+  uint32_t m;
+  uint32_t width;
+  uint32_t G;
+};
+
+// Field-by-field copy of a device-resident Union into registers (a struct
+// copy would land in local memory).
+struct UnionRegs {
+  const uint32_t* __restrict__ off;
+  const uint32_t* __restrict__ nbr;
+  const uint32_t* __restrict__ eid;
+  const uint32_t* __restrict__ ocol;
+  const uint32_t* __restrict__ osrc;
+  int32_t* sup;
+  uint32_t* tag;
+  uint32_t* act0;
+  uint32_t* act1;
+  unsigned long long* q0;
+  unsigned long long* q1;
+  __device__ __forceinline__ explicit UnionRegs(const Union* p)
+      : off(p->off), nbr(p->nbr), eid(p->eid), ocol(p->ocol), osrc(p->osrc), sup(p->sup), tag(p->tag),
+        act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]) {}
+};
+
+struct Member {  // static per-member ranges
+  uint32_t vb, n;   // vertices [vb, vb + n)
+  uint32_t sb, w;   // slots [sb, sb + w)
+  uint32_t eb, m;   // edge ids [eb, eb + m)
+};
+
+struct MemberState {  // dynamic per-member peel state
+  uint32_t phase, level, act_sel, q_sel;
+  uint32_t act_count;
+  uint32_t kept;            // wave accumulator: active edges kept by a scan
+  uint32_t min_kept;        // wave accumulator: min support among kept
+  uint32_t processed;       // edges whose truss is fixed
+  unsigned long long curr;  // packed (count << 36 | work) of the frontier being processed
+  unsigned long long next;  // wave accumulator: frontier being built
+  uint32_t levels, max_level, waves, pad;
+};
+
+struct Control {
+  uint32_t G;
+  uint32_t wave;       // current wave number (>= 1)
+  uint32_t done;
+  uint32_t err;
+  unsigned long long total_work;
+  unsigned long long max_waves;
+  unsigned long long t_start;
+  unsigned long long timeout_ns;
+  unsigned long long waves_run;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t deg_of(const uint32_t* off, uint32_t v) {
+  return __ldg(off + v + 1) - __ldg(off + v);
+}
+
+// degree order, ties by id: the orientation rank
+__device__ __forceinline__ bool rank_less(uint32_t du, uint32_t u, uint32_t dv, uint32_t v) {
+  return du < dv || (du == dv && u < v);
+}
+
+// lower_bound of x in sorted a[lo, hi)
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t lo,
+                                                    uint32_t hi, uint32_t x) {
+  while (lo < hi) {
+    uint32_t mid = lo + ((hi - lo) >> 1);
+    if (__ldg(a + mid) < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// largest i in [lo, hi] with pref[i] <= k (pref non-decreasing, pref[lo] <= k)
+__device__ __forceinline__ uint32_t last_le_u64(const unsigned long long* __restrict__ pref,
+                                                uint32_t lo, uint32_t hi, unsigned long long k) {
+  while (lo < hi) {
+    uint32_t mid = lo + ((hi - lo + 1) >> 1);
+    if (pref[mid] <= k) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// largest i in [lo, hi] with (q[i] >> 28) <= k
+__device__ __forceinline__ uint32_t last_entry_le(const unsigned long long* __restrict__ q,
+                                                  uint32_t lo, uint32_t hi, unsigned long long k) {
+  while (lo < hi) {
+    uint32_t mid = lo + ((hi - lo + 1) >> 1);
+    if ((q[mid] >> kEidBits) <= k) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Segmented inclusive warp scan; segments are runs of equal `key`, which is
+// non-decreasing across lanes.
+__device__ __forceinline__ void seg_scan(uint32_t key, unsigned long long& v, uint32_t& c) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    unsigned long long ov = __shfl_up_sync(kFull, v, d);
+    uint32_t oc = __shfl_up_sync(kFull, c, d);
+    uint32_t ok = __shfl_up_sync(kFull, key, d);
+    if (lane >= (uint32_t)d && ok == key) { v += ov; c += oc; }
+  }
+}
+
+__device__ __forceinline__ void seg_min(uint32_t key, uint32_t& v) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t ov = __shfl_up_sync(kFull, v, d);
+    uint32_t ok = __shfl_up_sync(kFull, key, d);
+    if (lane >= (uint32_t)d && ok == key) v = min(v, ov);
+  }
+}
+
+__device__ __forceinline__ int seg_tail(uint32_t key) {
+  unsigned grp = __match_any_sync(kFull, key);
+  return 31 - __clz(grp);
+}
+
+__device__ __forceinline__ int seg_head(uint32_t key) {
+  unsigned grp = __match_any_sync(kFull, key);
+  return __ffs(grp) - 1;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel A: narrowing (u64 ids -> u32) with range check.  Grid-stride.
+__global__ void k_narrow_ids(const unsigned long long* __restrict__ src, uint32_t* __restrict__ dst,
+                             unsigned long long count, unsigned long long n_limit, uint32_t base,
+                             uint32_t* __restrict__ err) {
+  unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  bool bad = false;
+  for (; i < count; i += stride) {
+    unsigned long long x = src[i];
+    bad |= x >= n_limit;
+    dst[i] = (uint32_t)x + base;
+  }
+  if (bad) atomicOr(err, kErrRange);
+}
+
+// u32 ids: range check, optionally copying with a base shift (dst may be null)
+__global__ void k_range_ids(const uint32_t* __restrict__ ids, uint32_t* __restrict__ dst,
+                            unsigned long long count, uint32_t n_limit, uint32_t base,
+                            uint32_t* __restrict__ err) {
+  unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  bool bad = false;
+  for (; i < count; i += stride) {
+    uint32_t x = __ldg(ids + i);
+    bad |= x >= n_limit;
+    if (dst) dst[i] = x + base;
+  }
+  if (bad) atomicOr(err, kErrRange);
+}
+
+// offsets u64 -> u32 (+ a member's slot base), checking monotonicity inside
+// this chunk; first/last values are checked when first_expect / last_expect
+// are >= 0 (device inputs), else by the host.
+__global__ void k_narrow_offsets(const unsigned long long* __restrict__ src, uint32_t* __restrict__ dst,
+                                 uint32_t count, uint32_t slot_base, long long first_expect,
+                                 long long last_expect, uint32_t* __restrict__ err) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (; i < count; i += stride) {
+    const unsigned long long x = src[i];
+    if (i == 0 && first_expect >= 0) bad |= x != (unsigned long long)first_expect;
+    if (i + 1 == count && last_expect >= 0) bad |= x != (unsigned long long)last_expect;
+    if (i + 1 < count) bad |= src[i + 1] < x;
+    dst[i] = (uint32_t)x + slot_base;
+  }
+  if (bad) atomicOr(err, kErrOffsets);
+}
+
+// shift a member's local vertex ids into union ids
+__global__ void k_shift_ids(uint32_t* __restrict__ ids, unsigned long long count, uint32_t base) {
+  unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (; i < count; i += stride) ids[i] += base;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel B1: per-row validation + oriented out-degree.  Warp per vertex.
+//   rows strictly ascending (equal -> multigraph), counts self-loops, and
+//   dplus[u] = #{v in N(u): v != u, rank(u) < rank(v)}.
+__global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict__ off,
+                                                      const uint32_t* __restrict__ nbr, uint32_t n,
+                                                      uint32_t* __restrict__ dplus,
+                                                      unsigned long long* __restrict__ self_loops,
+                                                      uint32_t* __restrict__ err) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t flags = 0;
+  unsigned long long selfc = 0;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    const uint32_t du = e - b;
+    uint32_t cnt = 0;
+    for (uint32_t s = b + lane; s < e; s += 32) {
+      uint32_t v = __ldg(nbr + s);
+      if (v >= n) { flags |= kErrRange; continue; }
+      if (s + 1 < e) {
+        uint32_t nx = __ldg(nbr + s + 1);
+        if (nx == v) flags |= kErrMulti;
+        else if (nx < v) flags |= kErrUnsorted;
+      }
+      if (v == u) { selfc++; continue; }
+      uint32_t dv = deg_of(off, v);
+      cnt += rank_less(du, u, dv, v);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) cnt += __shfl_down_sync(kFull, cnt, d);
+    if (lane == 0) dplus[u] = cnt;
+  }
+  if (flags) atomicOr(err, flags);
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) selfc += __shfl_down_sync(kFull, selfc, d);
+  if (lane == 0 && selfc) atomicAdd(self_loops, selfc);
+}
+
+// Kernel B2: fill oriented lists (kept in id order) and the slot -> eid map of
+// each vertex's out-slots; self-loop slots get kInvalid.  Warp per vertex.
+__global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict__ off,
+                                                     const uint32_t* __restrict__ nbr, uint32_t n,
+                                                     const uint32_t* __restrict__ opos,
+                                                     uint32_t* __restrict__ ocol,
+                                                     uint32_t* __restrict__ osrc,
+                                                     uint32_t* __restrict__ eid) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    const uint32_t du = e - b;
+    uint32_t base = __ldg(opos + u);
+    for (uint32_t s0 = b; s0 < e; s0 += 32) {
+      const uint32_t s = s0 + lane;
+      bool out = false;
+      uint32_t v = 0;
+      if (s < e) {
+        v = __ldg(nbr + s);
+        if (v == u || v >= n) eid[s] = kInvalid;
+        else out = rank_less(du, u, deg_of(off, v), v);
+      }
+      unsigned bal = __ballot_sync(kFull, out);
+      if (out) {
+        uint32_t p = base + __popc(bal & ((1u << lane) - 1));
+        ocol[p] = v;
+        osrc[p] = u;
+        eid[s] = p;
+      }
+      base += __popc(bal);
+    }
+  }
+}
+
+// Kernel B3: in-slots (rank(v) < rank(u)) take the id of v's out-slot to u,
+// found by binary search in v's oriented list.  Missing -> asymmetric.
+__global__ void __launch_bounds__(256) k_orient_reverse(const uint32_t* __restrict__ off,
+                                                        const uint32_t* __restrict__ nbr, uint32_t n,
+                                                        const uint32_t* __restrict__ opos,
+                                                        const uint32_t* __restrict__ ocol,
+                                                        uint32_t* __restrict__ eid,
+                                                        uint32_t* __restrict__ err) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  bool bad = false;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    const uint32_t du = e - b;
+    for (uint32_t s = b + lane; s < e; s += 32) {
+      uint32_t v = __ldg(nbr + s);
+      if (v == u || v >= n) continue;
+      if (rank_less(du, u, deg_of(off, v), v)) continue;
+      uint32_t lo = __ldg(opos + v), hi = __ldg(opos + v + 1);
+      uint32_t p = lower_bound_u32(ocol, lo, hi, u);
+      if (p < hi && __ldg(ocol + p) == u) eid[s] = p;
+      else { eid[s] = kInvalid; bad = true; }
+    }
+  }
+  if (bad) atomicOr(err, kErrAsym);
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scans (reduce-then-scan, 3 kernels), with the input produced by a
+// functor so work values need not be materialised.
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <class T>
+__device__ __forceinline__ T block_exclusive_scan(T x, T* smem_warp, T& total) {
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  T v = x;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    T o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
+  }
+  if (lane == 31) smem_warp[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    T w = lane < (uint32_t)nw ? smem_warp[lane] : T(0);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      T o = __shfl_up_sync(kFull, w, d);
+      if (lane >= (uint32_t)d) w += o;
+    }
+    if (lane < (uint32_t)nw) smem_warp[lane] = w;
+  }
+  __syncthreads();
+  T warp_off = wid ? smem_warp[wid - 1] : T(0);
+  total = smem_warp[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_off + v - x;
+}
+
+template <class T, class F>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(F f, unsigned long long count, T* tile_sums) {
+  __shared__ T sw[32];
+  const unsigned long long base = (unsigned long long)blockIdx.x * kScanTile;
+  T acc = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    unsigned long long i = base + (unsigned long long)j * kScanThreads + threadIdx.x;
+    if (i < count) acc += f(i);
+  }
+  T total;
+  block_exclusive_scan<T>(acc, sw, total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(T* tile_sums, unsigned long long tiles, T* grand_total) {
+  __shared__ T sw[32];
+  T carry = 0;
+  for (unsigned long long b = 0; b < tiles; b += kScanThreads) {
+    unsigned long long i = b + threadIdx.x;
+    T x = i < tiles ? tile_sums[i] : T(0);
+    T total;
+    T ex = block_exclusive_scan<T>(x, sw, total);
+    if (i < tiles) tile_sums[i] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) *grand_total = carry;
+}
+
+// out[i] = exclusive prefix; out[count] = total
+template <class T, class F>
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(F f, unsigned long long count, const T* tile_offsets,
+                                                             T* out) {
+  __shared__ T sw[32];
+  const unsigned long long base = (unsigned long long)blockIdx.x * kScanTile;
+  // each thread owns kScanItems consecutive items
+  const unsigned long long my = base + (unsigned long long)threadIdx.x * kScanItems;
+  T vals[kScanItems];
+  T acc = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    unsigned long long i = my + j;
+    vals[j] = i < count ? f(i) : T(0);
+    acc += vals[j];
+  }
+  T total;
+  T ex = block_exclusive_scan<T>(acc, sw, total) + tile_offsets[blockIdx.x];
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    unsigned long long i = my + j;
+    if (i < count) out[i] = ex;
+    ex += vals[j];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) out[count] = ex;
+}
+
+struct LoadU32 {
+  const uint32_t* p;
+  __device__ __forceinline__ uint32_t operator()(unsigned long long i) const { return __ldg(p + i); }
+};
+
+// support work of oriented edge e = min(d+(src), d+(dst))
+struct SupportWork {
+  const uint32_t* opos;
+  const uint32_t* osrc;
+  const uint32_t* ocol;
+  __device__ __forceinline__ unsigned long long operator()(unsigned long long e) const {
+    uint32_t a = __ldg(osrc + e), b = __ldg(ocol + e);
+    uint32_t da = __ldg(opos + a + 1) - __ldg(opos + a);
+    uint32_t db = __ldg(opos + b + 1) - __ldg(opos + b);
+    return min(da, db);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Kernel C (balanced form): per oriented edge e = (a -> b), each element of the
+// shorter of N+(a), N+(b) is searched in the longer; a hit c closes the
+// triangle (a, b, c), credited on e, (a -> c) and (b -> c).  Work elements are
+// spread evenly over warps through the exclusive prefix `spref`; a warp owns a
+// contiguous chunk and walks it 32 elements at a time.
+struct PrefStart {
+  const unsigned long long* p;
+  __device__ __forceinline__ unsigned long long operator()(uint32_t x) const { return p[x]; }
+};
+
+template <class StartF>
+__device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i, uint32_t count,
+                                                unsigned long long j, bool valid);
+
+__global__ void __launch_bounds__(256) k_support_balanced(
+    const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
+    const uint32_t* __restrict__ osrc, const unsigned long long* __restrict__ spref, uint32_t m,
+    int32_t* __restrict__ sup, unsigned long long* __restrict__ tri_total) {
+  const uint32_t lane = lane_id();
+  const unsigned long long total = spref[m];
+  const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  unsigned long long ch = total / (nwarps * 4);
+  ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
+  const PrefStart ps{spref};
+  unsigned long long found_total = 0;
+  for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
+    const unsigned long long kend = min(c0 + ch, total);
+    uint32_t i = last_le_u64(spref, 0, m - 1, c0);
+    for (unsigned long long kb = c0; kb < kend; kb += 32) {
+      const unsigned long long k = kb + lane;
+      const bool valid = k < kend;
+      const uint32_t e = window_find(ps, i, m, k, valid);
+      const uint32_t last = (uint32_t)min(31ull, kend - 1 - kb);
+      const uint32_t e_last = __shfl_sync(kFull, e, last);
+      bool hit = false;
+      if (valid) {
+        const uint32_t o = (uint32_t)(k - spref[e]);
+        const uint32_t a = __ldg(osrc + e), b = __ldg(ocol + e);
+        const uint32_t ab = __ldg(opos + a), ae = __ldg(opos + a + 1);
+        const uint32_t bb = __ldg(opos + b), be = __ldg(opos + b + 1);
+        uint32_t ia, ib;
+        if (ae - ab <= be - bb) {
+          ia = ab + o;
+          const uint32_t c = __ldg(ocol + ia);
+          ib = lower_bound_u32(ocol, bb, be, c);
+          hit = ib < be && __ldg(ocol + ib) == c;
+        } else {
+          ib = bb + o;
+          const uint32_t c = __ldg(ocol + ib);
+          ia = lower_bound_u32(ocol, ab, ae, c);
+          hit = ia < ae && __ldg(ocol + ia) == c;
+        }
+        if (hit) {
+          atomicAdd(sup + ia, 1);
+          atomicAdd(sup + ib, 1);
+          found_total++;
+        }
+      }
+      // credit e once per run of lanes sharing it
+      const unsigned hits = __ballot_sync(kFull, hit);
+      const unsigned grp = __match_any_sync(kFull, valid ? e : kInvalid);
+      if (valid && lane == (uint32_t)(__ffs(grp) - 1)) {
+        const int c = __popc(grp & hits);
+        if (c) atomicAdd(sup + e, c);
+      }
+      i = e_last;
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) found_total += __shfl_down_sync(kFull, found_total, d);
+  if (lane == 0 && found_total) atomicAdd(tri_total, found_total);
+}
+
+// ---------------------------------------------------------------------------
+// Peel setup: u8 wrap (u8 mode), per-member triangle sums and max support,
+// tags cleared, identity active lists (local ids inside each member's segment).
+// Per-lane running sums are flushed when the member changes, then reduced per
+// warp, so a single member costs one atomic per warp.
+__device__ __forceinline__ void flush_member_stats(uint32_t g, unsigned long long sum, uint32_t mx,
+                                                   unsigned long long* mem_tri, uint32_t* mem_maxsup) {
+  if (g == kInvalid) return;
+  if (sum) atomicAdd(mem_tri + g, sum);
+  if (mx) atomicMax(mem_maxsup + g, mx);
+}
+
+__global__ void __launch_bounds__(256) k_peel_setup(const Union* __restrict__ Up, const Member* __restrict__ mem,
+                                                    int u8mode, unsigned long long* __restrict__ mem_tri,
+                                                    uint32_t* __restrict__ mem_maxsup) {
+  const Union U = *Up;
+  const uint32_t G = U.G;
+  uint32_t cur = kInvalid;
+  unsigned long long sum = 0;
+  uint32_t mx = 0;
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < U.m; e += gridDim.x * blockDim.x) {
+    uint32_t g = 0;
+    if (G > 1) {
+      uint32_t lo = 0, hi = G - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (mem[mid].eb <= e) lo = mid; else hi = mid - 1;
+      }
+      g = lo;
+    }
+    if (g != cur) {
+      flush_member_stats(cur, sum, mx, mem_tri, mem_maxsup);
+      cur = g; sum = 0; mx = 0;
+    }
+    int32_t s = U.sup[e];
+    sum += (unsigned long long)s;
+    if (u8mode) s &= 0xFF;
+    U.sup[e] = s;
+    mx = max(mx, (uint32_t)s);
+    U.tag[e] = kTagActive;
+    U.act[0][e] = e - mem[g].eb;
+  }
+  // warp reduction when every lane ends on the same member
+  const unsigned same = __match_any_sync(kFull, cur);
+  if (same == kFull) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      sum += __shfl_down_sync(kFull, sum, d);
+      mx = max(mx, __shfl_down_sync(kFull, mx, d));
+    }
+    if (lane_id() == 0) flush_member_stats(cur, sum, mx, mem_tri, mem_maxsup);
+  } else {
+    flush_member_stats(cur, sum, mx, mem_tri, mem_maxsup);
+  }
+}
+
+// first wave: every member scans all its edges at level 0
+__global__ void k_peel_init(const Member* __restrict__ mem, MemberState* __restrict__ st, Control* ctl,
+                            unsigned long long* __restrict__ wpref, uint32_t G) {
+  // single block: prefix of m_g
+  __shared__ unsigned long long sw[32];
+  unsigned long long carry = 0;
+  for (uint32_t b = 0; b < G; b += blockDim.x) {
+    const uint32_t g = b + threadIdx.x;
+    unsigned long long w = 0;
+    if (g < G) {
+      MemberState s{};
+      s.phase = mem[g].m ? kPhaseScan0 : kPhaseDone;
+      s.act_count = mem[g].m;
+      s.min_kept = 0xFFFFFFFFu;
+      st[g] = s;
+      w = s.phase == kPhaseDone ? 0 : mem[g].m;
+    }
+    unsigned long long total;
+    unsigned long long ex = block_exclusive_scan<unsigned long long>(w, sw, total);
+    if (g < G) wpref[g] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) {
+    wpref[G] = carry;
+    ctl->total_work = carry;
+    ctl->wave = 1;
+    ctl->done = carry == 0;
+    ctl->waves_run = 0;
+    ctl->t_start = globaltimer();
+  }
+}
+
+struct WaveArgs {
+  const Union* Up;
+  const Member* mem;
+  MemberState* st;
+  Control* ctl;
+  const unsigned long long* wpref;
+  uint32_t* err;
+};
+
+// work of pushing edge x (union eid): the shorter full row of its endpoints
+__device__ __forceinline__ uint32_t edge_work(const UnionRegs& U, uint32_t x) {
+  const uint32_t u = __ldg(U.osrc + x), v = __ldg(U.ocol + x);
+  return min(deg_of(U.off, u), deg_of(U.off, v));
+}
+
+// PKT sub-level rule for one triangle (e, f, h) of frontier edge e at level l,
+// wave W (pkt.rs:409-479 restated on undirected edge ids):
+//   f or h processed (tag < W)         -> nothing
+//   both above l                        -> charge both
+//   only f above l                      -> charge f unless h is in this frontier
+//                                          with a smaller id than e
+//   only h above l                      -> symmetric
+// A charge that lands on l + 1 queues the edge for the next sub-level; a
+// charge that goes below l is restored to l.
+__device__ __forceinline__ void pkt_rule(const UnionRegs& U, uint32_t e, uint32_t f, uint32_t h, uint32_t l,
+                                         uint32_t W, bool& pf, bool& ph) {
+  pf = ph = false;
+  const uint32_t tf = U.tag[f], th = U.tag[h];
+  if (tf < W || th < W) return;
+  const int32_t sf = U.sup[f], sh = U.sup[h];
+  const int32_t L = (int32_t)l;
+  bool df = false, dh = false;
+  if (sf > L && sh > L) { df = true; dh = true; }
+  else if (sf > L) df = (e < h) || (th != W);
+  else if (sh > L) dh = (e < f) || (tf != W);
+  if (df) {
+    int32_t prev = atomicSub(U.sup + f, 1);
+    if (prev == L + 1) pf = true;
+    else if (prev <= L) atomicMax(U.sup + f, L);
+  }
+  if (dh) {
+    int32_t prev = atomicSub(U.sup + h, 1);
+    if (prev == L + 1) ph = true;
+    else if (prev <= L) atomicMax(U.sup + h, L);
+  }
+}
+
+// Entry lookup for a warp iteration over consecutive work indices.  `start(x)`
+// is the (non-decreasing) first work index of entry x; entry `i` owns the
+// iteration's first element.  Each lane finds the largest x with
+// start(x) <= j among entries i .. i+31 with a 5-step shuffle search; a lane
+// whose entry lies beyond the window (only possible when entries own no work)
+// falls back to a binary search in memory.
+template <class StartF>
+__device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i, uint32_t count,
+                                                unsigned long long j, bool valid) {
+  const uint32_t lane = lane_id();
+  const unsigned long long st = (i + lane < count) ? start(i + lane) : ~0ull;
+  uint32_t t = 0;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    const unsigned long long cand = __shfl_sync(kFull, st, t + d);
+    if (cand <= j) t += d;
+  }
+  uint32_t x = i + t;
+  if (valid && t == 31 && x + 1 < count && start(x + 1) <= j) {
+    uint32_t lo = x + 1, hi = count - 1;
+    while (lo < hi) {
+      uint32_t mid = lo + ((hi - lo + 1) >> 1);
+      if (start(mid) <= j) lo = mid; else hi = mid - 1;
+    }
+    x = lo;
+  }
+  return x;
+}
+
+struct QueueStart {
+  const unsigned long long* q;
+  __device__ __forceinline__ unsigned long long operator()(uint32_t x) const { return q[x] >> kEidBits; }
+};
+
+// Inclusive warp scan of (v, c); returns the warp totals from lane 31.
+__device__ __forceinline__ void warp_scan2(unsigned long long& v, uint32_t& c) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long ov = __shfl_up_sync(kFull, v, d);
+    const uint32_t oc = __shfl_up_sync(kFull, c, d);
+    if (lane >= (uint32_t)d) { v += ov; c += oc; }
+  }
+}
+
+// Warp-aggregated push of edge x (union eid) into member M's next queue with
+// tag W + 1.  All lanes call it; lanes belong to one member.
+__device__ __forceinline__ void push_next(const UnionRegs& U, const Member& M, MemberState* st, uint32_t* err,
+                                          bool want, uint32_t x, uint32_t qsel_next, uint32_t W) {
+  if (!__any_sync(kFull, want)) return;
+  unsigned long long w = 0;
+  if (want) {
+    w = edge_work(U, x);
+    U.tag[x] = W + 1;
+  }
+  unsigned long long v = w;
+  uint32_t c = want ? 1u : 0u;
+  warp_scan2(v, c);
+  unsigned long long old = 0;
+  if (lane_id() == 31) {
+    old = atomicAdd(&st->next, ((unsigned long long)c << kWorkBits) | v);
+    if ((old & kWorkMask) + v > kWorkMask) atomicOr(err, kErrCapacity);
+  }
+  old = __shfl_sync(kFull, old, 31);
+  if (want) {
+    const unsigned long long pos = (old >> kWorkBits) + c - 1;
+    const unsigned long long ws = (old & kWorkMask) + v - w;
+    if (pos < M.m) (qsel_next ? U.q1 : U.q0)[M.eb + pos] = (ws << kEidBits) | (unsigned long long)(x - M.eb);
+    else atomicOr(err, kErrCapacity);
+  }
+}
+
+// Kernel D: one peel wave.  The wave's work (all members' scan elements and
+// frontier elements, laid out by `wpref`) is cut into warp-sized chunks; a
+// warp walks its chunk member by member, 32 consecutive elements per
+// iteration, so every iteration belongs to one member.
+//   scan element j      active-list entry j: processed -> dropped; support
+//                       <= level -> queued for this level; else kept
+//   frontier element j  element o of the shorter row of frontier edge e,
+//                       searched in the longer row; a hit is a triangle
+__global__ void __launch_bounds__(256) k_wave(WaveArgs a) {
+  const Control* ctl = a.ctl;
+  if (ctl->done) return;
+  const unsigned long long total = ctl->total_work;
+  const uint32_t W = ctl->wave;
+  const uint32_t G = ctl->G;
+  const uint32_t lane = lane_id();
+  const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  const UnionRegs U(a.Up);
+  unsigned long long ch = total / (nwarps * 4);
+  ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
+
+  for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
+    const unsigned long long kend = min(c0 + ch, total);
+    unsigned long long k = c0;
+    uint32_t g = G > 1 ? last_le_u64(a.wpref, 0, G - 1, k) : 0;
+    while (k < kend) {
+      while (g + 1 < G && a.wpref[g + 1] <= k) ++g;
+      const unsigned long long mbeg = a.wpref[g];
+      const unsigned long long seg_end = min(kend, a.wpref[g + 1]);
+      const Member M = a.mem[g];
+      MemberState* st = a.st + g;
+      const uint32_t phase = st->phase, level = st->level, act_sel = st->act_sel, q_sel = st->q_sel;
+      const uint32_t qn = q_sel ^ 1u;
+      if (phase == kPhaseProc) {
+        const unsigned long long* q = (q_sel ? U.q1 : U.q0) + M.eb;
+        const uint32_t qcount = (uint32_t)(st->curr >> kWorkBits);
+        const QueueStart qs{q};
+        uint32_t i = last_entry_le(q, 0, qcount - 1, k - mbeg);
+        for (unsigned long long kb = k; kb < seg_end; kb += 32) {
+          const unsigned long long kk = kb + lane;
+          const bool valid = kk < seg_end;
+          const unsigned long long j = kk - mbeg;
+          const uint32_t x = window_find(qs, i, qcount, j, valid);
+          const uint32_t last = (uint32_t)min(31ull, seg_end - 1 - kb);
+          const uint32_t x_last = __shfl_sync(kFull, x, last);
+          bool pf = false, ph = false;
+          uint32_t f = 0, h = 0;
+          if (valid) {
+            const unsigned long long ent = q[x];
+            const uint32_t e = M.eb + (uint32_t)(ent & kEidMask);
+            const uint32_t o = (uint32_t)(j - (ent >> kEidBits));
+            const uint32_t u = __ldg(U.osrc + e), v = __ldg(U.ocol + e);
+            const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
+            const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
+            uint32_t sb, lb, le;
+            if (ue - ub <= ve - vb) { sb = ub; lb = vb; le = ve; }
+            else { sb = vb; lb = ub; le = ue; }
+            const uint32_t slot = sb + o;
+            const uint32_t w = __ldg(U.nbr + slot);
+            if (w != u && w != v) {
+              const uint32_t p = lower_bound_u32(U.nbr, lb, le, w);
+              if (p < le && __ldg(U.nbr + p) == w) {
+                f = __ldg(U.eid + slot);
+                h = __ldg(U.eid + p);
+                pkt_rule(U, e, f, h, level, W, pf, ph);
+              }
+            }
+          }
+          push_next(U, M, st, a.err, pf, f, qn, W);
+          push_next(U, M, st, a.err, ph, h, qn, W);
+          i = x_last;
+        }
+      } else if (phase == kPhaseScan0 || phase == kPhaseScan) {
+        const uint32_t* act = act_sel ? U.act1 : U.act0;
+        uint32_t* act_out = act_sel ? U.act0 : U.act1;
+        for (unsigned long long kb = k; kb < seg_end; kb += 32) {
+          const unsigned long long kk = kb + lane;
+          const bool valid = kk < seg_end;
+          bool keep = false, zero = false, queue = false;
+          uint32_t le = 0, e = 0, ks = 0xFFFFFFFFu;
+          if (valid) {
+            le = act[M.eb + (kk - mbeg)];
+            e = M.eb + le;
+            const int32_t s = U.sup[e];
+            if (phase == kPhaseScan0) {
+              if (s == 0) { U.tag[e] = 0; zero = true; }
+              else { keep = true; ks = (uint32_t)s; }
+            } else if (U.tag[e] == kTagActive) {  // processed edges leave the active list
+              if (s <= (int32_t)level) queue = true;
+              else { keep = true; ks = (uint32_t)s; }
+            }
+          }
+          push_next(U, M, st, a.err, queue, e, qn, W);
+          if (__any_sync(kFull, keep)) {
+            unsigned long long v = 0;
+            uint32_t c = keep ? 1u : 0u;
+            warp_scan2(v, c);
+            uint32_t mn = ks;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
+            uint32_t old = 0;
+            if (lane == 31) {
+              old = atomicAdd(&st->kept, c);
+              atomicMin(&st->min_kept, mn);
+            }
+            old = __shfl_sync(kFull, old, 31);
+            if (keep) act_out[M.eb + old + c - 1] = le;
+          }
+          const unsigned zb = __ballot_sync(kFull, zero);
+          if (zb && lane == 0) atomicAdd(&st->processed, (uint32_t)__popc(zb));
+        }
+      }
+      k = seg_end;
+    }
+  }
+}
+
+// Planner: one block advances every member's state machine after a wave and
+// lays out the next wave's work.  Sets the CUDA-graph loop condition.
+__global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, MemberState* __restrict__ st,
+                                               Control* ctl, unsigned long long* __restrict__ wpref,
+                                               uint32_t* __restrict__ err, cudaGraphConditionalHandle handle,
+                                               int use_handle) {
+  __shared__ unsigned long long sw[32];
+  __shared__ uint32_t s_live;
+  const uint32_t G = ctl->G;
+  if (threadIdx.x == 0) s_live = 0;
+  __syncthreads();
+  const bool was_done = ctl->done;
+  unsigned long long carry = 0;
+  for (uint32_t b = 0; b < G; b += blockDim.x) {
+    const uint32_t g = b + threadIdx.x;
+    unsigned long long w = 0;
+    if (g < G && !was_done) {
+      MemberState s = st[g];
+      const uint32_t m = mem[g].m;
+      switch (s.phase) {
+        case kPhaseScan0:
+          s.act_sel ^= 1u;
+          s.act_count = s.kept;
+          s.kept = 0;
+          if (s.processed >= m) s.phase = kPhaseDone;
+          else { s.level = s.min_kept; s.min_kept = 0xFFFFFFFFu; s.phase = kPhaseScan; }
+          break;
+        case kPhaseScan: {
+          s.act_sel ^= 1u;
+          s.act_count = s.kept;
+          s.kept = 0;
+          const unsigned long long cnt = s.next >> kWorkBits;
+          if (cnt) {
+            s.curr = s.next;
+            s.next = 0;
+            s.q_sel ^= 1u;
+            s.phase = kPhaseProc;
+            s.levels++;
+            s.max_level = s.level;
+          } else if (s.act_count == 0) {
+            s.phase = kPhaseDone;
+          } else {
+            s.level = s.min_kept;  // no edge at this level: jump to the next occupied one
+          }
+          s.min_kept = 0xFFFFFFFFu;
+          break;
+        }
+        case kPhaseProc: {
+          s.processed += (uint32_t)(s.curr >> kWorkBits);
+          const unsigned long long cnt = s.next >> kWorkBits;
+          if (cnt) {
+            s.curr = s.next;
+            s.next = 0;
+            s.q_sel ^= 1u;
+          } else {
+            s.curr = 0;
+            if (s.processed >= m) s.phase = kPhaseDone;
+            else { s.level += 1; s.phase = kPhaseScan; s.min_kept = 0xFFFFFFFFu; }
+          }
+          break;
+        }
+        default:
+          break;
+      }
+      if (s.phase != kPhaseDone) s.waves++;
+      st[g] = s;
+      if (s.phase == kPhaseScan0 || s.phase == kPhaseScan) w = s.act_count;
+      else if (s.phase == kPhaseProc) w = s.curr & kWorkMask;
+      if (s.phase != kPhaseDone) atomicAdd(&s_live, 1u);
+    }
+    unsigned long long total;
+    unsigned long long ex = block_exclusive_scan<unsigned long long>(w, sw, total);
+    if (g < G) wpref[g] = carry + ex;
+    carry += total;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    wpref[G] = carry;
+    uint32_t done = was_done;
+    if (!was_done) {
+      ctl->total_work = carry;
+      ctl->wave += 1;
+      ctl->waves_run += 1;
+      const uint32_t e = *err;
+      if (s_live == 0 || e) done = 1;
+      if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; }
+      if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; }
+      ctl->done = done;
+    }
+    if (use_handle) cudaGraphSetConditional(handle, done ? 0u : 1u);
+  }
+}
+
+// Kernel E: truss per slot = level + 2 (pkt.rs:524-526); self-loop slots 2.
+template <typename OutT>
+__global__ void k_finalize(const uint32_t* __restrict__ eid, const int32_t* __restrict__ sup,
+                           unsigned long long width, OutT* __restrict__ out, int u8mode, int out8,
+                           uint32_t* __restrict__ kmax, uint32_t* __restrict__ err) {
+  unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  uint32_t mx = 0;
+  bool ovf = false;
+  for (; i < width; i += stride) {
+    const uint32_t e = __ldg(eid + i);
+    uint32_t t = 2;
+    if (e != kInvalid) {
+      const uint32_t s = (uint32_t)__ldg(sup + e);
+      t = s + 2;
+      if (u8mode) { ovf |= s >= 255; t &= 0xFFu; }
+      else if (out8) ovf |= t > 255;
+    }
+    mx = max(mx, t);
+    out[i] = (OutT)t;
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) mx = max(mx, __shfl_down_sync(__activemask(), mx, d));
+  if ((threadIdx.x & 31) == 0) atomicMax(kmax, mx);
+  if (ovf) atomicOr(err, kErrOverflowU8);
+}
+
+// support per slot (Triangles::new layout): sup of the slot's edge, 0 for self-loops
+__global__ void k_support_slots(const uint32_t* __restrict__ eid, const int32_t* __restrict__ sup,
+                                unsigned long long width, uint32_t* __restrict__ out, int u8mode) {
+  unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (; i < width; i += stride) {
+    const uint32_t e = __ldg(eid + i);
+    uint32_t s = e == kInvalid ? 0u : (uint32_t)__ldg(sup + e);
+    out[i] = u8mode ? (s & 0xFFu) : s;
+  }
+}
+
+}  // namespace sparx

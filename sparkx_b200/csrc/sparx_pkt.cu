@@ -1,0 +1,740 @@
+// Host side of the B200 PKT k-truss engine: C ABI (include/sparx_pkt.h),
+// device workspace, pinned-staging upload, kernel sequencing and the
+// device-resident peel loop (a CUDA graph with a conditional WHILE node whose
+// body is one wave + the planner).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <omp.h>
+
+#include "../../include/sparx_pkt.h"
+#include "pkt_kernels.cuh"
+
+using namespace sparx;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& s) { g_last_error = s; }
+
+#define CU(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+      return e_ == cudaErrorMemoryAllocation ? SPARX_E_OOM : SPARX_E_CUDA;            \
+    }                                                                                 \
+  } while (0)
+
+inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+constexpr size_t kStageBytes = 64ull << 20;  // per staging buffer (pinned and device)
+constexpr unsigned long long kDefaultTimeoutMs = 600000ull;
+
+int status_from_flags(uint32_t f) {
+  if (!f) return SPARX_OK;
+  if (f & kErrMulti) return SPARX_E_MULTIGRAPH;
+  if (f & (kErrRange | kErrUnsorted | kErrAsym | kErrOffsets)) return SPARX_E_INVALID_CSR;
+  if (f & kErrCapacity) return SPARX_E_TOO_LARGE;
+  if (f & (kErrTimeout | kErrWaves)) return SPARX_E_TIMEOUT;
+  if (f & kErrOverflowU8) return SPARX_E_OVERFLOW_U8;
+  return SPARX_E_CUDA;
+}
+
+struct Counters {  // device scalars
+  uint32_t err;
+  uint32_t kmax;
+  unsigned long long self_loops;
+  unsigned long long tri;
+  unsigned long long grand;
+};
+
+struct Layout {
+  size_t off, nbr, eid, dplus, opos, ocol, osrc, sup, tag, act0, act1, q0, q1, out, stage0, stage1;
+  size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
+  size_t total;
+};
+
+Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_bytes) {
+  Layout L{};
+  size_t p = 0;
+  auto take = [&](size_t bytes) {
+    size_t r = p;
+    p = align_up(p + std::max<size_t>(bytes, 1));
+    return r;
+  };
+  const uint64_t M = std::max<uint64_t>(W / 2, 1);
+  L.off = take(4 * (N + 1));
+  L.nbr = own_nbr ? take(4 * W) : 0;
+  L.eid = take(4 * W);
+  L.dplus = take(4 * N);
+  L.opos = take(4 * (N + 1));
+  L.ocol = take(4 * M);
+  L.osrc = take(4 * M);
+  L.sup = take(4 * M);
+  L.tag = take(4 * M);
+  L.act0 = take(4 * M);
+  L.act1 = take(4 * M);
+  L.q0 = take(16 * M + 16);  // q0 and q1 back to back; also the support prefix (M + 1 u64)
+  L.q1 = L.q0 + 8 * M;
+  L.out = take(out_bytes);
+  L.stage0 = take(kStageBytes);
+  L.stage1 = take(kStageBytes);
+  const uint64_t tiles = (std::max<uint64_t>(N + 1, M + 1) + kScanTile - 1) / kScanTile + 2;
+  L.tiles = take(8 * tiles);
+  L.ctl = take(sizeof(Control));
+  L.mem = take(sizeof(Member) * G);
+  L.st = take(sizeof(MemberState) * G);
+  L.wpref = take(8ull * (G + 1));
+  L.cnt = take(sizeof(Counters));
+  L.mem_tri = take(8ull * G);
+  L.mem_maxsup = take(4ull * G);
+  L.uni = take(sizeof(Union));
+  L.total = p;
+  return L;
+}
+
+struct PeelGraph {
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  std::vector<size_t> key;
+};
+
+struct Engine {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  cudaStream_t capture = nullptr;
+  char* ws = nullptr;
+  size_t ws_cap = 0;
+  void* pinned[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+  cudaEvent_t tev[8] = {};
+  void* pinned_small = nullptr;  // 4 KB for scalar read-backs
+  PeelGraph peel;
+  int wave_blocks = 0;
+  std::mutex mu;
+};
+
+std::mutex g_engines_mu;
+std::map<int, Engine*> g_engines;
+
+int engine_init(Engine& E, int device) {
+  E.device = device;
+  CU(cudaSetDevice(device));
+  CU(cudaDeviceGetAttribute(&E.sm_count, cudaDevAttrMultiProcessorCount, device));
+  CU(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
+  CU(cudaStreamCreateWithFlags(&E.capture, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; ++i) {
+    CU(cudaHostAlloc(&E.pinned[i], kStageBytes, cudaHostAllocDefault));
+    CU(cudaEventCreateWithFlags(&E.pin_ev[i], cudaEventDisableTiming));
+    CU(cudaEventRecord(E.pin_ev[i], E.stream));
+  }
+  for (auto& e : E.tev) CU(cudaEventCreate(&e));
+  CU(cudaHostAlloc(&E.pinned_small, 4096, cudaHostAllocDefault));
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave, 256, 0));
+  E.wave_blocks = std::max(1, per_sm) * E.sm_count;
+  return SPARX_OK;
+}
+
+int get_engine(int device, Engine** out) {
+  if (device < 0) {
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+      return SPARX_E_CUDA;
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_engines_mu);
+  auto it = g_engines.find(device);
+  if (it != g_engines.end()) { *out = it->second; return SPARX_OK; }
+  Engine* E = new Engine();
+  int rc = engine_init(*E, device);
+  if (rc) { delete E; return rc; }
+  g_engines[device] = E;
+  *out = E;
+  return SPARX_OK;
+}
+
+int ensure_ws(Engine& E, size_t bytes) {
+  if (E.ws_cap >= bytes) return SPARX_OK;
+  if (E.peel.exec) {
+    cudaGraphExecDestroy(E.peel.exec);
+    cudaGraphDestroy(E.peel.graph);
+    E.peel = PeelGraph{};
+  }
+  if (E.ws) { CU(cudaStreamSynchronize(E.stream)); CU(cudaFree(E.ws)); E.ws = nullptr; E.ws_cap = 0; }
+  size_t cap = align_up(bytes + bytes / 8, 1 << 21);
+  cudaError_t e = cudaMalloc(&E.ws, cap);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMalloc(&E.ws, bytes);
+    cap = bytes;
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(std::string("workspace of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+      E.ws = nullptr;
+      return SPARX_E_OOM;
+    }
+  }
+  E.ws_cap = cap;
+  return SPARX_OK;
+}
+
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+  const size_t piece = 4ull << 20;
+  const long pieces = (long)((bytes + piece - 1) / piece);
+  if (pieces <= 1) { std::memcpy(dst, src, bytes); return; }
+  int nt = std::min<int>(omp_get_max_threads(), 16);
+#pragma omp parallel for num_threads(nt) schedule(static)
+  for (long i = 0; i < pieces; ++i) {
+    size_t o = (size_t)i * piece;
+    std::memcpy((char*)dst + o, (const char*)src + o, std::min(piece, bytes - o));
+  }
+}
+
+inline int grid_for(unsigned long long items, int threads, int cap_blocks) {
+  unsigned long long b = (items + threads - 1) / threads;
+  return (int)std::max<unsigned long long>(1, std::min<unsigned long long>(b, (unsigned long long)cap_blocks));
+}
+
+// host ids (u64 or u32) -> device u32 (+ base), chunked through pinned staging
+int upload_ids(Engine& E, const void* host, int bits, uint64_t count, uint32_t* dst, uint64_t n_limit,
+               uint32_t base, cudaStream_t s, char* stage[2], uint32_t* d_err) {
+  const size_t esz = bits == 64 ? 8 : 4;
+  const uint64_t chunk = kStageBytes / esz;
+  for (uint64_t c = 0, at = 0; at < count; ++c, at += chunk) {
+    const int slot = (int)(c & 1);
+    const uint64_t k = std::min<uint64_t>(chunk, count - at);
+    CU(cudaEventSynchronize(E.pin_ev[slot]));
+    parallel_copy(E.pinned[slot], (const char*)host + at * esz, k * esz);
+    CU(cudaMemcpyAsync(stage[slot], E.pinned[slot], k * esz, cudaMemcpyHostToDevice, s));
+    const int grid = grid_for(k, 256, E.sm_count * 16);
+    if (bits == 64)
+      k_narrow_ids<<<grid, 256, 0, s>>>((const unsigned long long*)stage[slot], dst + at, k, n_limit, base, d_err);
+    else
+      k_range_ids<<<grid, 256, 0, s>>>((const uint32_t*)stage[slot], dst + at, k, (uint32_t)n_limit, base, d_err);
+    CU(cudaEventRecord(E.pin_ev[slot], s));
+  }
+  return SPARX_OK;
+}
+
+int download(Engine& E, void* host, const void* dev, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return SPARX_OK;
+  const size_t chunk = kStageBytes;
+  const size_t nchunks = (bytes + chunk - 1) / chunk;
+  // issue chunk 0, then overlap copy-out of chunk c with the D2H of chunk c + 1
+  auto issue = [&](size_t c) -> int {
+    const int slot = (int)(c & 1);
+    const size_t at = c * chunk, k = std::min(chunk, bytes - at);
+    CU(cudaMemcpyAsync(E.pinned[slot], (const char*)dev + at, k, cudaMemcpyDeviceToHost, s));
+    CU(cudaEventRecord(E.pin_ev[slot], s));
+    return SPARX_OK;
+  };
+  CU(cudaEventSynchronize(E.pin_ev[0]));
+  CU(cudaEventSynchronize(E.pin_ev[1]));
+  int rc = issue(0);
+  if (rc) return rc;
+  for (size_t c = 0; c < nchunks; ++c) {
+    const int slot = (int)(c & 1);
+    if (c + 1 < nchunks) {
+      rc = issue(c + 1);
+      if (rc) return rc;
+    }
+    CU(cudaEventSynchronize(E.pin_ev[slot]));
+    const size_t at = c * chunk, k = std::min(chunk, bytes - at);
+    parallel_copy((char*)host + at, E.pinned[slot], k);
+  }
+  return SPARX_OK;
+}
+
+template <class T, class F>
+void exclusive_scan(F f, unsigned long long count, T* out, T* tiles, T* grand, cudaStream_t s) {
+  const unsigned long long ntiles = std::max<unsigned long long>(1, (count + kScanTile - 1) / kScanTile);
+  k_scan_reduce<T, F><<<(unsigned)ntiles, kScanThreads, 0, s>>>(f, count, tiles);
+  k_scan_tiles<T><<<1, kScanThreads, 0, s>>>(tiles, ntiles, grand);
+  k_scan_apply<T, F><<<(unsigned)ntiles, kScanThreads, 0, s>>>(f, count, tiles, out);
+}
+
+__global__ void k_member_edges(Member* mem, uint32_t G, const uint32_t* opos) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    const uint32_t eb = opos[mem[g].vb];
+    mem[g].eb = eb;
+    mem[g].m = opos[mem[g].vb + mem[g].n] - eb;
+  }
+}
+
+struct Opts {
+  uint32_t support_mode = SPARX_SUPPORT_WIDE;
+  uint32_t out_bits = 8;
+  int device = -1;
+  uint32_t loop = SPARX_LOOP_GRAPH;
+  uint32_t support_kernel = 0;
+  unsigned long long timeout_ms = kDefaultTimeoutMs;
+};
+
+int read_opts(const sparx_pkt_opts* o, Opts* out) {
+  Opts d;
+  if (o) {
+    if (o->struct_size && o->struct_size < sizeof(sparx_pkt_opts)) { set_error("opts.struct_size too small"); return SPARX_E_ARG; }
+    d.support_mode = o->support_mode;
+    d.out_bits = o->out_bits ? o->out_bits : 8;
+    d.device = o->device;
+    d.loop = o->loop;
+    d.support_kernel = o->support_kernel;
+    d.timeout_ms = o->timeout_ms ? o->timeout_ms : kDefaultTimeoutMs;
+  }
+  if (d.support_mode > 1 || (d.out_bits != 8 && d.out_bits != 32) || d.loop > 1) {
+    set_error("bad option value");
+    return SPARX_E_ARG;
+  }
+  *out = d;
+  return SPARX_OK;
+}
+
+// A prepared launch: members laid out in one union, CSR already on device.
+struct UnionJob {
+  uint64_t N = 0, W = 0;
+  std::vector<Member> members;  // vb, n, sb, w set; eb, m filled by the pipeline
+  Layout L{};
+  uint32_t* off = nullptr;
+  const uint32_t* nbr = nullptr;
+  void* out = nullptr;          // device truss output (u8 or u32 per slot)
+  bool support_only = false;
+  uint32_t* support_out = nullptr;  // device u32 per slot (support_only)
+  // results
+  std::vector<MemberState> states;
+  std::vector<unsigned long long> mem_tri;
+  std::vector<uint32_t> mem_maxsup;
+  unsigned long long self_loops = 0, tri = 0;
+  uint32_t kmax = 0;
+  uint32_t err = 0;
+  float ms_orient = 0, ms_support = 0, ms_peel = 0, ms_finalize = 0;
+};
+
+template <class T>
+T* at(Engine& E, size_t off) { return reinterpret_cast<T*>(E.ws + off); }
+
+int build_peel_graph(Engine& E, const UnionJob& J, cudaStream_t) {
+  const Layout& L = J.L;
+  std::vector<size_t> key = {(size_t)E.ws, L.uni, L.mem, L.st, L.ctl, L.wpref, L.cnt, (size_t)J.members.size(),
+                             (size_t)E.wave_blocks};
+  if (E.peel.exec && E.peel.key == key) return SPARX_OK;
+  if (E.peel.exec) {
+    cudaGraphExecDestroy(E.peel.exec);
+    cudaGraphDestroy(E.peel.graph);
+    E.peel = PeelGraph{};
+  }
+  cudaGraph_t g;
+  CU(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  CU(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  CU(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  WaveArgs wa;
+  wa.Up = at<Union>(E, L.uni);
+  wa.mem = at<Member>(E, L.mem);
+  wa.st = at<MemberState>(E, L.st);
+  wa.ctl = at<Control>(E, L.ctl);
+  wa.wpref = at<unsigned long long>(E, L.wpref);
+  wa.err = &at<Counters>(E, L.cnt)->err;
+  CU(cudaStreamBeginCaptureToGraph(E.capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  k_wave<<<E.wave_blocks, 256, 0, E.capture>>>(wa);
+  k_plan<<<1, 1024, 0, E.capture>>>(wa.mem, wa.st, wa.ctl, at<unsigned long long>(E, L.wpref), wa.err, h, 1);
+  cudaGraph_t captured;
+  CU(cudaStreamEndCapture(E.capture, &captured));
+  cudaGraphExec_t ex;
+  CU(cudaGraphInstantiate(&ex, g, 0));
+  E.peel.exec = ex;
+  E.peel.graph = g;
+  E.peel.key = key;
+  return SPARX_OK;
+}
+
+// Orientation, support, peel and finalize over a prepared union.
+int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
+  const Layout& L = J.L;
+  const uint32_t G = (uint32_t)J.members.size();
+  const uint32_t N = (uint32_t)J.N;
+  const uint64_t W = J.W;
+  Counters* cnt = at<Counters>(E, L.cnt);
+  uint32_t* err = &cnt->err;
+  uint32_t* eid = at<uint32_t>(E, L.eid);
+  uint32_t* dplus = at<uint32_t>(E, L.dplus);
+  uint32_t* opos = at<uint32_t>(E, L.opos);
+  uint32_t* ocol = at<uint32_t>(E, L.ocol);
+  uint32_t* osrc = at<uint32_t>(E, L.osrc);
+  int32_t* sup = at<int32_t>(E, L.sup);
+  Member* dmem = at<Member>(E, L.mem);
+  const int vgrid = grid_for((unsigned long long)N * 32, 256, E.sm_count * 32);
+
+  CU(cudaEventRecord(E.tev[1], s));
+  {
+    // offsets / ids validated by the upload must be sound before any kernel
+    // dereferences them
+    uint32_t* herr = (uint32_t*)E.pinned_small;
+    CU(cudaMemcpyAsync(herr, err, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (*herr) { J.err = *herr; return status_from_flags(*herr); }
+  }
+  // -- orientation (Kernel B) --
+  k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err);
+  exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
+  CU(cudaMemcpyAsync(dmem, J.members.data(), sizeof(Member) * G, cudaMemcpyHostToDevice, s));
+  k_member_edges<<<grid_for(G, 256, 1024), 256, 0, s>>>(dmem, G, opos);
+  CU(cudaMemcpyAsync(J.members.data(), dmem, sizeof(Member) * G, cudaMemcpyDeviceToHost, s));
+  Counters hc;
+  CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  uint32_t m32 = 0;
+  CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  J.self_loops = hc.self_loops;
+  if (hc.err) { J.err = hc.err; return status_from_flags(hc.err); }
+  const uint64_t m = m32;
+  if (2 * m + hc.self_loops != W) { J.err = kErrAsym; return SPARX_E_INVALID_CSR; }
+  for (const Member& M : J.members)
+    if (M.m > kEidMask) { set_error("a graph has >= 2^28 edges"); return SPARX_E_TOO_LARGE; }
+  k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, eid);
+  k_orient_reverse<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, eid, err);
+  CU(cudaEventRecord(E.tev[2], s));
+
+  // -- support (Kernel C) --
+  CU(cudaMemsetAsync(sup, 0, 4 * std::max<uint64_t>(m, 1), s));
+  unsigned long long* spref = at<unsigned long long>(E, L.q0);
+  if (m > 0) {
+    exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, at<unsigned long long>(E, L.tiles),
+                                       &cnt->grand, s);
+    k_support_balanced<<<E.sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, sup, &cnt->tri);
+  }
+  CU(cudaEventRecord(E.tev[3], s));
+
+  if (J.support_only) {
+    k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(eid, sup, W, J.support_out,
+                                                                       O.support_mode == SPARX_SUPPORT_U8);
+    CU(cudaEventRecord(E.tev[4], s));
+    CU(cudaEventRecord(E.tev[5], s));
+  } else {
+    // -- peel (Kernel D) --
+    Union U;
+    U.off = J.off;
+    U.nbr = J.nbr;
+    U.eid = eid;
+    U.opos = opos;
+    U.ocol = ocol;
+    U.osrc = osrc;
+    U.sup = sup;
+    U.tag = at<uint32_t>(E, L.tag);
+    U.act[0] = at<uint32_t>(E, L.act0);
+    U.act[1] = at<uint32_t>(E, L.act1);
+    U.q[0] = at<unsigned long long>(E, L.q0);
+    U.q[1] = at<unsigned long long>(E, L.q1);
+    U.n = N;
+    U.m = (uint32_t)m;
+    U.width = (uint32_t)W;
+    U.G = G;
+    CU(cudaMemcpyAsync(at<Union>(E, L.uni), &U, sizeof(Union), cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(at<unsigned long long>(E, L.mem_tri), 0, 8ull * G, s));
+    CU(cudaMemsetAsync(at<uint32_t>(E, L.mem_maxsup), 0, 4ull * G, s));
+    Control c0{};
+    c0.G = G;
+    c0.max_waves = 2ull * m + 64;
+    c0.timeout_ns = O.timeout_ms * 1000000ull;
+    CU(cudaMemcpyAsync(at<Control>(E, L.ctl), &c0, sizeof(Control), cudaMemcpyHostToDevice, s));
+    if (m > 0)
+      k_peel_setup<<<grid_for(m, 256, E.sm_count * 8), 256, 0, s>>>(at<Union>(E, L.uni), dmem,
+                                                                     O.support_mode == SPARX_SUPPORT_U8,
+                                                                     at<unsigned long long>(E, L.mem_tri),
+                                                                     at<uint32_t>(E, L.mem_maxsup));
+    k_peel_init<<<1, 1024, 0, s>>>(dmem, at<MemberState>(E, L.st), at<Control>(E, L.ctl),
+                                   at<unsigned long long>(E, L.wpref), G);
+    CU(cudaEventRecord(E.tev[4], s));
+    if (O.loop == SPARX_LOOP_GRAPH) {
+      int rc = build_peel_graph(E, J, s);
+      if (rc) return rc;
+      CU(cudaGraphLaunch(E.peel.exec, s));
+    } else {
+      WaveArgs wa;
+      wa.Up = at<Union>(E, L.uni);
+      wa.mem = dmem;
+      wa.st = at<MemberState>(E, L.st);
+      wa.ctl = at<Control>(E, L.ctl);
+      wa.wpref = at<unsigned long long>(E, L.wpref);
+      wa.err = err;
+      uint32_t* hdone = (uint32_t*)E.pinned_small;
+      for (;;) {
+        for (int i = 0; i < 16; ++i) {
+          k_wave<<<E.wave_blocks, 256, 0, s>>>(wa);
+          k_plan<<<1, 1024, 0, s>>>(wa.mem, wa.st, wa.ctl, at<unsigned long long>(E, L.wpref), err,
+                                    cudaGraphConditionalHandle{}, 0);
+        }
+        CU(cudaMemcpyAsync(hdone, &wa.ctl->done, 4, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (*hdone) break;
+      }
+    }
+    CU(cudaEventRecord(E.tev[5], s));
+    // -- finalize (Kernel E) --
+    const int fgrid = grid_for(W, 256, E.sm_count * 16);
+    const int u8 = O.support_mode == SPARX_SUPPORT_U8;
+    if (W > 0) {
+      if (O.out_bits == 8)
+        k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(eid, sup, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err);
+      else
+        k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(eid, sup, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err);
+    }
+  }
+  CU(cudaEventRecord(E.tev[6], s));
+  // read back
+  J.states.resize(G);
+  J.mem_tri.resize(G);
+  J.mem_maxsup.resize(G);
+  if (!J.support_only) {
+    CU(cudaMemcpyAsync(J.states.data(), at<MemberState>(E, L.st), sizeof(MemberState) * G, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(J.mem_tri.data(), at<unsigned long long>(E, L.mem_tri), 8ull * G, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(J.mem_maxsup.data(), at<uint32_t>(E, L.mem_maxsup), 4ull * G, cudaMemcpyDeviceToHost, s));
+  }
+  CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  J.tri = hc.tri;
+  J.kmax = hc.kmax;
+  J.err = hc.err;
+  CU(cudaEventElapsedTime(&J.ms_orient, E.tev[1], E.tev[2]));
+  CU(cudaEventElapsedTime(&J.ms_support, E.tev[2], E.tev[3]));
+  CU(cudaEventElapsedTime(&J.ms_peel, E.tev[4], E.tev[5]));
+  CU(cudaEventElapsedTime(&J.ms_finalize, E.tev[5], E.tev[6]));
+  CU(cudaGetLastError());
+  return status_from_flags(hc.err);
+}
+
+void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
+  if (!st) return;
+  std::memset(st, 0, sizeof(*st));
+  const Member& M = J.members[g];
+  st->n = M.n;
+  st->width = M.w;
+  st->m = M.m;
+  st->self_loops = M.w - 2ull * M.m;
+  if (g < J.mem_tri.size()) st->triangles = J.mem_tri[g] / 3;
+  if (g < J.mem_maxsup.size()) st->max_support = J.mem_maxsup[g];
+  if (g < J.states.size()) {
+    st->levels = J.states[g].levels;
+    st->waves = J.states[g].waves;
+    st->k_max = M.w ? J.states[g].max_level + 2 : 0;
+  }
+  if (J.members.size() == 1 && J.support_only) st->triangles = J.tri;
+  st->ms_orient = J.ms_orient;
+  st->ms_support = J.ms_support;
+  st->ms_peel = J.ms_peel;
+  st->ms_finalize = J.ms_finalize;
+}
+
+int check_dims(uint64_t n_plus_1, uint64_t width) {
+  if (n_plus_1 < 1) { set_error("n_plus_1 must be >= 1"); return SPARX_E_ARG; }
+  if (n_plus_1 - 1 >= 0xFFFFFFFFull || width >= 0xFFFFFFFFull) {
+    set_error("n or width does not fit 32 bits");
+    return SPARX_E_TOO_LARGE;
+  }
+  return SPARX_OK;
+}
+
+// Single graph from host memory (ids u64 or u32).
+int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int bits, uint64_t width,
+             void* out_host, bool support_only, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
+  g_last_error.clear();
+  if (!offsets || (!nbrs && width) || (!out_host && width)) { set_error("null pointer"); return SPARX_E_ARG; }
+  int rc = check_dims(n_plus_1, width);
+  if (rc) return rc;
+  Opts O;
+  rc = read_opts(opts, &O);
+  if (rc) return rc;
+  Engine* Ep;
+  rc = get_engine(O.device, &Ep);
+  if (rc) return rc;
+  Engine& E = *Ep;
+  std::lock_guard<std::mutex> lk(E.mu);
+  CU(cudaSetDevice(E.device));
+  const uint64_t n = n_plus_1 - 1;
+  UnionJob J;
+  J.N = n;
+  J.W = width;
+  J.members.push_back(Member{0, (uint32_t)n, 0, (uint32_t)width, 0, 0});
+  J.support_only = support_only;
+  const size_t out_bytes = support_only ? 4 * width : (O.out_bits / 8) * width;
+  J.L = make_layout(n, width, 1, true, out_bytes);
+  rc = ensure_ws(E, J.L.total);
+  if (rc) return rc;
+  cudaStream_t s = E.stream;
+  J.off = at<uint32_t>(E, J.L.off);
+  J.nbr = at<uint32_t>(E, J.L.nbr);
+  if (support_only) J.support_out = at<uint32_t>(E, J.L.out);
+  else J.out = at<void>(E, J.L.out);
+  char* stage[2] = {E.ws + J.L.stage0, E.ws + J.L.stage1};
+  Counters* cnt = at<Counters>(E, J.L.cnt);
+  auto t0 = std::chrono::steady_clock::now();
+  CU(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
+  CU(cudaEventRecord(E.tev[0], s));
+  bool bad_host = false;
+  {
+    // offsets: stage -> narrow (one chunk suffices below 8M vertices; larger
+    // offset arrays go through the same double-buffered loop)
+    const uint64_t chunk = kStageBytes / 8;
+    bad_host = offsets[0] != 0 || offsets[n] != width;
+    for (uint64_t c = 0, a = 0; a < n_plus_1; ++c, a += chunk) {
+      const int slot = (int)(c & 1);
+      const uint64_t k = std::min<uint64_t>(chunk, n_plus_1 - a);
+      if (a > 0 && offsets[a] < offsets[a - 1]) bad_host = true;
+      CU(cudaEventSynchronize(E.pin_ev[slot]));
+      parallel_copy(E.pinned[slot], offsets + a, k * 8);
+      CU(cudaMemcpyAsync(stage[slot], E.pinned[slot], k * 8, cudaMemcpyHostToDevice, s));
+      k_narrow_offsets<<<grid_for(k, 256, E.sm_count * 16), 256, 0, s>>>(
+          (const unsigned long long*)stage[slot], J.off + a, (uint32_t)k, 0u, -1ll, -1ll, &cnt->err);
+      CU(cudaEventRecord(E.pin_ev[slot], s));
+    }
+  }
+  if (bad_host) { set_error("offsets: first must be 0, last must equal width, non-decreasing"); return SPARX_E_INVALID_CSR; }
+  rc = upload_ids(E, nbrs, bits, width, (uint32_t*)J.nbr, n, 0, s, stage, &cnt->err);
+  if (rc) return rc;
+  auto t_up_host = std::chrono::steady_clock::now();
+  (void)t_up_host;
+  rc = run_union(E, J, O, s);
+  if (rc) {
+    fill_stats(J, 0, stats);
+    return rc;
+  }
+  CU(cudaEventRecord(E.tev[7], s));
+  rc = download(E, out_host, support_only ? (void*)J.support_out : J.out, out_bytes, s);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s));
+  auto t1 = std::chrono::steady_clock::now();
+  fill_stats(J, 0, stats);
+  if (stats) {
+    float up = 0;
+    cudaEventElapsedTime(&up, E.tev[0], E.tev[1]);
+    stats->ms_upload = up;
+    stats->ms_total = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    stats->ms_download = stats->ms_total - (up + J.ms_orient + J.ms_support + J.ms_peel + J.ms_finalize);
+  }
+  return SPARX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sparx_pkt_default_opts(sparx_pkt_opts* o) {
+  if (!o) return SPARX_E_ARG;
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = sizeof(sparx_pkt_opts);
+  o->support_mode = SPARX_SUPPORT_WIDE;
+  o->out_bits = 8;
+  o->device = -1;
+  o->loop = SPARX_LOOP_GRAPH;
+  o->support_kernel = 0;
+  o->timeout_ms = kDefaultTimeoutMs;
+  return SPARX_OK;
+}
+
+const char* sparx_strerror(int s) {
+  switch (s) {
+    case SPARX_OK: return "ok";
+    case SPARX_E_INVALID_CSR: return "invalid CSR (unsorted row, asymmetric, id >= n or bad offsets)";
+    case SPARX_E_MULTIGRAPH: return "parallel edges are not supported";
+    case SPARX_E_OVERFLOW_U8: return "truss number exceeds 255 with 8-bit output";
+    case SPARX_E_OOM: return "out of device memory / HBM budget";
+    case SPARX_E_TIMEOUT: return "device peel exceeded its time budget";
+    case SPARX_E_CUDA: return "CUDA error";
+    case SPARX_E_TOO_LARGE: return "graph too large (width >= 2^32 or m >= 2^28)";
+    case SPARX_E_ARG: return "bad argument";
+    case SPARX_E_NOT_FOUND: return "unknown ticket";
+    case SPARX_E_CANCELLED: return "request cancelled";
+    default: return "unknown status";
+  }
+}
+
+const char* sparx_last_error(void) { return g_last_error.c_str(); }
+
+int sparx_pkt_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
+                  void* truss_out, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
+  return run_host(offsets, n_plus_1, neighbours, 64, width, truss_out, false, opts, stats);
+}
+
+int sparx_pkt_run_u32(const uint64_t* offsets, uint64_t n_plus_1, const uint32_t* neighbours, uint64_t width,
+                      void* truss_out, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
+  return run_host(offsets, n_plus_1, neighbours, 32, width, truss_out, false, opts, stats);
+}
+
+int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
+                        uint32_t* support_out, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
+  return run_host(offsets, n_plus_1, neighbours, 64, width, support_out, true, opts, stats);
+}
+
+int sparx_pkt_run_device(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_neighbours, uint64_t width,
+                         void* d_truss_out, const sparx_pkt_opts* opts, sparx_pkt_stats* stats, void* cuda_stream) {
+  g_last_error.clear();
+  if (!d_offsets || (!d_neighbours && width) || (!d_truss_out && width)) { set_error("null pointer"); return SPARX_E_ARG; }
+  int rc = check_dims(n_plus_1, width);
+  if (rc) return rc;
+  Opts O;
+  rc = read_opts(opts, &O);
+  if (rc) return rc;
+  Engine* Ep;
+  rc = get_engine(O.device, &Ep);
+  if (rc) return rc;
+  Engine& E = *Ep;
+  std::lock_guard<std::mutex> lk(E.mu);
+  CU(cudaSetDevice(E.device));
+  const uint64_t n = n_plus_1 - 1;
+  UnionJob J;
+  J.N = n;
+  J.W = width;
+  J.members.push_back(Member{0, (uint32_t)n, 0, (uint32_t)width, 0, 0});
+  J.L = make_layout(n, width, 1, false, 0);
+  rc = ensure_ws(E, J.L.total);
+  if (rc) return rc;
+  cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : E.stream;
+  J.off = at<uint32_t>(E, J.L.off);
+  J.nbr = d_neighbours;
+  J.out = d_truss_out;
+  Counters* cnt = at<Counters>(E, J.L.cnt);
+  auto t0 = std::chrono::steady_clock::now();
+  CU(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
+  CU(cudaEventRecord(E.tev[0], s));
+  k_narrow_offsets<<<grid_for(n_plus_1, 256, E.sm_count * 16), 256, 0, s>>>(
+      (const unsigned long long*)d_offsets, J.off, (uint32_t)n_plus_1, 0u, 0ll, (long long)width, &cnt->err);
+  if (width)
+    k_range_ids<<<grid_for(width, 256, E.sm_count * 16), 256, 0, s>>>(d_neighbours, nullptr, width, (uint32_t)n, 0u,
+                                                                       &cnt->err);
+  rc = run_union(E, J, O, s);
+  fill_stats(J, 0, stats);
+  if (rc) return rc;
+  auto t1 = std::chrono::steady_clock::now();
+  if (stats) {
+    float up = 0;
+    cudaEventElapsedTime(&up, E.tev[0], E.tev[1]);
+    stats->ms_upload = up;
+    stats->ms_total = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  }
+  return SPARX_OK;
+}
+
+}  // extern "C"

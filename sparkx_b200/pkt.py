@@ -1,0 +1,291 @@
+"""``AlgoPKT`` / ``Triangles`` over the CUDA engine (``libsparx_pkt.so``).
+
+Mirrors the reference's PKT entry point (``src/k_truss/pkt.rs:29-123``):
+
+* ``AlgoPKT.new(g)``                 pkt.rs:45-52   (threads argument of the
+  ``AlgoPKT.new_with_conf(g, threads)`` pkt.rs:85-95   reference is accepted and
+                                                    ignored: the GPU does the work)
+* ``AlgoPKT.get_or_compute(g)``      pkt.rs:61-76   (re-uses the cached result file)
+* ``trussness(e)``                   pkt.rs:104-107 (asserts ``e < g.width()``)
+* ``k_trusses()``                    pkt.rs:112-114 (u8 per CSR slot)
+* ``drop_cache()``                   pkt.rs:117-122 (removes the result file)
+
+and ``Triangles`` (``src/k_truss/triangles.rs:16-69``): support per CSR slot.
+
+Errors are raised as ``PktError`` carrying the C status, the way the reference
+returns ``Box<dyn Error>`` (e.g. the u8 level overflow at pkt.rs:508-516).
+The native library is mandatory; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+
+import numpy as np
+
+from ._native import load_library
+from .graph import GraphMemoryMap
+
+OK = 0
+E_INVALID_CSR = 1
+E_MULTIGRAPH = 2
+E_OVERFLOW_U8 = 3
+E_OOM = 4
+E_TIMEOUT = 5
+E_CUDA = 6
+E_TOO_LARGE = 7
+E_ARG = 8
+E_NOT_FOUND = 9
+E_CANCELLED = 10
+
+SUPPORT_WIDE = 0
+SUPPORT_U8 = 1
+LOOP_GRAPH = 0
+LOOP_HOST = 1
+
+CACHE_DIR = os.environ.get("SPARX_CACHE_DIR", "./.cache")
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("support_mode", ctypes.c_uint32),
+        ("out_bits", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("loop", ctypes.c_uint32),
+        ("support_kernel", ctypes.c_uint32),
+        ("timeout_ms", ctypes.c_uint64),
+    ]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint64), ("width", ctypes.c_uint64), ("m", ctypes.c_uint64),
+        ("self_loops", ctypes.c_uint64), ("triangles", ctypes.c_uint64),
+        ("max_support", ctypes.c_uint64), ("k_max", ctypes.c_uint32), ("levels", ctypes.c_uint32),
+        ("waves", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+        ("ms_upload", ctypes.c_double), ("ms_orient", ctypes.c_double),
+        ("ms_support", ctypes.c_double), ("ms_peel", ctypes.c_double),
+        ("ms_finalize", ctypes.c_double), ("ms_download", ctypes.c_double),
+        ("ms_total", ctypes.c_double),
+    ]
+
+
+class _GraphView(ctypes.Structure):
+    _fields_ = [
+        ("offsets", ctypes.c_void_p), ("n_plus_1", ctypes.c_uint64),
+        ("neighbours", ctypes.c_void_p), ("width", ctypes.c_uint64),
+        ("neighbour_bits", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+        ("truss_out", ctypes.c_void_p),
+    ]
+
+
+EXPORTS = [
+    "sparx_pkt_default_opts", "sparx_strerror", "sparx_last_error", "sparx_pkt_run",
+    "sparx_pkt_run_u32", "sparx_pkt_run_device", "sparx_triangles_run", "sparx_pkt_run_batch",
+    "sparx_server_create", "sparx_server_submit", "sparx_server_poll", "sparx_server_wait",
+    "sparx_server_cancel", "sparx_server_destroy",
+]
+
+
+def lib():
+    L = load_library("libsparx_pkt.so")
+    if getattr(L, "_sparx_typed", False):
+        return L
+    vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+    P = ctypes.POINTER
+    L.sparx_pkt_default_opts.restype = i32
+    L.sparx_pkt_default_opts.argtypes = [P(_Opts)]
+    L.sparx_strerror.restype = ctypes.c_char_p
+    L.sparx_strerror.argtypes = [i32]
+    L.sparx_last_error.restype = ctypes.c_char_p
+    L.sparx_last_error.argtypes = []
+    for name in ("sparx_pkt_run", "sparx_pkt_run_u32", "sparx_triangles_run"):
+        f = getattr(L, name)
+        f.restype = i32
+        f.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats)]
+    L.sparx_pkt_run_device.restype = i32
+    L.sparx_pkt_run_device.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats), vp]
+    if hasattr(L, "sparx_pkt_run_batch"):
+        L.sparx_pkt_run_batch.restype = i32
+        L.sparx_pkt_run_batch.argtypes = [P(_GraphView), u64, u64, P(_Opts), P(ctypes.c_int), P(_Stats)]
+    L._sparx_typed = True
+    return L
+
+
+class PktError(RuntimeError):
+    def __init__(self, status: int, detail: str = ""):
+        self.status = status
+        msg = lib().sparx_strerror(status).decode()
+        super().__init__(f"{msg} (status {status})" + (f": {detail}" if detail else ""))
+
+
+@dataclasses.dataclass
+class PktOptions:
+    support_mode: int = SUPPORT_WIDE   # SUPPORT_U8 reproduces the reference's u8 counters
+    out_bits: int = 8                  # 8: reference layout (u8 per slot); 32: u32
+    device: int = -1
+    loop: int = LOOP_GRAPH
+    support_kernel: int = 0
+    timeout_ms: int = 0
+
+    def c(self) -> _Opts:
+        o = _Opts()
+        lib().sparx_pkt_default_opts(ctypes.byref(o))
+        o.support_mode = self.support_mode
+        o.out_bits = self.out_bits
+        o.device = self.device
+        o.loop = self.loop
+        o.support_kernel = self.support_kernel
+        if self.timeout_ms:
+            o.timeout_ms = self.timeout_ms
+        return o
+
+
+@dataclasses.dataclass
+class PktStats:
+    n: int = 0
+    width: int = 0
+    m: int = 0
+    self_loops: int = 0
+    triangles: int = 0
+    max_support: int = 0
+    k_max: int = 0
+    levels: int = 0
+    waves: int = 0
+    ms_upload: float = 0.0
+    ms_orient: float = 0.0
+    ms_support: float = 0.0
+    ms_peel: float = 0.0
+    ms_finalize: float = 0.0
+    ms_download: float = 0.0
+    ms_total: float = 0.0
+
+    @classmethod
+    def from_c(cls, s: _Stats) -> "PktStats":
+        return cls(**{f.name: getattr(s, f.name) for f in dataclasses.fields(cls)})
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise PktError(rc, lib().sparx_last_error().decode())
+
+
+def _arrays(g: GraphMemoryMap):
+    off = np.ascontiguousarray(g.offsets(), dtype=np.uint64)
+    nbr = np.ascontiguousarray(g.neighbours())
+    return off, nbr
+
+
+def run_pkt(offsets: np.ndarray, neighbours: np.ndarray, opts: PktOptions | None = None):
+    """Truss per CSR slot (u8 or u32 per ``opts.out_bits``) and stats."""
+    opts = opts or PktOptions()
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    nbr = np.ascontiguousarray(neighbours)
+    out = np.empty(nbr.shape[0], dtype=np.uint8 if opts.out_bits == 8 else np.uint32)
+    st = _Stats()
+    o = opts.c()
+    L = lib()
+    if nbr.dtype == np.uint64:
+        rc = L.sparx_pkt_run(off.ctypes.data, off.shape[0], nbr.ctypes.data, nbr.shape[0],
+                             out.ctypes.data, ctypes.byref(o), ctypes.byref(st))
+    elif nbr.dtype == np.uint32:
+        rc = L.sparx_pkt_run_u32(off.ctypes.data, off.shape[0], nbr.ctypes.data, nbr.shape[0],
+                                 out.ctypes.data, ctypes.byref(o), ctypes.byref(st))
+    else:
+        raise TypeError("neighbours must be u64 or u32")
+    _check(rc)
+    return out, PktStats.from_c(st)
+
+
+def run_triangles(offsets: np.ndarray, neighbours: np.ndarray, opts: PktOptions | None = None):
+    """Triangle support per CSR slot (u32), as ``Triangles::new`` computes it."""
+    opts = opts or PktOptions()
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    nbr = np.ascontiguousarray(neighbours, dtype=np.uint64)
+    out = np.empty(nbr.shape[0], dtype=np.uint32)
+    st = _Stats()
+    o = opts.c()
+    _check(lib().sparx_triangles_run(off.ctypes.data, off.shape[0], nbr.ctypes.data, nbr.shape[0],
+                                     out.ctypes.data, ctypes.byref(o), ctypes.byref(st)))
+    return out, PktStats.from_c(st)
+
+
+def _cache_file(g: GraphMemoryMap, kind: str) -> str:
+    os.makedirs(CACHE_DIR, exist_ok=True)
+    return os.path.join(CACHE_DIR, f"{kind}_{g.graph_id()}.mmap")
+
+
+class AlgoPKT:
+    """PKT k-truss decomposition of a ``GraphMemoryMap`` (pkt.rs:29-35)."""
+
+    def __init__(self, g: GraphMemoryMap, k_trusses: np.ndarray, threads: int,
+                 stats: PktStats | None = None):
+        self.g = g
+        self._k_trusses = k_trusses
+        self.threads = threads
+        self.stats = stats
+
+    @classmethod
+    def new(cls, g: GraphMemoryMap, opts: PktOptions | None = None) -> "AlgoPKT":
+        return cls.new_with_conf(g, g.thread_num(), opts)
+
+    @classmethod
+    def new_with_conf(cls, g: GraphMemoryMap, threads: int,
+                      opts: PktOptions | None = None) -> "AlgoPKT":
+        opts = opts or PktOptions()
+        off, nbr = _arrays(g)
+        truss, stats = run_pkt(off, nbr, opts)
+        if opts.out_bits == 8:
+            path = _cache_file(g, "ktrusspkt")
+            mm = np.memmap(path, dtype=np.uint8, mode="w+", shape=(max(1, truss.shape[0]),))
+            mm[: truss.shape[0]] = truss
+            mm.flush()
+        return cls(g, truss, max(1, int(threads)), stats)
+
+    @classmethod
+    def get_or_compute(cls, g: GraphMemoryMap, opts: PktOptions | None = None) -> "AlgoPKT":
+        path = _cache_file(g, "ktrusspkt")
+        if os.path.exists(path):
+            mm = np.memmap(path, dtype=np.uint8, mode="r")
+            if mm.shape[0] >= g.width():
+                return cls(g, np.asarray(mm[: g.width()]), g.thread_num())
+        return cls.new(g, opts)
+
+    def trussness(self, e_idx: int) -> int:
+        assert e_idx < self.g.width()
+        return int(self._k_trusses[e_idx])
+
+    def k_trusses(self) -> np.ndarray:
+        return self._k_trusses
+
+    def drop_cache(self) -> None:
+        path = _cache_file(self.g, "ktrusspkt")
+        os.remove(path)
+
+    def get_throughput_factor(self) -> int:
+        """pkt.rs:176-178: the bench divides by the CSR width."""
+        return self.g.width()
+
+
+class Triangles:
+    """Per-slot triangle support of a ``GraphMemoryMap`` (triangles.rs:16-69)."""
+
+    def __init__(self, g: GraphMemoryMap, support: np.ndarray, stats: PktStats):
+        self.g = g
+        self._support = support
+        self.stats = stats
+
+    @classmethod
+    def new(cls, g: GraphMemoryMap, opts: PktOptions | None = None) -> "Triangles":
+        off, nbr = _arrays(g)
+        sup, stats = run_triangles(off, nbr, opts)
+        return cls(g, sup, stats)
+
+    def triangles(self, e_idx: int) -> int:
+        assert e_idx < self.g.width()
+        return int(self._support[e_idx])
+
+    def all_triangles(self) -> np.ndarray:
+        return self._support
