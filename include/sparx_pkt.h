@@ -63,8 +63,14 @@ typedef struct sparx_pkt_stats {
   uint32_t k_max;          /* largest truss number */
   uint32_t levels;         /* non-empty peel levels */
   uint32_t waves;          /* device peel waves (sub-levels + level scans) */
-  uint32_t reserved;
+  uint32_t launches;       /* kernels this call launched (graph-internal ones included) */
   double ms_upload, ms_orient, ms_support, ms_peel, ms_finalize, ms_download, ms_total;
+  /* work counters behind the roofline figures */
+  uint64_t support_elements;  /* shorter-out-list entries searched by the support kernel */
+  uint64_t peel_elements;     /* shorter-row entries searched by the peel (all waves) */
+  uint64_t peel_hits;         /* triangles found by the peel (processed or skipped) */
+  uint64_t peel_scanned;      /* active-list entries read by level scans */
+  uint64_t peel_edges;        /* frontier edges processed (= m minus zero-support edges) */
 } sparx_pkt_stats;
 
 /* Fill `opts` with defaults (wide support, u8 output, device loop). */
@@ -134,30 +140,6 @@ typedef struct sparx_graph_view {
  */
 int sparx_pkt_run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
                         const sparx_pkt_opts* opts, int* status_out, sparx_pkt_stats* stats_out);
-
-/* ---- serving: continuous batching ------------------------------------ */
-typedef struct sparx_server sparx_server;
-
-/* Create a server on opts->device with an HBM budget (0 = 150 GB). */
-int sparx_server_create(sparx_server** out, uint64_t hbm_budget_bytes, const sparx_pkt_opts* opts);
-
-/* Queue a decomposition; the arrays must stay valid until sparx_server_poll
- * reports it done.  *ticket identifies the request. */
-int sparx_server_submit(sparx_server* s, const sparx_graph_view* graph, uint64_t* ticket);
-
-/* Non-blocking: *done = 1 once finished; *status is that request's status. */
-int sparx_server_poll(sparx_server* s, uint64_t ticket, int* done, int* status,
-                      sparx_pkt_stats* stats);
-
-/* Block until the request finishes (timeout_ms 0 = forever). */
-int sparx_server_wait(sparx_server* s, uint64_t ticket, uint64_t timeout_ms, int* status,
-                      sparx_pkt_stats* stats);
-
-/* Cancel a queued (not yet admitted) request. */
-int sparx_server_cancel(sparx_server* s, uint64_t ticket);
-
-/* Drain and free. */
-int sparx_server_destroy(sparx_server* s);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <omp.h>
+
 namespace {
 
 enum {
@@ -488,105 +490,139 @@ uint64_t verify(const Csr& g, const uint64_t* er, const uint32_t* truss, int T) 
 
 // Independent exact truss decomposition (no reference counterpart), used for
 // the workloads the restatements are too slow for.  Support per undirected
-// edge by degree-oriented intersection, then a level-synchronous peel in
-// which every triangle of a peeled edge is resolved against the edge ids
-// (not a slot tie-break): a triangle charges its surviving edges once, when
-// its first edge is peeled; ties inside one frontier go to the smaller id.
-struct Oriented {
-  std::vector<uint64_t> eid;     // per slot, UINT64_MAX for self-loops
-  std::vector<uint64_t> src, dst;
-};
-
+// edge by degree-oriented merge intersection; then a level-synchronous peel:
+// every triangle of a peeled edge is resolved on edge ids -- a triangle
+// charges its surviving edges once, when its first edge is peeled, and ties
+// inside one frontier go to the smallest id.  Rows are rebuilt without
+// peeled edges whenever the live edge count halves.
 int fast_truss(const Csr& g, int T, int u8mode, uint32_t* truss_out, uint64_t* tri_out,
                uint64_t* levels_out) {
   const uint64_t n = g.n, W = g.width();
+  omp_set_num_threads(T);
   auto deg = [&](uint64_t x) { return g.off[x + 1] - g.off[x]; };
-  auto before = [&](uint64_t a, uint64_t b) {  // degree order, ties by id
+  auto before = [&](uint64_t a, uint64_t b) {
     uint64_t da = deg(a), db = deg(b);
     return da < db || (da == db && a < b);
   };
   // undirected edge ids: upper slots (u < v) in CSR order
+  std::vector<uint64_t> upc(n + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (uint64_t u = 0; u < n; ++u) {
+    uint64_t c = 0;
+    for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s) c += g.nbr[s] > u;
+    upc[u + 1] = c;
+  }
+  for (uint64_t u = 0; u < n; ++u) upc[u + 1] += upc[u];
+  const uint64_t m = upc[n];
   std::vector<uint64_t> eid(W, UINT64_MAX);
-  std::vector<uint64_t> src, dst;
-  for (uint64_t u = 0; u < n; ++u)
+  std::vector<uint32_t> src(m), dst(m);
+  std::atomic<int> bad{0};
+#pragma omp parallel for schedule(static)
+  for (uint64_t u = 0; u < n; ++u) {
+    uint64_t p = upc[u];
     for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s)
-      if (g.nbr[s] > u) { eid[s] = src.size(); src.push_back(u); dst.push_back(g.nbr[s]); }
-  const uint64_t m = src.size();
+      if (g.nbr[s] > u) { eid[s] = p; src[p] = (uint32_t)u; dst[p] = g.nbr[s]; ++p; }
+  }
+#pragma omp parallel for schedule(dynamic, 1024)
   for (uint64_t u = 0; u < n; ++u)
     for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s) {
       uint64_t v = g.nbr[s];
       if (v >= u) continue;
       uint64_t lo = g.off[v], hi = g.off[v + 1];
       while (lo < hi) { uint64_t mid = (lo + hi) / 2; if (g.nbr[mid] < u) lo = mid + 1; else hi = mid; }
-      if (lo == g.off[v + 1] || g.nbr[lo] != u) return ORC_E_INVALID;
+      if (lo == g.off[v + 1] || g.nbr[lo] != u) { bad = 1; continue; }
       eid[s] = eid[lo];
     }
+  if (bad) return ORC_E_INVALID;
   // oriented out-lists (vertex ids ascending), with edge ids
   std::vector<uint64_t> opos(n + 1, 0);
+#pragma omp parallel for schedule(static)
   for (uint64_t u = 0; u < n; ++u) {
     uint64_t c = 0;
     for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s)
       if (g.nbr[s] != u && before(u, g.nbr[s])) ++c;
-    opos[u + 1] = opos[u] + c;
+    opos[u + 1] = c;
   }
+  for (uint64_t u = 0; u < n; ++u) opos[u + 1] += opos[u];
   std::vector<uint32_t> ocol(m);
   std::vector<uint64_t> oeid(m);
+#pragma omp parallel for schedule(static)
   for (uint64_t u = 0; u < n; ++u) {
     uint64_t p = opos[u];
     for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s)
       if (g.nbr[s] != u && before(u, g.nbr[s])) { ocol[p] = g.nbr[s]; oeid[p] = eid[s]; ++p; }
   }
-  std::vector<std::atomic<uint32_t>> sup(m);
-  for (uint64_t e = 0; e < m; ++e) sup[e].store(0, std::memory_order_relaxed);
-  std::atomic<uint64_t> tri{0};
-  std::atomic<uint64_t> next_u{0};
-  run_threads(T, [&](int) {
-    uint64_t local = 0;
-    for (;;) {
-      uint64_t u0 = next_u.fetch_add(256);
-      if (u0 >= n) break;
-      for (uint64_t a = u0; a < std::min<uint64_t>(u0 + 256, n); ++a) {
-        for (uint64_t p = opos[a]; p < opos[a + 1]; ++p) {
-          uint64_t b = ocol[p];
-          uint64_t i = opos[a], ie = opos[a + 1], j = opos[b], je = opos[b + 1];
-          uint32_t cnt = 0;
-          while (i < ie && j < je) {
-            if (ocol[i] < ocol[j]) ++i;
-            else if (ocol[j] < ocol[i]) ++j;
-            else {
-              ++cnt;
-              sup[oeid[i]].fetch_add(1, std::memory_order_relaxed);
-              sup[oeid[j]].fetch_add(1, std::memory_order_relaxed);
-              ++i; ++j;
-            }
-          }
-          if (cnt) sup[oeid[p]].fetch_add(cnt, std::memory_order_relaxed);
-          local += cnt;
+  std::vector<std::atomic<int64_t>> as(m);
+#pragma omp parallel for schedule(static)
+  for (uint64_t e = 0; e < m; ++e) as[e].store(0, std::memory_order_relaxed);
+  uint64_t tri = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : tri)
+  for (uint64_t a = 0; a < n; ++a) {
+    for (uint64_t p = opos[a]; p < opos[a + 1]; ++p) {
+      uint64_t b = ocol[p];
+      uint64_t i = opos[a], ie = opos[a + 1], j = opos[b], je = opos[b + 1];
+      int64_t cnt = 0;
+      while (i < ie && j < je) {
+        if (ocol[i] < ocol[j]) ++i;
+        else if (ocol[j] < ocol[i]) ++j;
+        else {
+          ++cnt;
+          as[oeid[i]].fetch_add(1, std::memory_order_relaxed);
+          as[oeid[j]].fetch_add(1, std::memory_order_relaxed);
+          ++i; ++j;
         }
       }
+      if (cnt) as[oeid[p]].fetch_add(cnt, std::memory_order_relaxed);
+      tri += cnt;
     }
-    tri += local;
-  });
-  if (tri_out) *tri_out = tri.load();
+  }
+  if (tri_out) *tri_out = tri;
   std::vector<int64_t> s(m);
+#pragma omp parallel for schedule(static)
   for (uint64_t e = 0; e < m; ++e) {
-    uint32_t v = sup[e].load(std::memory_order_relaxed);
-    s[e] = u8mode ? (v & 0xFF) : v;
+    int64_t v = as[e].load(std::memory_order_relaxed);
+    if (u8mode) v &= 0xFF;
+    s[e] = v;
+    as[e].store(v, std::memory_order_relaxed);
   }
-  // peel: state 0 live, 1 in current frontier, 2 done
-  std::vector<uint8_t> state(m, 0);
+  // live adjacency (rows of live edges: neighbour + edge id), rebuilt as edges die
+  std::vector<uint8_t> state(m, 0);  // 0 live, 1 frontier, 2 done
+  for (uint64_t e = 0; e < m; ++e) if (s[e] == 0) state[e] = 2;
+  std::vector<uint64_t> loff(n + 1);
+  std::vector<uint32_t> lnbr;
+  std::vector<uint64_t> leid;
+  uint64_t live_in_rows = 0;
+  auto rebuild = [&]() {
+    std::vector<uint64_t> cnt(n + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (uint64_t u = 0; u < n; ++u) {
+      uint64_t c = 0;
+      for (uint64_t x = g.off[u]; x < g.off[u + 1]; ++x) c += eid[x] != UINT64_MAX && state[eid[x]] != 2;
+      cnt[u + 1] = c;
+    }
+    for (uint64_t u = 0; u < n; ++u) cnt[u + 1] += cnt[u];
+    loff = cnt;
+    lnbr.assign(loff[n], 0);
+    leid.assign(loff[n], 0);
+#pragma omp parallel for schedule(static)
+    for (uint64_t u = 0; u < n; ++u) {
+      uint64_t p = loff[u];
+      for (uint64_t x = g.off[u]; x < g.off[u + 1]; ++x)
+        if (eid[x] != UINT64_MAX && state[eid[x]] != 2) { lnbr[p] = g.nbr[x]; leid[p] = eid[x]; ++p; }
+    }
+    live_in_rows = loff[n] / 2;
+  };
+  rebuild();
   std::vector<uint64_t> live, frontier, nextf;
-  live.reserve(m);
-  for (uint64_t e = 0; e < m; ++e) {
-    if (s[e] == 0) state[e] = 2; else live.push_back(e);
-  }
-  std::vector<std::atomic<int64_t>> as(m);
-  for (uint64_t e = 0; e < m; ++e) as[e].store(s[e], std::memory_order_relaxed);
+  for (uint64_t e = 0; e < m; ++e) if (state[e] == 0) live.push_back(e);
   uint64_t levels = 0;
   int64_t l = 0;
+  std::vector<std::vector<uint64_t>> pushed(T);
   while (!live.empty()) {
+    if (live.size() * 2 < live_in_rows) rebuild();
     int64_t mn = INT64_MAX;
-    for (uint64_t e : live) mn = std::min<int64_t>(mn, as[e].load(std::memory_order_relaxed));
+#pragma omp parallel for schedule(static) reduction(min : mn)
+    for (uint64_t i = 0; i < live.size(); ++i) mn = std::min<int64_t>(mn, as[live[i]].load(std::memory_order_relaxed));
     l = mn;
     if (u8mode && l > 254) return ORC_E_OVERFLOW;
     frontier.clear();
@@ -598,52 +634,49 @@ int fast_truss(const Csr& g, int T, int u8mode, uint32_t* truss_out, uint64_t* t
     live.swap(keep);
     ++levels;
     while (!frontier.empty()) {
-      std::vector<std::vector<uint64_t>> pushed(T);
-      std::atomic<uint64_t> cursor{0};
-      run_threads(T, [&](int tid) {
-        for (;;) {
-          uint64_t i = cursor.fetch_add(64);
-          if (i >= frontier.size()) break;
-          for (uint64_t k = i; k < std::min<uint64_t>(i + 64, frontier.size()); ++k) {
-            uint64_t e = frontier[k];
-            uint64_t u = src[e], v = dst[e];
-            uint64_t small = deg(u) <= deg(v) ? u : v, large = small == u ? v : u;
-            for (uint64_t si = g.off[small]; si < g.off[small + 1]; ++si) {
-              uint64_t w = g.nbr[si];
-              if (w == u || w == v) continue;
-              uint64_t lo = g.off[large], hi = g.off[large + 1];
-              while (lo < hi) { uint64_t mid = (lo + hi) / 2; if (g.nbr[mid] < w) lo = mid + 1; else hi = mid; }
-              if (lo == g.off[large + 1] || g.nbr[lo] != w) continue;
-              uint64_t f = eid[si], h = eid[lo];
-              if (state[f] == 2 || state[h] == 2) continue;
-              bool fin = state[f] == 1, hin = state[h] == 1;
-              auto dec = [&](uint64_t x) {
-                int64_t prev = as[x].fetch_sub(1, std::memory_order_relaxed);
-                if (prev == l + 1) pushed[tid].push_back(x);
-              };
-              // charge surviving edges once: if another frontier edge shares
-              // the triangle, the smallest frontier id charges
-              if (fin && f < e) continue;
-              if (hin && h < e) continue;
-              if (!fin && as[f].load(std::memory_order_relaxed) > l) dec(f);
-              if (!hin && as[h].load(std::memory_order_relaxed) > l) dec(h);
-            }
+      for (auto& p : pushed) p.clear();
+#pragma omp parallel
+      {
+        std::vector<uint64_t>& mine = pushed[omp_get_thread_num()];
+#pragma omp for schedule(dynamic, 16)
+        for (uint64_t k = 0; k < frontier.size(); ++k) {
+          uint64_t e = frontier[k];
+          uint64_t u = src[e], v = dst[e];
+          uint64_t du = loff[u + 1] - loff[u], dv = loff[v + 1] - loff[v];
+          uint64_t small = du <= dv ? u : v, large = small == u ? v : u;
+          for (uint64_t si = loff[small]; si < loff[small + 1]; ++si) {
+            uint64_t w = lnbr[si];
+            if (w == u || w == v) continue;
+            uint64_t lo = loff[large], hi = loff[large + 1];
+            while (lo < hi) { uint64_t mid = (lo + hi) / 2; if (lnbr[mid] < w) lo = mid + 1; else hi = mid; }
+            if (lo == loff[large + 1] || lnbr[lo] != w) continue;
+            uint64_t f = leid[si], h = leid[lo];
+            if (state[f] == 2 || state[h] == 2) continue;
+            bool fin = state[f] == 1, hin = state[h] == 1;
+            if (fin && f < e) continue;
+            if (hin && h < e) continue;
+            auto dec = [&](uint64_t x) {
+              int64_t prev = as[x].fetch_sub(1, std::memory_order_relaxed);
+              if (prev == l + 1) mine.push_back(x);
+            };
+            if (!fin && as[f].load(std::memory_order_relaxed) > l) dec(f);
+            if (!hin && as[h].load(std::memory_order_relaxed) > l) dec(h);
           }
         }
-      });
+      }
       for (uint64_t e : frontier) { state[e] = 2; s[e] = l; }
       nextf.clear();
       for (auto& p : pushed) nextf.insert(nextf.end(), p.begin(), p.end());
       for (uint64_t e : nextf) state[e] = 1;
-      // edges whose count fell below l are pinned at l
       frontier.swap(nextf);
-      std::vector<uint64_t> keep2;
-      keep2.reserve(live.size());
-      for (uint64_t e : live) if (state[e] == 0) keep2.push_back(e);
-      live.swap(keep2);
     }
+    std::vector<uint64_t> keep2;
+    keep2.reserve(live.size());
+    for (uint64_t e : live) if (state[e] == 0) keep2.push_back(e);
+    live.swap(keep2);
   }
   if (levels_out) *levels_out = levels;
+#pragma omp parallel for schedule(static)
   for (uint64_t x = 0; x < W; ++x) {
     uint64_t e = eid[x];
     uint64_t v = (e == UINT64_MAX) ? 2 : (uint64_t)s[e] + 2;

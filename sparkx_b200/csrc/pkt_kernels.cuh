@@ -110,6 +110,11 @@ struct Control {
   unsigned long long t_start;
   unsigned long long timeout_ns;
   unsigned long long waves_run;
+  // work counters (roofline accounting)
+  unsigned long long el_proc;     // frontier elements searched
+  unsigned long long el_scan;     // active-list entries scanned
+  unsigned long long hits;        // triangles found by frontier elements
+  unsigned long long edges_proc;  // frontier edges processed
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -622,6 +627,7 @@ __global__ void k_peel_init(const Member* __restrict__ mem, MemberState* __restr
     ctl->wave = 1;
     ctl->done = carry == 0;
     ctl->waves_run = 0;
+    ctl->el_scan = carry;
     ctl->t_start = globaltimer();
   }
 }
@@ -765,6 +771,7 @@ __global__ void __launch_bounds__(256) k_wave(WaveArgs a) {
   const UnionRegs U(a.Up);
   unsigned long long ch = total / (nwarps * 4);
   ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
+  uint32_t hits = 0;
 
   for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
     const unsigned long long kend = min(c0 + ch, total);
@@ -809,6 +816,7 @@ __global__ void __launch_bounds__(256) k_wave(WaveArgs a) {
               if (p < le && __ldg(U.nbr + p) == w) {
                 f = __ldg(U.eid + slot);
                 h = __ldg(U.eid + p);
+                ++hits;
                 pkt_rule(U, e, f, h, level, W, pf, ph);
               }
             }
@@ -860,6 +868,9 @@ __global__ void __launch_bounds__(256) k_wave(WaveArgs a) {
       k = seg_end;
     }
   }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) hits += __shfl_xor_sync(kFull, hits, d);
+  if (lane == 0 && hits) atomicAdd(&a.ctl->hits, (unsigned long long)hits);
 }
 
 // Planner: one block advances every member's state machine after a wave and
@@ -870,8 +881,9 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
                                                int use_handle) {
   __shared__ unsigned long long sw[32];
   __shared__ uint32_t s_live;
+  __shared__ unsigned long long s_proc, s_scan, s_edges;
   const uint32_t G = ctl->G;
-  if (threadIdx.x == 0) s_live = 0;
+  if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; }
   __syncthreads();
   const bool was_done = ctl->done;
   unsigned long long carry = 0;
@@ -928,8 +940,14 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
       }
       if (s.phase != kPhaseDone) s.waves++;
       st[g] = s;
-      if (s.phase == kPhaseScan0 || s.phase == kPhaseScan) w = s.act_count;
-      else if (s.phase == kPhaseProc) w = s.curr & kWorkMask;
+      if (s.phase == kPhaseScan0 || s.phase == kPhaseScan) {
+        w = s.act_count;
+        if (w) atomicAdd(&s_scan, w);
+      } else if (s.phase == kPhaseProc) {
+        w = s.curr & kWorkMask;
+        atomicAdd(&s_proc, w);
+        atomicAdd(&s_edges, s.curr >> kWorkBits);
+      }
       if (s.phase != kPhaseDone) atomicAdd(&s_live, 1u);
     }
     unsigned long long total;
@@ -942,6 +960,9 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
     wpref[G] = carry;
     uint32_t done = was_done;
     if (!was_done) {
+      ctl->el_proc += s_proc;
+      ctl->el_scan += s_scan;
+      ctl->edges_proc += s_edges;
       ctl->total_work = carry;
       ctl->wave += 1;
       ctl->waves_run += 1;

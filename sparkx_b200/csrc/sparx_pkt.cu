@@ -324,6 +324,9 @@ struct UnionJob {
   uint32_t kmax = 0;
   uint32_t err = 0;
   float ms_orient = 0, ms_support = 0, ms_peel = 0, ms_finalize = 0;
+  uint32_t launches = 0;
+  unsigned long long support_elements = 0;
+  Control ctl{};
 };
 
 template <class T>
@@ -400,8 +403,10 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   // -- orientation (Kernel B) --
   k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err);
   exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
+  J.launches += 4;
   CU(cudaMemcpyAsync(dmem, J.members.data(), sizeof(Member) * G, cudaMemcpyHostToDevice, s));
   k_member_edges<<<grid_for(G, 256, 1024), 256, 0, s>>>(dmem, G, opos);
+  J.launches += 1;
   CU(cudaMemcpyAsync(J.members.data(), dmem, sizeof(Member) * G, cudaMemcpyDeviceToHost, s));
   Counters hc;
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
@@ -416,6 +421,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     if (M.m > kEidMask) { set_error("a graph has >= 2^28 edges"); return SPARX_E_TOO_LARGE; }
   k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, eid);
   k_orient_reverse<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, eid, err);
+  J.launches += 2;
   CU(cudaEventRecord(E.tev[2], s));
 
   // -- support (Kernel C) --
@@ -425,12 +431,15 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, at<unsigned long long>(E, L.tiles),
                                        &cnt->grand, s);
     k_support_balanced<<<E.sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, sup, &cnt->tri);
+    J.launches += 4;
+    CU(cudaMemcpyAsync(&J.support_elements, spref + m, 8, cudaMemcpyDeviceToHost, s));
   }
   CU(cudaEventRecord(E.tev[3], s));
 
   if (J.support_only) {
     k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(eid, sup, W, J.support_out,
                                                                        O.support_mode == SPARX_SUPPORT_U8);
+    J.launches += 1;
     CU(cudaEventRecord(E.tev[4], s));
     CU(cudaEventRecord(E.tev[5], s));
   } else {
@@ -467,6 +476,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
                                                                      at<uint32_t>(E, L.mem_maxsup));
     k_peel_init<<<1, 1024, 0, s>>>(dmem, at<MemberState>(E, L.st), at<Control>(E, L.ctl),
                                    at<unsigned long long>(E, L.wpref), G);
+    J.launches += m > 0 ? 2 : 1;
     CU(cudaEventRecord(E.tev[4], s));
     if (O.loop == SPARX_LOOP_GRAPH) {
       int rc = build_peel_graph(E, J, s);
@@ -501,6 +511,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
         k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(eid, sup, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err);
       else
         k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(eid, sup, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err);
+      J.launches += 1;
     }
   }
   CU(cudaEventRecord(E.tev[6], s));
@@ -512,11 +523,14 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaMemcpyAsync(J.states.data(), at<MemberState>(E, L.st), sizeof(MemberState) * G, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(J.mem_tri.data(), at<unsigned long long>(E, L.mem_tri), 8ull * G, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(J.mem_maxsup.data(), at<uint32_t>(E, L.mem_maxsup), 4ull * G, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&J.ctl, at<Control>(E, L.ctl), sizeof(Control), cudaMemcpyDeviceToHost, s));
   }
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   J.tri = hc.tri;
   J.kmax = hc.kmax;
+  // each WHILE-loop iteration is one wave kernel + one planner kernel
+  if (!J.support_only) J.launches += 2 * (uint32_t)std::max<unsigned long long>(J.ctl.waves_run, 1);
   J.err = hc.err;
   CU(cudaEventElapsedTime(&J.ms_orient, E.tev[1], E.tev[2]));
   CU(cudaEventElapsedTime(&J.ms_support, E.tev[2], E.tev[3]));
@@ -542,6 +556,14 @@ void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
     st->k_max = M.w ? J.states[g].max_level + 2 : 0;
   }
   if (J.members.size() == 1 && J.support_only) st->triangles = J.tri;
+  st->launches = J.launches;
+  st->support_elements = J.support_elements;
+  if (J.members.size() == 1) {
+    st->peel_elements = J.ctl.el_proc;
+    st->peel_hits = J.ctl.hits;
+    st->peel_scanned = J.ctl.el_scan;
+    st->peel_edges = J.ctl.edges_proc;
+  }
   st->ms_orient = J.ms_orient;
   st->ms_support = J.ms_support;
   st->ms_peel = J.ms_peel;
@@ -614,6 +636,8 @@ int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int b
   if (bad_host) { set_error("offsets: first must be 0, last must equal width, non-decreasing"); return SPARX_E_INVALID_CSR; }
   rc = upload_ids(E, nbrs, bits, width, (uint32_t*)J.nbr, n, 0, s, stage, &cnt->err);
   if (rc) return rc;
+  J.launches += (uint32_t)((n_plus_1 + kStageBytes / 8 - 1) / (kStageBytes / 8)) +
+                (uint32_t)((width + kStageBytes / (bits / 8) - 1) / (kStageBytes / (bits / 8)));
   auto t_up_host = std::chrono::steady_clock::now();
   (void)t_up_host;
   rc = run_union(E, J, O, s);
@@ -637,9 +661,238 @@ int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int b
   return SPARX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batched decomposition: independent graphs packed into unions.
+
+struct HostMember {
+  const uint64_t* off = nullptr;
+  uint64_t n = 0;
+  const void* nbr = nullptr;
+  int bits = 64;
+  uint64_t w = 0;
+  void* out = nullptr;
+  uint64_t index = 0;
+};
+
+inline uint64_t host_id(const HostMember& h, uint64_t i) {
+  return h.bits == 64 ? ((const uint64_t*)h.nbr)[i] : ((const uint32_t*)h.nbr)[i];
+}
+
+// Host checks that need no device: offsets run from 0 to width without
+// decreasing, ids < n.  Row order, duplicates and symmetry are checked on the
+// device during orientation.
+int host_validate(const HostMember& h) {
+  if (h.off[0] != 0 || h.off[h.n] != h.w) return SPARX_E_INVALID_CSR;
+  for (uint64_t v = 0; v < h.n; ++v)
+    if (h.off[v + 1] < h.off[v]) return SPARX_E_INVALID_CSR;
+  bool bad = false;
+  if (h.w > (1u << 20)) {
+#pragma omp parallel for schedule(static) reduction(|| : bad)
+    for (long long i = 0; i < (long long)h.w; ++i) bad = bad || host_id(h, (uint64_t)i) >= h.n;
+  } else {
+    for (uint64_t i = 0; i < h.w && !bad; ++i) bad = host_id(h, i) >= h.n;
+  }
+  return bad ? SPARX_E_INVALID_CSR : SPARX_OK;
+}
+
+// Stream a union's u32 offsets and ids to the device through the pinned
+// staging buffers: host threads narrow and shift each member's arrays into a
+// chunk, which is then copied straight to its final place in HBM.
+int upload_union(Engine& E, const std::vector<HostMember>& hm, const std::vector<Member>& mem, uint64_t N,
+                 uint64_t W, uint32_t* d_off, uint32_t* d_nbr, cudaStream_t s) {
+  const uint64_t chunk = kStageBytes / 4;
+  for (int pass = 0; pass < 2; ++pass) {
+    const uint64_t total = pass == 0 ? N + 1 : W;
+    uint32_t* dst = pass == 0 ? d_off : d_nbr;
+    size_t g0 = 0;  // first member that can overlap the chunk
+    for (uint64_t c = 0, a = 0; a < total; ++c, a += chunk) {
+      const int slot = (int)(c & 1);
+      const uint64_t b = std::min<uint64_t>(a + chunk, total);
+      CU(cudaEventSynchronize(E.pin_ev[slot]));
+      uint32_t* buf = (uint32_t*)E.pinned[slot];
+      auto lo_of = [&](const Member& M) -> uint64_t { return pass == 0 ? M.vb : M.sb; };
+      auto len_of = [&](const Member& M) -> uint64_t { return pass == 0 ? M.n : M.w; };
+      while (g0 < mem.size() && lo_of(mem[g0]) + len_of(mem[g0]) <= a) ++g0;
+      size_t g1 = g0;
+      while (g1 < mem.size() && lo_of(mem[g1]) < b) ++g1;
+#pragma omp parallel for schedule(dynamic, 1)
+      for (long long gi = (long long)g0; gi < (long long)g1; ++gi) {
+        const Member& M = mem[gi];
+        const HostMember& H = hm[gi];
+        const uint64_t lo = std::max<uint64_t>(a, lo_of(M)), hi = std::min<uint64_t>(b, lo_of(M) + len_of(M));
+        if (pass == 0) {
+          for (uint64_t x = lo; x < hi; ++x) buf[x - a] = (uint32_t)(H.off[x - M.vb] + M.sb);
+        } else if (H.bits == 64) {
+          const uint64_t* src = (const uint64_t*)H.nbr;
+          for (uint64_t x = lo; x < hi; ++x) buf[x - a] = (uint32_t)src[x - M.sb] + M.vb;
+        } else {
+          const uint32_t* src = (const uint32_t*)H.nbr;
+          for (uint64_t x = lo; x < hi; ++x) buf[x - a] = src[x - M.sb] + M.vb;
+        }
+      }
+      if (pass == 0 && b == total) buf[total - 1 - a] = (uint32_t)W;  // the closing offset
+      CU(cudaMemcpyAsync(dst + a, buf, (b - a) * 4, cudaMemcpyHostToDevice, s));
+      CU(cudaEventRecord(E.pin_ev[slot], s));
+    }
+  }
+  return SPARX_OK;
+}
+
+// Decompose one union of validated members; on a device-detected input error
+// the members are re-run one by one to attribute the status.
+int run_batch_union(Engine& E, std::vector<HostMember>& hm, const Opts& O, int* status_out,
+                    sparx_pkt_stats* stats_out, int* first_fail) {
+  const size_t G = hm.size();
+  UnionJob J;
+  uint64_t N = 0, Wt = 0;
+  for (const HostMember& h : hm) {
+    J.members.push_back(Member{(uint32_t)N, (uint32_t)h.n, (uint32_t)Wt, (uint32_t)h.w, 0, 0});
+    N += h.n;
+    Wt += h.w;
+  }
+  J.N = N;
+  J.W = Wt;
+  const size_t out_bytes = (O.out_bits / 8) * Wt;
+  J.L = make_layout(N, Wt, (uint32_t)G, true, out_bytes);
+  int rc = ensure_ws(E, J.L.total);
+  auto fail_all = [&](int code) {
+    for (size_t g = 0; g < G; ++g) {
+      if (status_out) status_out[hm[g].index] = code;
+      if (!*first_fail) *first_fail = code;
+    }
+  };
+  if (rc) { fail_all(rc); return rc; }
+  cudaStream_t s = E.stream;
+  J.off = at<uint32_t>(E, J.L.off);
+  J.nbr = at<uint32_t>(E, J.L.nbr);
+  J.out = at<void>(E, J.L.out);
+  Counters* cnt = at<Counters>(E, J.L.cnt);
+  auto t0 = std::chrono::steady_clock::now();
+  CU(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
+  CU(cudaEventRecord(E.tev[0], s));
+  rc = upload_union(E, hm, J.members, N, Wt, J.off, (uint32_t*)J.nbr, s);
+  if (rc) { fail_all(rc); return rc; }
+  J.launches += 0;
+  rc = run_union(E, J, O, s);
+  if (rc == SPARX_E_INVALID_CSR || rc == SPARX_E_MULTIGRAPH || rc == SPARX_E_OVERFLOW_U8 ||
+      rc == SPARX_E_TOO_LARGE) {
+    if (G == 1) {
+      fill_stats(J, 0, stats_out ? stats_out + hm[0].index : nullptr);
+      if (status_out) status_out[hm[0].index] = rc;
+      if (!*first_fail) *first_fail = rc;
+      return rc;
+    }
+    // attribute: one member at a time
+    for (size_t g = 0; g < G; ++g) {
+      std::vector<HostMember> one{hm[g]};
+      run_batch_union(E, one, O, status_out, stats_out, first_fail);
+    }
+    return SPARX_OK;
+  }
+  if (rc) { fail_all(rc); return rc; }
+  const size_t esz = O.out_bits / 8;
+  // download the union's truss numbers, then hand each member its slot range
+  std::vector<uint8_t> host_out;
+  void* dst_all = nullptr;
+  if (G == 1) dst_all = hm[0].out;
+  else { host_out.resize(out_bytes); dst_all = host_out.data(); }
+  rc = download(E, dst_all, J.out, out_bytes, s);
+  if (rc) { fail_all(rc); return rc; }
+  CU(cudaStreamSynchronize(s));
+  if (G > 1) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long g = 0; g < (long long)G; ++g)
+      std::memcpy(hm[g].out, host_out.data() + (size_t)J.members[g].sb * esz, (size_t)J.members[g].w * esz);
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  const double total_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  for (size_t g = 0; g < G; ++g) {
+    if (status_out) status_out[hm[g].index] = SPARX_OK;
+    if (stats_out) {
+      fill_stats(J, (uint32_t)g, stats_out + hm[g].index);
+      stats_out[hm[g].index].ms_total = total_ms;  // the union's wall time, shared by its members
+    }
+  }
+  return SPARX_OK;
+}
+
+int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, const sparx_pkt_opts* opts,
+              int* status_out, sparx_pkt_stats* stats_out) {
+  g_last_error.clear();
+  if (!graphs && count) { set_error("null graph list"); return SPARX_E_ARG; }
+  Opts O;
+  int rc = read_opts(opts, &O);
+  if (rc) return rc;
+  Engine* Ep;
+  rc = get_engine(O.device, &Ep);
+  if (rc) return rc;
+  Engine& E = *Ep;
+  std::lock_guard<std::mutex> lk(E.mu);
+  CU(cudaSetDevice(E.device));
+  if (!budget) budget = 150ull << 30;
+  if (stats_out) std::memset(stats_out, 0, sizeof(sparx_pkt_stats) * count);
+  int first_fail = SPARX_OK;
+  // host validation, then greedy packing in input order
+  std::vector<HostMember> valid;
+  valid.reserve(count);
+  for (uint64_t i = 0; i < count; ++i) {
+    const sparx_graph_view& v = graphs[i];
+    HostMember h;
+    h.off = v.offsets;
+    h.n = v.n_plus_1 ? v.n_plus_1 - 1 : 0;
+    h.nbr = v.neighbours;
+    h.bits = v.neighbour_bits == 32 ? 32 : 64;
+    h.w = v.width;
+    h.out = v.truss_out;
+    h.index = i;
+    int st = SPARX_OK;
+    if (!v.offsets || v.n_plus_1 < 1 || (v.width && (!v.neighbours || !v.truss_out)) ||
+        (v.neighbour_bits != 32 && v.neighbour_bits != 64))
+      st = SPARX_E_ARG;
+    else if ((st = check_dims(v.n_plus_1, v.width)) == SPARX_OK)
+      st = host_validate(h);
+    if (st == SPARX_OK && h.w / 2 > kEidMask) st = SPARX_E_TOO_LARGE;
+    if (status_out) status_out[i] = st;
+    if (st != SPARX_OK) {
+      if (!first_fail) first_fail = st;
+      continue;
+    }
+    valid.push_back(h);
+  }
+  size_t at_i = 0;
+  while (at_i < valid.size()) {
+    std::vector<HostMember> wave;
+    uint64_t N = 0, Wt = 0;
+    while (at_i < valid.size()) {
+      const HostMember& h = valid[at_i];
+      const uint64_t N2 = N + h.n, W2 = Wt + h.w;
+      const size_t bytes = make_layout(N2, W2, (uint32_t)wave.size() + 1, true, (O.out_bits / 8) * W2).total;
+      const bool fits = N2 < 0xFFFFFFFFull && W2 < 0xFFFFFFFFull && bytes <= budget && wave.size() < 65536;
+      if (!fits && !wave.empty()) break;
+      if (!fits) {  // a single graph over the budget
+        if (status_out) status_out[h.index] = SPARX_E_OOM;
+        if (!first_fail) first_fail = SPARX_E_OOM;
+        ++at_i;
+        continue;
+      }
+      wave.push_back(h);
+      N = N2;
+      Wt = W2;
+      ++at_i;
+    }
+    if (!wave.empty()) run_batch_union(E, wave, O, status_out, stats_out, &first_fail);
+  }
+  return first_fail;
+}
+
 }  // namespace
 
 extern "C" {
+
+int sparx_pkt_run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
+                        const sparx_pkt_opts* opts, int* status_out, sparx_pkt_stats* stats_out) {
+  return run_batch(graphs, count, hbm_budget_bytes, opts, status_out, stats_out);
+}
 
 int sparx_pkt_default_opts(sparx_pkt_opts* o) {
   if (!o) return SPARX_E_ARG;
@@ -724,6 +977,7 @@ int sparx_pkt_run_device(const uint64_t* d_offsets, uint64_t n_plus_1, const uin
   if (width)
     k_range_ids<<<grid_for(width, 256, E.sm_count * 16), 256, 0, s>>>(d_neighbours, nullptr, width, (uint32_t)n, 0u,
                                                                        &cnt->err);
+  J.launches += width ? 2 : 1;
   rc = run_union(E, J, O, s);
   fill_stats(J, 0, stats);
   if (rc) return rc;

@@ -64,11 +64,14 @@ class _Stats(ctypes.Structure):
         ("n", ctypes.c_uint64), ("width", ctypes.c_uint64), ("m", ctypes.c_uint64),
         ("self_loops", ctypes.c_uint64), ("triangles", ctypes.c_uint64),
         ("max_support", ctypes.c_uint64), ("k_max", ctypes.c_uint32), ("levels", ctypes.c_uint32),
-        ("waves", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+        ("waves", ctypes.c_uint32), ("launches", ctypes.c_uint32),
         ("ms_upload", ctypes.c_double), ("ms_orient", ctypes.c_double),
         ("ms_support", ctypes.c_double), ("ms_peel", ctypes.c_double),
         ("ms_finalize", ctypes.c_double), ("ms_download", ctypes.c_double),
         ("ms_total", ctypes.c_double),
+        ("support_elements", ctypes.c_uint64), ("peel_elements", ctypes.c_uint64),
+        ("peel_hits", ctypes.c_uint64), ("peel_scanned", ctypes.c_uint64),
+        ("peel_edges", ctypes.c_uint64),
     ]
 
 
@@ -154,6 +157,7 @@ class PktStats:
     k_max: int = 0
     levels: int = 0
     waves: int = 0
+    launches: int = 0
     ms_upload: float = 0.0
     ms_orient: float = 0.0
     ms_support: float = 0.0
@@ -161,6 +165,11 @@ class PktStats:
     ms_finalize: float = 0.0
     ms_download: float = 0.0
     ms_total: float = 0.0
+    support_elements: int = 0
+    peel_elements: int = 0
+    peel_hits: int = 0
+    peel_scanned: int = 0
+    peel_edges: int = 0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "PktStats":
@@ -289,3 +298,47 @@ class Triangles:
 
     def all_triangles(self) -> np.ndarray:
         return self._support
+
+
+def run_pkt_device(d_offsets: int, n_plus_1: int, d_neighbours: int, width: int, d_out: int,
+                   opts: PktOptions | None = None, stream: int = 0) -> PktStats:
+    """Device-resident run: raw device pointers (u64 offsets, u32 ids, output per
+    ``opts.out_bits``) on ``stream`` (a cudaStream_t as int, 0 = library stream)."""
+    opts = opts or PktOptions()
+    st = _Stats()
+    o = opts.c()
+    _check(lib().sparx_pkt_run_device(d_offsets, n_plus_1, d_neighbours, width, d_out,
+                                      ctypes.byref(o), ctypes.byref(st), stream or None))
+    return PktStats.from_c(st)
+
+
+def run_batch(graphs, opts: PktOptions | None = None, hbm_budget_bytes: int = 0):
+    """Decompose many independent graphs with ``sparx_pkt_run_batch``.
+
+    ``graphs``: sequence of (offsets u64[n+1], neighbours u64|u32[width]).
+    Returns a list of (truss, PktStats, status) in input order; a failing graph
+    gets ``truss=None`` and its status (the others still complete)."""
+    opts = opts or PktOptions()
+    views = (_GraphView * max(1, len(graphs)))()
+    keep, outs = [], []
+    for i, (off, nbr) in enumerate(graphs):
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        nbr = np.ascontiguousarray(nbr)
+        if nbr.dtype not in (np.uint64, np.uint32):
+            nbr = nbr.astype(np.uint64)
+        out = np.empty(nbr.shape[0], dtype=np.uint8 if opts.out_bits == 8 else np.uint32)
+        keep += [off, nbr]
+        outs.append(out)
+        v = views[i]
+        v.offsets = off.ctypes.data
+        v.n_plus_1 = off.shape[0]
+        v.neighbours = nbr.ctypes.data
+        v.width = nbr.shape[0]
+        v.neighbour_bits = 64 if nbr.dtype == np.uint64 else 32
+        v.truss_out = out.ctypes.data
+    n = len(graphs)
+    status = (ctypes.c_int * max(1, n))()
+    stats = (_Stats * max(1, n))()
+    o = opts.c()
+    lib().sparx_pkt_run_batch(views, n, hbm_budget_bytes, ctypes.byref(o), status, stats)
+    return [(outs[i] if status[i] == OK else None, PktStats.from_c(stats[i]), int(status[i])) for i in range(n)]

@@ -1,0 +1,157 @@
+"""The CPU oracle (restatements of the reference's PKT path) against hand-derived
+known answers, a brute-force definition and each other."""
+import numpy as np
+import pytest
+
+from conftest import book, expected_truss, kats, kn, random_graph
+from oracle import oracle as O
+from sparkx_b200 import gen
+
+
+def all_oracles(g, mode=O.MODE_WIDE):
+    off, nbr = g.offsets, g.neighbours
+    return {
+        "pkt_t1": O.pkt(off, nbr, mode=mode, threads=1),
+        "pkt_t3": O.pkt(off, nbr, mode=mode, threads=3),
+        "pkt_hash": O.pkt(off, nbr, mode=mode, threads=2, hash_map=True),
+        "burkhardt": O.burkhardt(off, nbr, mode=mode),
+        "fast": O.fast_truss(off, nbr, mode=mode, threads=2)[0],
+    }
+
+
+@pytest.mark.parametrize("name,n,edges,special,default", kats(), ids=[k[0] for k in kats()])
+def test_known_answers(name, n, edges, special, default):
+    g = gen.from_edges(n, edges)
+    exp = expected_truss(g, special, default)
+    for impl, t in all_oracles(g).items():
+        assert np.array_equal(t, exp), (name, impl, t, exp)
+    assert np.array_equal(O.brute_force_truss(g.offsets, g.neighbours), exp)
+    assert O.verify(g.offsets, g.neighbours, exp) == -1
+
+
+def test_random_graphs_agree_with_definition():
+    rng = np.random.default_rng(7)
+    for _ in range(120):
+        g = random_graph(rng)
+        bf = O.brute_force_truss(g.offsets, g.neighbours)
+        for impl, t in all_oracles(g).items():
+            assert np.array_equal(t, bf), impl
+        assert O.verify(g.offsets, g.neighbours, bf) == -1
+
+
+def test_triangles_per_slot_match_definition():
+    rng = np.random.default_rng(3)
+    for _ in range(40):
+        g = random_graph(rng)
+        sup = O.triangles(g.offsets, g.neighbours)
+        off = g.offsets.astype(np.int64)
+        nb = [set(int(x) for x in g.neighbours[off[u]:off[u + 1]]) - {u} for u in range(g.n)]
+        for u in range(g.n):
+            for s in range(off[u], off[u + 1]):
+                v = int(g.neighbours[s])
+                want = 0 if v == u else len(nb[u] & nb[v])
+                assert sup[s] == want
+
+
+def test_edge_index_reciprocals():
+    g = gen.rmat(10, 8, seed=5)
+    eo, er = O.edge_index(g.offsets, g.neighbours, threads=3)
+    off = g.offsets.astype(np.int64)
+    for u in range(g.n):
+        row = g.neighbours[off[u]:off[u + 1]]
+        assert eo[u] == off[u] + int(np.searchsorted(row, u, side="right"))
+    src = np.repeat(np.arange(g.n), np.diff(off))
+    assert np.array_equal(er[er], np.arange(g.width))
+    assert np.array_equal(g.neighbours[er], src.astype(np.uint32))
+
+
+def test_verify_rejects_wrong_assignments():
+    g = kn(5)
+    good = np.full(g.width, 5, dtype=np.uint32)
+    assert O.verify(g.offsets, g.neighbours, good) == -1
+    bad = good.copy()
+    bad[3] = 4  # asymmetric
+    assert O.verify(g.offsets, g.neighbours, bad) >= 0
+    assert O.verify(g.offsets, g.neighbours, np.full(g.width, 6, dtype=np.uint32)) >= 0
+
+
+def test_invalid_inputs_rejected():
+    off = np.array([0, 1, 3, 4, 4], dtype=np.uint64)
+    with pytest.raises(O.OracleError):
+        O.edge_index(off, np.array([1, 0, 2, 3], dtype=np.uint32))  # asymmetric
+    with pytest.raises(O.OracleError):
+        O.edge_index(np.array([0, 2, 3, 4], dtype=np.uint64), np.array([1, 1, 0, 0], dtype=np.uint32))
+    with pytest.raises(O.OracleError):
+        O.edge_index(np.array([0, 2, 4, 6], dtype=np.uint64), np.array([2, 1, 0, 2, 0, 1], dtype=np.uint32))
+
+
+def test_u8_mode_wraps_support_like_the_reference():
+    # spine support 256 wraps to 0: the reference marks it processed at level 0
+    # (truss 2) and never charges its triangles, so the pages keep truss 3
+    g = book(256)
+    sup = O.triangles(g.offsets, g.neighbours, mode=O.MODE_U8)
+    wide = O.triangles(g.offsets, g.neighbours)
+    assert wide.max() == 256 and sup.max() == 1
+    res = all_oracles(g, mode=O.MODE_U8)
+    spine = [s for s in range(g.width) if g.neighbours[s] in (0, 1) and s < g.offsets[2]]
+    for impl, t in res.items():
+        assert all(t[s] == 2 for s in spine if (s < g.offsets[1] and g.neighbours[s] == 1)
+                   or (s >= g.offsets[1] and g.neighbours[s] == 0)), impl
+    base = res["pkt_t1"]
+    for impl, t in res.items():
+        assert np.array_equal(t, base), impl
+    for impl, t in all_oracles(g).items():
+        assert (t == 3).all(), impl
+    # below 256 the two widths agree
+    g2 = book(200)
+    assert np.array_equal(O.pkt(g2.offsets, g2.neighbours, mode=O.MODE_U8),
+                          O.pkt(g2.offsets, g2.neighbours))
+
+
+def test_u8_level_overflow_is_an_error():
+    # K_257: support 255 everywhere -> level 255 -> the reference's u8 level
+    # counter overflows (pkt.rs:508-516)
+    g = kn(257)
+    with pytest.raises(O.OracleError):
+        O.pkt(g.offsets, g.neighbours, mode=O.MODE_U8, threads=4)
+    t = O.pkt(g.offsets, g.neighbours, threads=4)
+    assert (t == 257).all()
+
+
+def test_medium_graphs_three_way():
+    for g in (gen.erdos_renyi(3000, 30000, 11), gen.rmat(12, 16, seed=4), gen.debruijn(20000, 7, 20, 500, 0.05, 9)):
+        base = O.pkt(g.offsets, g.neighbours, threads=4)
+        assert np.array_equal(base, O.burkhardt(g.offsets, g.neighbours))
+        assert np.array_equal(base, O.fast_truss(g.offsets, g.neighbours, threads=4)[0])
+        assert O.verify(g.offsets, g.neighbours, base, threads=4) == -1
+
+
+@pytest.mark.parametrize("name", ["arr_rmat10", "arr_dbg_k6", "arr_er"])
+def test_oracle_against_committed_vectors(name):
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz"))
+    off, nbr = z["offsets"], z["neighbours"]
+    assert np.array_equal(O.pkt(off, nbr, threads=2), z["truss_mode0"])
+    assert np.array_equal(O.burkhardt(off, nbr), z["truss_mode0"])
+    assert np.array_equal(z["brute_force"], z["truss_mode0"])
+    if "truss_mode1" in z:
+        assert np.array_equal(O.pkt(off, nbr, mode=O.MODE_U8), z["truss_mode1"])
+
+
+def test_generators_reproduce_fixture_graphs():
+    import hashlib
+    import json
+    import os
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "fixtures.json")))
+    for name in ("rmat16", "cfg1_er_100k_1m", "dbg_small"):
+        p = fx[name]["params"]
+        if p["fn"] == "er":
+            g = gen.erdos_renyi(p["n"], p["m"], p["seed"])
+        elif p["fn"] == "rmat":
+            g = gen.rmat(p["scale"], p["ef"], seed=p["seed"])
+        else:
+            g = gen.debruijn(p["seq_len"], p["k"], p["copies"], p["seg_len"], p["mut_rate"], p["seed"])
+        h = hashlib.sha256()
+        h.update(np.ascontiguousarray(g.offsets, dtype="<u8").tobytes())
+        h.update(np.ascontiguousarray(g.neighbours, dtype="<u4").tobytes())
+        assert h.hexdigest() == fx[name]["csr_sha256"], name
