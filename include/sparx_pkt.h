@@ -118,6 +118,34 @@ int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64
                         uint64_t width, uint32_t* support_out, const sparx_pkt_opts* opts,
                         sparx_pkt_stats* stats);
 
+/*
+ * Allocation-free PKT decomposition of one graph in DEVICE memory.  No
+ * counterpart in the reference.
+ *
+ * For callers that must not allocate device memory when they ask for a
+ * decomposition: code running while a stream is captured into a CUDA graph in
+ * global or thread-local mode (cudaMalloc is not permitted there), services
+ * whose device memory is reserved up front by their own pool, and
+ * latency-critical paths that cannot wait for or fail on cudaMalloc.  All
+ * scratch lives in one fixed file-scope device array of
+ * SPARX_NOALLOC_SCRATCH_BYTES per device (present on every GPU that loads the
+ * library, until exit); graphs needing more get SPARX_E_TOO_LARGE (roughly
+ * 2.5 M CSR slots).  The call allocates no device or pinned memory, streams or
+ * events.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture begins.  All
+ * calls on a device share the array and it keeps the previous call's
+ * contents: calls that overlap on the GPU (other streams, other host
+ * threads) race and corrupt each other; serialize them.  The peel runs as
+ * host-launched waves on `cuda_stream` and the call returns when the stream
+ * has finished.
+ *   d_offsets u64[n_plus_1], d_neighbours u32[width], d_truss_out u32[width]
+ *   device: CUDA ordinal (-1 = current)
+ */
+#define SPARX_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int sparx_pkt_run_device_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1,
+                                 const uint32_t* d_neighbours, uint64_t width, uint32_t* d_truss_out,
+                                 int device, void* cuda_stream);
+
 /* ---- batched decomposition -------------------------------------------- */
 /* One member of a batch: host arrays in the reference's layout (u64 ids) or
  * u32 ids (neighbour_bits 32).  truss_out follows opts->out_bits. */

@@ -992,3 +992,221 @@ int sparx_pkt_run_device(const uint64_t* d_offsets, uint64_t n_plus_1, const uin
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point (no counterpart in the reference).
+//
+// Some callers cannot allocate device memory at the moment they need a
+// decomposition: code that runs while a CUDA stream is being captured into a
+// graph in global or thread-local capture mode (cudaMalloc is not permitted
+// then), services that reserve all device memory up front through their own
+// pool and treat any allocation outside it as a fault, and latency-critical
+// request paths that must neither wait for nor fail on cudaMalloc.  For them
+// this variant of the single-graph pipeline keeps every scratch array in one
+// fixed, file-scope device array instead of the engine's workspace.  It
+// allocates nothing (device or pinned host memory, streams or events): the
+// caller passes device inputs and the device output, and a stream.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // per device; bounds the graph size below
+
+// Lives in every GPU that loads this library, until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+constexpr int kMaxDevices = 64;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of the scratch array for `device` (which must be current).
+// Host code cannot use the symbol itself as a device pointer, so the address is
+// looked up once per device and cached.
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kMaxDevices) {
+    set_error("device ordinal out of range");
+    return SPARX_E_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+      return SPARX_E_CUDA;
+    }
+    g_noalloc_addr[device] = p;
+  }
+  *out = (unsigned char*)g_noalloc_addr[device];
+  return SPARX_OK;
+}
+
+// The same arrays as the engine's workspace, minus staging and output.
+Layout make_noalloc_layout(uint64_t N, uint64_t W) {
+  Layout L{};
+  size_t p = 0;
+  auto take = [&](size_t bytes) {
+    size_t r = p;
+    p = align_up(p + std::max<size_t>(bytes, 1));
+    return r;
+  };
+  const uint64_t M = std::max<uint64_t>(W / 2, 1);
+  L.off = take(4 * (N + 1));
+  L.eid = take(4 * W);
+  L.dplus = take(4 * N);
+  L.opos = take(4 * (N + 1));
+  L.ocol = take(4 * M);
+  L.osrc = take(4 * M);
+  L.sup = take(4 * M);
+  L.tag = take(4 * M);
+  L.act0 = take(4 * M);
+  L.act1 = take(4 * M);
+  L.q0 = take(16 * M + 16);
+  L.q1 = L.q0 + 8 * M;
+  const uint64_t tiles = (std::max<uint64_t>(N + 1, M + 1) + kScanTile - 1) / kScanTile + 2;
+  L.tiles = take(8 * tiles);
+  L.ctl = take(sizeof(Control));
+  L.mem = take(sizeof(Member));
+  L.st = take(sizeof(MemberState));
+  L.wpref = take(16);
+  L.cnt = take(sizeof(Counters));
+  L.mem_tri = take(8);
+  L.mem_maxsup = take(4);
+  L.uni = take(sizeof(Union));
+  L.total = p;
+  return L;
+}
+
+int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_nbr, uint64_t width,
+                uint32_t* d_out, int device, cudaStream_t s) {
+  g_last_error.clear();
+  if (!d_offsets || (width && (!d_nbr || !d_out))) { set_error("null pointer"); return SPARX_E_ARG; }
+  int rc = check_dims(n_plus_1, width);
+  if (rc) return rc;
+  if (device < 0) CU(cudaGetDevice(&device));
+  CU(cudaSetDevice(device));
+  unsigned char* base = nullptr;
+  rc = noalloc_scratch(device, &base);
+  if (rc) return rc;
+  const uint64_t n = n_plus_1 - 1;
+  const Layout L = make_noalloc_layout(n, width);
+  if (L.total > kNoAllocScratchBytes) {
+    set_error("graph needs " + std::to_string(L.total) + " bytes of scratch; the allocation-free entry point has " +
+              std::to_string(kNoAllocScratchBytes) + " (about 2.5 M CSR slots); use sparx_pkt_run_device");
+    return SPARX_E_TOO_LARGE;
+  }
+  auto P = [&](size_t off) { return base + off; };
+  uint32_t* off = (uint32_t*)P(L.off);
+  uint32_t* eid = (uint32_t*)P(L.eid);
+  uint32_t* dplus = (uint32_t*)P(L.dplus);
+  uint32_t* opos = (uint32_t*)P(L.opos);
+  uint32_t* ocol = (uint32_t*)P(L.ocol);
+  uint32_t* osrc = (uint32_t*)P(L.osrc);
+  int32_t* sup = (int32_t*)P(L.sup);
+  Counters* cnt = (Counters*)P(L.cnt);
+  uint32_t* err = &cnt->err;
+  int sm = 148, per_sm = 1;
+  CU(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave, 256, 0));
+  const int wave_blocks = std::max(1, per_sm) * sm;
+  const uint32_t N = (uint32_t)n;
+
+  // the array keeps the previous call's contents: reset what must start at zero
+  CU(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
+  k_narrow_offsets<<<grid_for(n_plus_1, 256, sm * 16), 256, 0, s>>>((const unsigned long long*)d_offsets, off,
+                                                                    (uint32_t)n_plus_1, 0u, 0ll, (long long)width, err);
+  if (width) k_range_ids<<<grid_for(width, 256, sm * 16), 256, 0, s>>>(d_nbr, nullptr, width, N, 0u, err);
+  Counters hc;
+  CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (hc.err) return status_from_flags(hc.err);
+
+  const int vgrid = grid_for((unsigned long long)N * 32, 256, sm * 32);
+  k_orient_count<<<vgrid, 256, 0, s>>>(off, d_nbr, N, dplus, &cnt->self_loops, err);
+  exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, (uint32_t*)P(L.tiles), (uint32_t*)&cnt->grand, s);
+  uint32_t m32 = 0;
+  CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (hc.err) return status_from_flags(hc.err);
+  const uint64_t m = m32;
+  if (2 * m + hc.self_loops != width) return SPARX_E_INVALID_CSR;
+  if (m > kEidMask) return SPARX_E_TOO_LARGE;
+  k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, eid);
+  k_orient_reverse<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, eid, err);
+
+  CU(cudaMemsetAsync(sup, 0, 4 * std::max<uint64_t>(m, 1), s));
+  unsigned long long* spref = (unsigned long long*)P(L.q0);
+  if (m > 0) {
+    exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, (unsigned long long*)P(L.tiles),
+                                       &cnt->grand, s);
+    k_support_balanced<<<sm * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, sup, &cnt->tri);
+  }
+
+  Union U;
+  U.off = off;
+  U.nbr = d_nbr;
+  U.eid = eid;
+  U.opos = opos;
+  U.ocol = ocol;
+  U.osrc = osrc;
+  U.sup = sup;
+  U.tag = (uint32_t*)P(L.tag);
+  U.act[0] = (uint32_t*)P(L.act0);
+  U.act[1] = (uint32_t*)P(L.act1);
+  U.q[0] = (unsigned long long*)P(L.q0);
+  U.q[1] = (unsigned long long*)P(L.q1);
+  U.n = N;
+  U.m = (uint32_t)m;
+  U.width = (uint32_t)width;
+  U.G = 1;
+  const Member M0{0, N, 0, (uint32_t)width, 0, (uint32_t)m};
+  Control c0{};
+  c0.G = 1;
+  c0.max_waves = 2ull * m + 64;
+  c0.timeout_ns = kDefaultTimeoutMs * 1000000ull;
+  Union* dU = (Union*)P(L.uni);
+  Member* dM = (Member*)P(L.mem);
+  Control* dC = (Control*)P(L.ctl);
+  MemberState* dS = (MemberState*)P(L.st);
+  unsigned long long* wpref = (unsigned long long*)P(L.wpref);
+  // pageable sources: the copies are staged before these calls return
+  CU(cudaMemcpyAsync(dU, &U, sizeof(Union), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(dM, &M0, sizeof(Member), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(dC, &c0, sizeof(Control), cudaMemcpyHostToDevice, s));
+  CU(cudaMemsetAsync(P(L.mem_tri), 0, 8, s));
+  CU(cudaMemsetAsync(P(L.mem_maxsup), 0, 4, s));
+  if (m > 0)
+    k_peel_setup<<<grid_for(m, 256, sm * 8), 256, 0, s>>>(dU, dM, 0, (unsigned long long*)P(L.mem_tri),
+                                                           (uint32_t*)P(L.mem_maxsup));
+  k_peel_init<<<1, 1024, 0, s>>>(dM, dS, dC, wpref, 1);
+  WaveArgs wa;
+  wa.Up = dU;
+  wa.mem = dM;
+  wa.st = dS;
+  wa.ctl = dC;
+  wa.wpref = wpref;
+  wa.err = err;
+  for (;;) {
+    for (int i = 0; i < 16; ++i) {
+      k_wave<<<wave_blocks, 256, 0, s>>>(wa);
+      k_plan<<<1, 1024, 0, s>>>(dM, dS, dC, wpref, err, cudaGraphConditionalHandle{}, 0);
+    }
+    uint32_t done = 0;
+    CU(cudaMemcpyAsync(&done, &dC->done, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (done) break;
+  }
+  if (width)
+    k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(eid, sup, width, d_out, 0, 0, &cnt->kmax, err);
+  CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  CU(cudaGetLastError());
+  return status_from_flags(hc.err);
+}
+
+}  // namespace
+
+extern "C" int sparx_pkt_run_device_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1,
+                                            const uint32_t* d_neighbours, uint64_t width, uint32_t* d_truss_out,
+                                            int device, void* cuda_stream) {
+  return run_noalloc(d_offsets, n_plus_1, d_neighbours, width, d_truss_out, device, (cudaStream_t)cuda_stream);
+}

@@ -87,6 +87,7 @@ class _GraphView(ctypes.Structure):
 EXPORTS = [
     "sparx_pkt_default_opts", "sparx_strerror", "sparx_last_error", "sparx_pkt_run",
     "sparx_pkt_run_u32", "sparx_pkt_run_device", "sparx_triangles_run", "sparx_pkt_run_batch",
+    "sparx_pkt_run_device_noalloc",
     "sparx_server_create", "sparx_server_submit", "sparx_server_poll", "sparx_server_wait",
     "sparx_server_cancel", "sparx_server_destroy",
 ]
@@ -110,6 +111,9 @@ def lib():
         f.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats)]
     L.sparx_pkt_run_device.restype = i32
     L.sparx_pkt_run_device.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats), vp]
+    if hasattr(L, "sparx_pkt_run_device_noalloc"):
+        L.sparx_pkt_run_device_noalloc.restype = i32
+        L.sparx_pkt_run_device_noalloc.argtypes = [vp, u64, vp, u64, vp, ctypes.c_int, vp]
     if hasattr(L, "sparx_pkt_run_batch"):
         L.sparx_pkt_run_batch.restype = i32
         L.sparx_pkt_run_batch.argtypes = [P(_GraphView), u64, u64, P(_Opts), P(ctypes.c_int), P(_Stats)]
@@ -342,3 +346,12 @@ def run_batch(graphs, opts: PktOptions | None = None, hbm_budget_bytes: int = 0)
     o = opts.c()
     lib().sparx_pkt_run_batch(views, n, hbm_budget_bytes, ctypes.byref(o), status, stats)
     return [(outs[i] if status[i] == OK else None, PktStats.from_c(stats[i]), int(status[i])) for i in range(n)]
+
+
+def run_pkt_device_noalloc(d_offsets: int, n_plus_1: int, d_neighbours: int, width: int, d_out: int,
+                           device: int = -1, stream: int = 0) -> None:
+    """Allocation-free variant (``sparx_pkt_run_device_noalloc``): u32 truss per
+    slot into ``d_out``; scratch is the library's fixed per-device array, so the
+    graph must fit it and calls must not overlap on the GPU."""
+    _check(lib().sparx_pkt_run_device_noalloc(d_offsets, n_plus_1, d_neighbours, width, d_out, device,
+                                              stream or None))
