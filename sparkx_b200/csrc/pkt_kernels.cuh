@@ -7,9 +7,10 @@
 // frontier, and one device "wave" advances every member by one step (a level
 // scan or one PKT sub-level).  A single graph is a union of one.
 //
-// Layout in HBM (u32 everywhere: width < 2^32, m < 2^28 per member):
+// Layout in HBM (u32 indices: width < 2^32, m < 2^28 per member):
 //   off[n+1], nbr[width]        narrowed CSR, rows sorted ascending
-//   eid[width]                  slot -> undirected edge id (0xFFFFFFFF: self-loop)
+//   row0[width] (u64)           the same rows as (id | edge id << 32) pairs, in
+//                               slot order (edge id 0xFFFFFFFF: self-loop)
 //   dplus[n], opos[n+1]         degree-ordered out-degree and its prefix
 //   ocol[m], osrc[m]            oriented edge e = (osrc[e] -> ocol[e]); e is the
 //                               undirected edge id; rank(osrc) < rank(ocol)
@@ -17,6 +18,9 @@
 //                               edge is processed (0xFFFFFFFF: not yet queued)
 //   act[2][m], q[2][m] (u64)    per-member active lists and frontier queues,
 //                               segment [eb_g, eb_g + m_g) for member g
+//   working CSR (off, row)      the peel's view: row0 at first, then rebuilt
+//                               without processed edges whenever the live
+//                               edges halve (two ping-pong buffers)
 #pragma once
 
 #include <cstdint>
@@ -47,10 +51,9 @@ enum : uint32_t {
 
 enum : uint32_t { kPhaseScan0 = 0, kPhaseScan = 1, kPhaseProc = 2, kPhaseDone = 3 };
 
-struct Union {  // the prepared concatenated graph
-  const uint32_t* off;
-  const uint32_t* nbr;
-  const uint32_t* eid;
+struct Union {  // the prepared concatenated graph, as the peel sees it
+  const uint32_t* off;             // working row offsets
+  const unsigned long long* row;   // working rows: (id | edge id << 32)
   const uint32_t* opos;
   const uint32_t* ocol;
   const uint32_t* osrc;
@@ -68,8 +71,7 @@ struct Union {  // the prepared concatenated graph
 // copy would land in local memory).
 struct UnionRegs {
   const uint32_t* __restrict__ off;
-  const uint32_t* __restrict__ nbr;
-  const uint32_t* __restrict__ eid;
+  const unsigned long long* __restrict__ row;
   const uint32_t* __restrict__ ocol;
   const uint32_t* __restrict__ osrc;
   int32_t* sup;
@@ -79,7 +81,7 @@ struct UnionRegs {
   unsigned long long* q0;
   unsigned long long* q1;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
-      : off(p->off), nbr(p->nbr), eid(p->eid), ocol(p->ocol), osrc(p->osrc), sup(p->sup), tag(p->tag),
+      : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), sup(p->sup), tag(p->tag),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]) {}
 };
 
@@ -115,7 +117,13 @@ struct Control {
   unsigned long long el_scan;     // active-list entries scanned
   unsigned long long hits;        // triangles found by frontier elements
   unsigned long long edges_proc;  // frontier edges processed
+  unsigned long long csr_slots;   // entries in the working rows
+  unsigned long long compact_min; // do not compact working rows smaller than this
+  uint32_t exit_reason;           // why the loop stopped: kExit*
+  uint32_t compactions;
 };
+
+enum : uint32_t { kExitNone = 0, kExitDone = 1, kExitCompact = 2, kExitError = 3 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -142,6 +150,31 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__
     if (__ldg(a + mid) < x) lo = mid + 1; else hi = mid;
   }
   return lo;
+}
+
+// Position of id w in the sorted row pairs [lo, hi) or kInvalid.  Ids inside
+// a row are spread close to uniformly (vertex ids carry no degree order), so
+// up to three interpolation probes narrow a long row before the binary search:
+// on a 160k-entry hub row that is ~6 dependent loads instead of ~17.
+__device__ __forceinline__ uint32_t find_in_row(const unsigned long long* __restrict__ row, uint32_t lo,
+                                                uint32_t hi, uint32_t w) {
+#pragma unroll 1
+  for (int it = 0; it < 3 && hi - lo > 48; ++it) {
+    const uint32_t a = (uint32_t)__ldg(row + lo), b = (uint32_t)__ldg(row + hi - 1);
+    if (w < a || w > b) return kInvalid;
+    // g in [lo, hi - 1] because w - a <= b - a
+    const uint32_t g =
+        lo + (uint32_t)(((unsigned long long)(w - a) * (hi - 1 - lo)) / ((unsigned long long)(b - a) + 1));
+    const uint32_t x = (uint32_t)__ldg(row + g);
+    if (x == w) return g;
+    if (x < w) lo = g + 1; else hi = g;
+  }
+  const uint32_t end = hi;
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if ((uint32_t)__ldg(row + mid) < w) lo = mid + 1; else hi = mid;
+  }
+  return (lo < end && (uint32_t)__ldg(row + lo) == w) ? lo : kInvalid;
 }
 
 // largest i in [lo, hi] with pref[i] <= k (pref non-decreasing, pref[lo] <= k)
@@ -294,14 +327,19 @@ __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict
   if (lane == 0 && selfc) atomicAdd(self_loops, selfc);
 }
 
-// Kernel B2: fill oriented lists (kept in id order) and the slot -> eid map of
-// each vertex's out-slots; self-loop slots get kInvalid.  Warp per vertex.
+// Kernel B2: fill oriented lists (kept in id order) and, for each vertex's
+// out-slots, the (id | edge id << 32) pair of row0; self-loop slots get edge id
+// 0xFFFFFFFF.  Warp per vertex.
+__device__ __forceinline__ unsigned long long make_pair(uint32_t id, uint32_t e) {
+  return (unsigned long long)id | ((unsigned long long)e << 32);
+}
+
 __global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict__ off,
                                                      const uint32_t* __restrict__ nbr, uint32_t n,
                                                      const uint32_t* __restrict__ opos,
                                                      uint32_t* __restrict__ ocol,
                                                      uint32_t* __restrict__ osrc,
-                                                     uint32_t* __restrict__ eid) {
+                                                     unsigned long long* __restrict__ row0) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -315,7 +353,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict_
       uint32_t v = 0;
       if (s < e) {
         v = __ldg(nbr + s);
-        if (v == u || v >= n) eid[s] = kInvalid;
+        if (v == u || v >= n) row0[s] = make_pair(v, kInvalid);
         else out = rank_less(du, u, deg_of(off, v), v);
       }
       unsigned bal = __ballot_sync(kFull, out);
@@ -323,7 +361,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict_
         uint32_t p = base + __popc(bal & ((1u << lane) - 1));
         ocol[p] = v;
         osrc[p] = u;
-        eid[s] = p;
+        row0[s] = make_pair(v, p);
       }
       base += __popc(bal);
     }
@@ -336,7 +374,7 @@ __global__ void __launch_bounds__(256) k_orient_reverse(const uint32_t* __restri
                                                         const uint32_t* __restrict__ nbr, uint32_t n,
                                                         const uint32_t* __restrict__ opos,
                                                         const uint32_t* __restrict__ ocol,
-                                                        uint32_t* __restrict__ eid,
+                                                        unsigned long long* __restrict__ row0,
                                                         uint32_t* __restrict__ err) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -351,8 +389,8 @@ __global__ void __launch_bounds__(256) k_orient_reverse(const uint32_t* __restri
       if (rank_less(du, u, deg_of(off, v), v)) continue;
       uint32_t lo = __ldg(opos + v), hi = __ldg(opos + v + 1);
       uint32_t p = lower_bound_u32(ocol, lo, hi, u);
-      if (p < hi && __ldg(ocol + p) == u) eid[s] = p;
-      else { eid[s] = kInvalid; bad = true; }
+      if (p < hi && __ldg(ocol + p) == u) row0[s] = make_pair(v, p);
+      else { row0[s] = make_pair(v, kInvalid); bad = true; }
     }
   }
   if (bad) atomicOr(err, kErrAsym);
@@ -641,7 +679,7 @@ struct WaveArgs {
   uint32_t* err;
 };
 
-// work of pushing edge x (union eid): the shorter full row of its endpoints
+// work of pushing edge x (union eid): the shorter working row of its endpoints
 __device__ __forceinline__ uint32_t edge_work(const UnionRegs& U, uint32_t x) {
   const uint32_t u = __ldg(U.osrc + x), v = __ldg(U.ocol + x);
   return min(deg_of(U.off, u), deg_of(U.off, v));
@@ -713,42 +751,72 @@ struct QueueStart {
   __device__ __forceinline__ unsigned long long operator()(uint32_t x) const { return q[x] >> kEidBits; }
 };
 
-// Inclusive warp scan of (v, c); returns the warp totals from lane 31.
-__device__ __forceinline__ void warp_scan2(unsigned long long& v, uint32_t& c) {
+__device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long v) {
   const uint32_t lane = lane_id();
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
-    const unsigned long long ov = __shfl_up_sync(kFull, v, d);
-    const uint32_t oc = __shfl_up_sync(kFull, c, d);
-    if (lane >= (uint32_t)d) { v += ov; c += oc; }
+    const unsigned long long o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
   }
+  return v;
 }
 
-// Warp-aggregated push of edge x (union eid) into member M's next queue with
-// tag W + 1.  All lanes call it; lanes belong to one member.
-__device__ __forceinline__ void push_next(const UnionRegs& U, const Member& M, MemberState* st, uint32_t* err,
-                                          bool want, uint32_t x, uint32_t qsel_next, uint32_t W) {
-  if (!__any_sync(kFull, want)) return;
-  unsigned long long w = 0;
-  if (want) {
-    w = edge_work(U, x);
-    U.tag[x] = W + 1;
-  }
-  unsigned long long v = w;
-  uint32_t c = want ? 1u : 0u;
-  warp_scan2(v, c);
+// Per-warp staging of frontier pushes in shared memory: entries are gathered
+// across iterations and published with one 64-bit atomic (count and work) per
+// kPushBuf entries, instead of one per iteration on a single hot counter.
+constexpr int kPushBuf = 64;
+constexpr int kWaveThreads = 256;
+constexpr int kWaveWarps = kWaveThreads / 32;
+
+struct PushStage {
+  uint2* buf;   // this warp's kPushBuf (edge, work) slots
+  uint32_t n;   // warp-uniform fill
+};
+
+__device__ __forceinline__ void push_flush(PushStage& ps, const Member& M, MemberState* st, uint32_t* err,
+                                           unsigned long long* qnext) {
+  __syncwarp();
+  const uint32_t n = ps.n;
+  if (n == 0) return;
+  const uint32_t lane = lane_id();
+  const uint2 e0 = lane < n ? ps.buf[lane] : make_uint2(0, 0);
+  const uint2 e1 = lane + 32 < n ? ps.buf[lane + 32] : make_uint2(0, 0);
+  const unsigned long long p0 = warp_incl_scan(e0.y), p1 = warp_incl_scan(e1.y);
+  const unsigned long long t0 = __shfl_sync(kFull, p0, 31), t1 = __shfl_sync(kFull, p1, 31);
   unsigned long long old = 0;
-  if (lane_id() == 31) {
-    old = atomicAdd(&st->next, ((unsigned long long)c << kWorkBits) | v);
-    if ((old & kWorkMask) + v > kWorkMask) atomicOr(err, kErrCapacity);
+  if (lane == 0) {
+    old = atomicAdd(&st->next, ((unsigned long long)n << kWorkBits) | (t0 + t1));
+    if ((old & kWorkMask) + t0 + t1 > kWorkMask) atomicOr(err, kErrCapacity);
   }
-  old = __shfl_sync(kFull, old, 31);
-  if (want) {
-    const unsigned long long pos = (old >> kWorkBits) + c - 1;
-    const unsigned long long ws = (old & kWorkMask) + v - w;
-    if (pos < M.m) (qsel_next ? U.q1 : U.q0)[M.eb + pos] = (ws << kEidBits) | (unsigned long long)(x - M.eb);
+  old = __shfl_sync(kFull, old, 0);
+  const unsigned long long pos = old >> kWorkBits, ws = old & kWorkMask;
+  if (lane < n) {
+    if (pos + lane < M.m) qnext[M.eb + pos + lane] = ((ws + p0 - e0.y) << kEidBits) | (e0.x - M.eb);
     else atomicOr(err, kErrCapacity);
   }
+  if (lane + 32 < n) {
+    if (pos + 32 + lane < M.m)
+      qnext[M.eb + pos + 32 + lane] = ((ws + t0 + p1 - e1.y) << kEidBits) | (e1.x - M.eb);
+    else atomicOr(err, kErrCapacity);
+  }
+  ps.n = 0;
+  __syncwarp();
+}
+
+// Queue edge x (union eid) for wave W + 1.  All lanes call it.
+__device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, const Member& M, MemberState* st,
+                                          uint32_t* err, unsigned long long* qnext, bool want, uint32_t x,
+                                          uint32_t W) {
+  const unsigned bal = __ballot_sync(kFull, want);
+  if (!bal) return;
+  const uint32_t k = __popc(bal);
+  if (ps.n + k > kPushBuf) push_flush(ps, M, st, err, qnext);
+  if (want) {
+    U.tag[x] = W + 1;
+    const uint32_t r = __popc(bal & ((1u << lane_id()) - 1));
+    ps.buf[ps.n + r] = make_uint2(x, edge_work(U, x));
+  }
+  ps.n += k;
 }
 
 // Kernel D: one peel wave.  The wave's work (all members' scan elements and
@@ -757,21 +825,25 @@ __device__ __forceinline__ void push_next(const UnionRegs& U, const Member& M, M
 // iteration, so every iteration belongs to one member.
 //   scan element j      active-list entry j: processed -> dropped; support
 //                       <= level -> queued for this level; else kept
-//   frontier element j  element o of the shorter row of frontier edge e,
-//                       searched in the longer row; a hit is a triangle
-__global__ void __launch_bounds__(256) k_wave(WaveArgs a) {
+//   frontier element j  element o of the shorter working row of frontier
+//                       edge e, searched in the longer row; a hit is a triangle
+__global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
+  __shared__ uint2 s_push[kWaveWarps][kPushBuf];
+  __shared__ uint32_t s_keep[kWaveWarps][kPushBuf];
   const Control* ctl = a.ctl;
   if (ctl->done) return;
   const unsigned long long total = ctl->total_work;
   const uint32_t W = ctl->wave;
   const uint32_t G = ctl->G;
   const uint32_t lane = lane_id();
+  const uint32_t wib = threadIdx.x >> 5;
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   const UnionRegs U(a.Up);
   unsigned long long ch = total / (nwarps * 4);
   ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
   uint32_t hits = 0;
+  PushStage ps{s_push[wib], 0};
 
   for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
     const unsigned long long kend = min(c0 + ch, total);
@@ -784,7 +856,7 @@ __global__ void __launch_bounds__(256) k_wave(WaveArgs a) {
       const Member M = a.mem[g];
       MemberState* st = a.st + g;
       const uint32_t phase = st->phase, level = st->level, act_sel = st->act_sel, q_sel = st->q_sel;
-      const uint32_t qn = q_sel ^ 1u;
+      unsigned long long* qnext = q_sel ? U.q0 : U.q1;
       if (phase == kPhaseProc) {
         const unsigned long long* q = (q_sel ? U.q1 : U.q0) + M.eb;
         const uint32_t qcount = (uint32_t)(st->curr >> kWorkBits);
@@ -806,71 +878,154 @@ __global__ void __launch_bounds__(256) k_wave(WaveArgs a) {
             const uint32_t u = __ldg(U.osrc + e), v = __ldg(U.ocol + e);
             const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
             const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
-            uint32_t sb, lb, le;
-            if (ue - ub <= ve - vb) { sb = ub; lb = vb; le = ve; }
-            else { sb = vb; lb = ub; le = ue; }
-            const uint32_t slot = sb + o;
-            const uint32_t w = __ldg(U.nbr + slot);
-            if (w != u && w != v) {
-              const uint32_t p = lower_bound_u32(U.nbr, lb, le, w);
-              if (p < le && __ldg(U.nbr + p) == w) {
-                f = __ldg(U.eid + slot);
-                h = __ldg(U.eid + p);
-                ++hits;
-                pkt_rule(U, e, f, h, level, W, pf, ph);
+            uint32_t sb, slen, lb, le;
+            if (ue - ub <= ve - vb) { sb = ub; slen = ue - ub; lb = vb; le = ve; }
+            else { sb = vb; slen = ve - vb; lb = ub; le = ue; }
+            // rows may have been compacted since the entry's work was counted
+            if (o < slen) {
+              const unsigned long long pr = __ldg(U.row + sb + o);
+              const uint32_t w = (uint32_t)pr;
+              f = (uint32_t)(pr >> 32);
+              if (w != u && w != v && f != kInvalid) {
+                const uint32_t p = find_in_row(U.row, lb, le, w);
+                if (p != kInvalid) {
+                  h = (uint32_t)(__ldg(U.row + p) >> 32);
+                  ++hits;
+                  pkt_rule(U, e, f, h, level, W, pf, ph);
+                }
               }
             }
           }
-          push_next(U, M, st, a.err, pf, f, qn, W);
-          push_next(U, M, st, a.err, ph, h, qn, W);
+          push_edge(ps, U, M, st, a.err, qnext, pf, f, W);
+          push_edge(ps, U, M, st, a.err, qnext, ph, h, W);
           i = x_last;
         }
       } else if (phase == kPhaseScan0 || phase == kPhaseScan) {
         const uint32_t* act = act_sel ? U.act1 : U.act0;
         uint32_t* act_out = act_sel ? U.act0 : U.act1;
+        uint32_t* keepbuf = s_keep[wib];
+        uint32_t nkeep = 0, nzero = 0, mn = 0xFFFFFFFFu;
         for (unsigned long long kb = k; kb < seg_end; kb += 32) {
           const unsigned long long kk = kb + lane;
           const bool valid = kk < seg_end;
           bool keep = false, zero = false, queue = false;
-          uint32_t le = 0, e = 0, ks = 0xFFFFFFFFu;
+          uint32_t le = 0, e = 0;
           if (valid) {
             le = act[M.eb + (kk - mbeg)];
             e = M.eb + le;
             const int32_t s = U.sup[e];
             if (phase == kPhaseScan0) {
               if (s == 0) { U.tag[e] = 0; zero = true; }
-              else { keep = true; ks = (uint32_t)s; }
+              else { keep = true; mn = min(mn, (uint32_t)s); }
             } else if (U.tag[e] == kTagActive) {  // processed edges leave the active list
               if (s <= (int32_t)level) queue = true;
-              else { keep = true; ks = (uint32_t)s; }
+              else { keep = true; mn = min(mn, (uint32_t)s); }
             }
           }
-          push_next(U, M, st, a.err, queue, e, qn, W);
-          if (__any_sync(kFull, keep)) {
-            unsigned long long v = 0;
-            uint32_t c = keep ? 1u : 0u;
-            warp_scan2(v, c);
-            uint32_t mn = ks;
-#pragma unroll
-            for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
-            uint32_t old = 0;
-            if (lane == 31) {
-              old = atomicAdd(&st->kept, c);
-              atomicMin(&st->min_kept, mn);
+          push_edge(ps, U, M, st, a.err, qnext, queue, e, W);
+          const unsigned kb_bal = __ballot_sync(kFull, keep);
+          if (kb_bal) {
+            const uint32_t kc = __popc(kb_bal);
+            if (nkeep + kc > kPushBuf) {
+              __syncwarp();
+              uint32_t old = 0;
+              if (lane == 0) old = atomicAdd(&st->kept, nkeep);
+              old = __shfl_sync(kFull, old, 0);
+              if (lane < nkeep) act_out[M.eb + old + lane] = keepbuf[lane];
+              if (lane + 32 < nkeep) act_out[M.eb + old + 32 + lane] = keepbuf[lane + 32];
+              nkeep = 0;
+              __syncwarp();
             }
-            old = __shfl_sync(kFull, old, 31);
-            if (keep) act_out[M.eb + old + c - 1] = le;
+            if (keep) keepbuf[nkeep + __popc(kb_bal & ((1u << lane) - 1))] = le;
+            nkeep += kc;
           }
-          const unsigned zb = __ballot_sync(kFull, zero);
-          if (zb && lane == 0) atomicAdd(&st->processed, (uint32_t)__popc(zb));
+          nzero += __popc(__ballot_sync(kFull, zero));
         }
+        __syncwarp();
+        if (nkeep) {
+          uint32_t old = 0;
+          if (lane == 0) old = atomicAdd(&st->kept, nkeep);
+          old = __shfl_sync(kFull, old, 0);
+          if (lane < nkeep) act_out[M.eb + old + lane] = keepbuf[lane];
+          if (lane + 32 < nkeep) act_out[M.eb + old + 32 + lane] = keepbuf[lane + 32];
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
+        if (lane == 0) {
+          if (mn != 0xFFFFFFFFu) atomicMin(&st->min_kept, mn);
+          if (nzero) atomicAdd(&st->processed, nzero);
+        }
+        __syncwarp();
       }
+      push_flush(ps, M, st, a.err, qnext);  // entries belong to this member: publish before moving on
       k = seg_end;
     }
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) hits += __shfl_xor_sync(kFull, hits, d);
   if (lane == 0 && hits) atomicAdd(&a.ctl->hits, (unsigned long long)hits);
+}
+
+// Working-row compaction (between waves): keep the entries whose edge is not
+// processed (tag >= the next wave).  Count, scan (host), fill; warp per vertex.
+__global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restrict__ off,
+                                                       const unsigned long long* __restrict__ row, uint32_t n,
+                                                       const uint32_t* __restrict__ tag, const Control* ctl,
+                                                       uint32_t* __restrict__ cnt) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t W = ctl->wave;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    uint32_t c = 0;
+    for (uint32_t s = b + lane; s < e; s += 32) {
+      const uint32_t x = (uint32_t)(__ldg(row + s) >> 32);
+      c += x != kInvalid && __ldg(tag + x) >= W;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(kFull, c, d);
+    if (lane == 0) cnt[u] = c;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict__ off,
+                                                      const unsigned long long* __restrict__ row, uint32_t n,
+                                                      const uint32_t* __restrict__ tag, const Control* ctl,
+                                                      const uint32_t* __restrict__ off2,
+                                                      unsigned long long* __restrict__ row2) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t W = ctl->wave;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    uint32_t at = __ldg(off2 + u);
+    for (uint32_t s0 = b; s0 < e; s0 += 32) {
+      const uint32_t s = s0 + lane;
+      unsigned long long pr = 0;
+      bool keep = false;
+      if (s < e) {
+        pr = __ldg(row + s);
+        const uint32_t x = (uint32_t)(pr >> 32);
+        keep = x != kInvalid && __ldg(tag + x) >= W;
+      }
+      const unsigned bal = __ballot_sync(kFull, keep);
+      if (keep) row2[at + __popc(bal & ((1u << lane) - 1))] = pr;
+      at += __popc(bal);
+    }
+  }
+}
+
+// Publish the compacted rows and resume the loop.
+__global__ void k_compact_commit(Union* U, const uint32_t* off2, const unsigned long long* row2,
+                                 const uint32_t* new_slots, Control* ctl) {
+  U->off = off2;
+  U->row = row2;
+  ctl->csr_slots = *new_slots;
+  ctl->compactions += 1;
+  ctl->exit_reason = kExitNone;
+  ctl->done = 0;
 }
 
 // Planner: one block advances every member's state machine after a wave and
@@ -881,9 +1036,9 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
                                                int use_handle) {
   __shared__ unsigned long long sw[32];
   __shared__ uint32_t s_live;
-  __shared__ unsigned long long s_proc, s_scan, s_edges;
+  __shared__ unsigned long long s_proc, s_scan, s_edges, s_live_edges;
   const uint32_t G = ctl->G;
-  if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; }
+  if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; s_live_edges = 0; }
   __syncthreads();
   const bool was_done = ctl->done;
   unsigned long long carry = 0;
@@ -948,7 +1103,10 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
         atomicAdd(&s_proc, w);
         atomicAdd(&s_edges, s.curr >> kWorkBits);
       }
-      if (s.phase != kPhaseDone) atomicAdd(&s_live, 1u);
+      if (s.phase != kPhaseDone) {
+        atomicAdd(&s_live, 1u);
+        atomicAdd(&s_live_edges, (unsigned long long)(m - s.processed));
+      }
     }
     unsigned long long total;
     unsigned long long ex = block_exclusive_scan<unsigned long long>(w, sw, total);
@@ -967,10 +1125,18 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
       ctl->wave += 1;
       ctl->waves_run += 1;
       const uint32_t e = *err;
-      if (s_live == 0 || e) done = 1;
-      if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; }
-      if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; }
+      uint32_t reason = kExitNone;
+      if (s_live == 0) { done = 1; reason = kExitDone; }
+      if (e) { done = 1; reason = kExitError; }
+      if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; reason = kExitError; }
+      if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; reason = kExitError; }
+      // working rows at most half live: stop so the host can compact them
+      if (!done && ctl->csr_slots >= ctl->compact_min && 4 * s_live_edges <= ctl->csr_slots) {
+        done = 1;
+        reason = kExitCompact;
+      }
       ctl->done = done;
+      ctl->exit_reason = reason;
     }
     if (use_handle) cudaGraphSetConditional(handle, done ? 0u : 1u);
   }
@@ -978,7 +1144,7 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
 
 // Kernel E: truss per slot = level + 2 (pkt.rs:524-526); self-loop slots 2.
 template <typename OutT>
-__global__ void k_finalize(const uint32_t* __restrict__ eid, const int32_t* __restrict__ sup,
+__global__ void k_finalize(const unsigned long long* __restrict__ row0, const int32_t* __restrict__ sup,
                            unsigned long long width, OutT* __restrict__ out, int u8mode, int out8,
                            uint32_t* __restrict__ kmax, uint32_t* __restrict__ err) {
   unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -986,7 +1152,7 @@ __global__ void k_finalize(const uint32_t* __restrict__ eid, const int32_t* __re
   uint32_t mx = 0;
   bool ovf = false;
   for (; i < width; i += stride) {
-    const uint32_t e = __ldg(eid + i);
+    const uint32_t e = (uint32_t)(__ldg(row0 + i) >> 32);
     uint32_t t = 2;
     if (e != kInvalid) {
       const uint32_t s = (uint32_t)__ldg(sup + e);
@@ -1004,12 +1170,12 @@ __global__ void k_finalize(const uint32_t* __restrict__ eid, const int32_t* __re
 }
 
 // support per slot (Triangles::new layout): sup of the slot's edge, 0 for self-loops
-__global__ void k_support_slots(const uint32_t* __restrict__ eid, const int32_t* __restrict__ sup,
+__global__ void k_support_slots(const unsigned long long* __restrict__ row0, const int32_t* __restrict__ sup,
                                 unsigned long long width, uint32_t* __restrict__ out, int u8mode) {
   unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (; i < width; i += stride) {
-    const uint32_t e = __ldg(eid + i);
+    const uint32_t e = (uint32_t)(__ldg(row0 + i) >> 32);
     uint32_t s = e == kInvalid ? 0u : (uint32_t)__ldg(sup + e);
     out[i] = u8mode ? (s & 0xFFu) : s;
   }

@@ -43,6 +43,8 @@ inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 constexpr size_t kStageBytes = 64ull << 20;  // per staging buffer (pinned and device)
 constexpr unsigned long long kDefaultTimeoutMs = 600000ull;
+// working rows below this many entries are never compacted (not worth a pass)
+constexpr unsigned long long kCompactMinSlots = 1ull << 20;
 
 int status_from_flags(uint32_t f) {
   if (!f) return SPARX_OK;
@@ -63,7 +65,8 @@ struct Counters {  // device scalars
 };
 
 struct Layout {
-  size_t off, nbr, eid, dplus, opos, ocol, osrc, sup, tag, act0, act1, q0, q1, out, stage0, stage1;
+  size_t off, nbr, row0, dplus, opos, ocol, osrc, sup, tag, act0, act1, q0, q1, out, stage0, stage1;
+  size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
   size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
   size_t total;
 };
@@ -79,7 +82,7 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   const uint64_t M = std::max<uint64_t>(W / 2, 1);
   L.off = take(4 * (N + 1));
   L.nbr = own_nbr ? take(4 * W) : 0;
-  L.eid = take(4 * W);
+  L.row0 = take(8 * W);
   L.dplus = take(4 * N);
   L.opos = take(4 * (N + 1));
   L.ocol = take(4 * M);
@@ -91,6 +94,10 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   L.q0 = take(16 * M + 16);  // q0 and q1 back to back; also the support prefix (M + 1 u64)
   L.q1 = L.q0 + 8 * M;
   L.out = take(out_bytes);
+  L.offA = take(4 * (N + 1));
+  L.offB = take(4 * (N + 1));
+  L.rowA = take(8 * W);
+  L.rowB = take(8 * W);
   L.stage0 = take(kStageBytes);
   L.stage1 = take(kStageBytes);
   const uint64_t tiles = (std::max<uint64_t>(N + 1, M + 1) + kScanTile - 1) / kScanTile + 2;
@@ -382,7 +389,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   const uint64_t W = J.W;
   Counters* cnt = at<Counters>(E, L.cnt);
   uint32_t* err = &cnt->err;
-  uint32_t* eid = at<uint32_t>(E, L.eid);
+  unsigned long long* row0 = at<unsigned long long>(E, L.row0);
   uint32_t* dplus = at<uint32_t>(E, L.dplus);
   uint32_t* opos = at<uint32_t>(E, L.opos);
   uint32_t* ocol = at<uint32_t>(E, L.ocol);
@@ -419,8 +426,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   if (2 * m + hc.self_loops != W) { J.err = kErrAsym; return SPARX_E_INVALID_CSR; }
   for (const Member& M : J.members)
     if (M.m > kEidMask) { set_error("a graph has >= 2^28 edges"); return SPARX_E_TOO_LARGE; }
-  k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, eid);
-  k_orient_reverse<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, eid, err);
+  k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, row0);
+  k_orient_reverse<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, row0, err);
   J.launches += 2;
   CU(cudaEventRecord(E.tev[2], s));
 
@@ -437,7 +444,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   CU(cudaEventRecord(E.tev[3], s));
 
   if (J.support_only) {
-    k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(eid, sup, W, J.support_out,
+    k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(row0, sup, W, J.support_out,
                                                                        O.support_mode == SPARX_SUPPORT_U8);
     J.launches += 1;
     CU(cudaEventRecord(E.tev[4], s));
@@ -446,8 +453,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     // -- peel (Kernel D) --
     Union U;
     U.off = J.off;
-    U.nbr = J.nbr;
-    U.eid = eid;
+    U.row = row0;
     U.opos = opos;
     U.ocol = ocol;
     U.osrc = osrc;
@@ -468,6 +474,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     c0.G = G;
     c0.max_waves = 2ull * m + 64;
     c0.timeout_ns = O.timeout_ms * 1000000ull;
+    c0.csr_slots = W;
+    c0.compact_min = kCompactMinSlots;
     CU(cudaMemcpyAsync(at<Control>(E, L.ctl), &c0, sizeof(Control), cudaMemcpyHostToDevice, s));
     if (m > 0)
       k_peel_setup<<<grid_for(m, 256, E.sm_count * 8), 256, 0, s>>>(at<Union>(E, L.uni), dmem,
@@ -478,29 +486,50 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
                                    at<unsigned long long>(E, L.wpref), G);
     J.launches += m > 0 ? 2 : 1;
     CU(cudaEventRecord(E.tev[4], s));
-    if (O.loop == SPARX_LOOP_GRAPH) {
-      int rc = build_peel_graph(E, J, s);
-      if (rc) return rc;
-      CU(cudaGraphLaunch(E.peel.exec, s));
-    } else {
-      WaveArgs wa;
-      wa.Up = at<Union>(E, L.uni);
-      wa.mem = dmem;
-      wa.st = at<MemberState>(E, L.st);
-      wa.ctl = at<Control>(E, L.ctl);
-      wa.wpref = at<unsigned long long>(E, L.wpref);
-      wa.err = err;
-      uint32_t* hdone = (uint32_t*)E.pinned_small;
-      for (;;) {
-        for (int i = 0; i < 16; ++i) {
-          k_wave<<<E.wave_blocks, 256, 0, s>>>(wa);
-          k_plan<<<1, 1024, 0, s>>>(wa.mem, wa.st, wa.ctl, at<unsigned long long>(E, L.wpref), err,
-                                    cudaGraphConditionalHandle{}, 0);
-        }
-        CU(cudaMemcpyAsync(hdone, &wa.ctl->done, 4, cudaMemcpyDeviceToHost, s));
+    WaveArgs wa;
+    wa.Up = at<Union>(E, L.uni);
+    wa.mem = dmem;
+    wa.st = at<MemberState>(E, L.st);
+    wa.ctl = at<Control>(E, L.ctl);
+    wa.wpref = at<unsigned long long>(E, L.wpref);
+    wa.err = err;
+    Control* hctl = (Control*)E.pinned_small;
+    const uint32_t* cur_off = J.off;
+    const unsigned long long* cur_row = row0;
+    int next_buf = 0;
+    for (;;) {
+      if (O.loop == SPARX_LOOP_GRAPH) {
+        int rc = build_peel_graph(E, J, s);
+        if (rc) return rc;
+        CU(cudaGraphLaunch(E.peel.exec, s));
+        CU(cudaMemcpyAsync(hctl, wa.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
-        if (*hdone) break;
+      } else {
+        for (;;) {
+          for (int i = 0; i < 16; ++i) {
+            k_wave<<<E.wave_blocks, 256, 0, s>>>(wa);
+            k_plan<<<1, 1024, 0, s>>>(wa.mem, wa.st, wa.ctl, at<unsigned long long>(E, L.wpref), err,
+                                      cudaGraphConditionalHandle{}, 0);
+          }
+          J.launches += 32;
+          CU(cudaMemcpyAsync(hctl, wa.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
+          CU(cudaStreamSynchronize(s));
+          if (hctl->done) break;
+        }
       }
+      if (hctl->exit_reason != kExitCompact) break;
+      // drop processed edges from the working rows, then resume the loop
+      uint32_t* off2 = at<uint32_t>(E, next_buf ? L.offB : L.offA);
+      unsigned long long* row2 = at<unsigned long long>(E, next_buf ? L.rowB : L.rowA);
+      const uint32_t* tag = at<uint32_t>(E, L.tag);
+      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, tag, wa.ctl, dplus);
+      exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
+      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, tag, wa.ctl, off2, row2);
+      k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + N, wa.ctl);
+      J.launches += 6;
+      cur_off = off2;
+      cur_row = row2;
+      next_buf ^= 1;
     }
     CU(cudaEventRecord(E.tev[5], s));
     // -- finalize (Kernel E) --
@@ -508,9 +537,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     const int u8 = O.support_mode == SPARX_SUPPORT_U8;
     if (W > 0) {
       if (O.out_bits == 8)
-        k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(eid, sup, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err);
+        k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(row0, sup, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err);
       else
-        k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(eid, sup, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err);
+        k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(row0, sup, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err);
       J.launches += 1;
     }
   }
@@ -530,7 +559,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   J.tri = hc.tri;
   J.kmax = hc.kmax;
   // each WHILE-loop iteration is one wave kernel + one planner kernel
-  if (!J.support_only) J.launches += 2 * (uint32_t)std::max<unsigned long long>(J.ctl.waves_run, 1);
+  if (!J.support_only && O.loop == SPARX_LOOP_GRAPH)
+    J.launches += 2 * (uint32_t)std::max<unsigned long long>(J.ctl.waves_run, 1);
   J.err = hc.err;
   CU(cudaEventElapsedTime(&J.ms_orient, E.tev[1], E.tev[2]));
   CU(cudaEventElapsedTime(&J.ms_support, E.tev[2], E.tev[3]));
@@ -1050,7 +1080,7 @@ Layout make_noalloc_layout(uint64_t N, uint64_t W) {
   };
   const uint64_t M = std::max<uint64_t>(W / 2, 1);
   L.off = take(4 * (N + 1));
-  L.eid = take(4 * W);
+  L.row0 = take(8 * W);
   L.dplus = take(4 * N);
   L.opos = take(4 * (N + 1));
   L.ocol = take(4 * M);
@@ -1095,7 +1125,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   }
   auto P = [&](size_t off) { return base + off; };
   uint32_t* off = (uint32_t*)P(L.off);
-  uint32_t* eid = (uint32_t*)P(L.eid);
+  unsigned long long* row0 = (unsigned long long*)P(L.row0);
   uint32_t* dplus = (uint32_t*)P(L.dplus);
   uint32_t* opos = (uint32_t*)P(L.opos);
   uint32_t* ocol = (uint32_t*)P(L.ocol);
@@ -1130,8 +1160,8 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   const uint64_t m = m32;
   if (2 * m + hc.self_loops != width) return SPARX_E_INVALID_CSR;
   if (m > kEidMask) return SPARX_E_TOO_LARGE;
-  k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, eid);
-  k_orient_reverse<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, eid, err);
+  k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, row0);
+  k_orient_reverse<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, row0, err);
 
   CU(cudaMemsetAsync(sup, 0, 4 * std::max<uint64_t>(m, 1), s));
   unsigned long long* spref = (unsigned long long*)P(L.q0);
@@ -1143,8 +1173,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
 
   Union U;
   U.off = off;
-  U.nbr = d_nbr;
-  U.eid = eid;
+  U.row = row0;
   U.opos = opos;
   U.ocol = ocol;
   U.osrc = osrc;
@@ -1163,6 +1192,8 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   c0.G = 1;
   c0.max_waves = 2ull * m + 64;
   c0.timeout_ns = kDefaultTimeoutMs * 1000000ull;
+  c0.csr_slots = width;
+  c0.compact_min = ~0ull;  // no compaction buffers in the fixed scratch
   Union* dU = (Union*)P(L.uni);
   Member* dM = (Member*)P(L.mem);
   Control* dC = (Control*)P(L.ctl);
@@ -1196,7 +1227,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
     if (done) break;
   }
   if (width)
-    k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(eid, sup, width, d_out, 0, 0, &cnt->kmax, err);
+    k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(row0, sup, width, d_out, 0, 0, &cnt->kmax, err);
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   CU(cudaGetLastError());
