@@ -219,7 +219,9 @@ def main():
             st = step()
         torch.cuda.synchronize(dev)
         print(json.dumps({"profile": args.workload, "waves": st.waves, "ms_support": st.ms_support,
-                          "ms_peel": st.ms_peel, "launches": st.launches}), flush=True)
+                          "ms_peel": st.ms_peel, "launches": st.launches, "peel_elements": st.peel_elements,
+                          "peel_hits": st.peel_hits, "peel_scanned": st.peel_scanned,
+                          "compactions": st.compactions}), flush=True)
         return 0
     for _ in range(max(3, args.warmup)):
         st = step()
@@ -323,6 +325,9 @@ def main():
                        "dominant": dominant},
             "phases_ms": {"orient": last.ms_orient, "support": ms_sup, "peel": ms_peel,
                           "finalize": last.ms_finalize, "upload": last.ms_upload},
+            "work": {"support_elements": last.support_elements, "peel_elements": last.peel_elements,
+                     "peel_hits": last.peel_hits, "peel_scanned": last.peel_scanned,
+                     "peel_edges": last.peel_edges, "compactions": last.compactions},
             "e2e": {"value": world * g.width / e2e_s, "unit": "edges/s",
                     "h2d_bytes_per_step": 8 * n1 + 8 * g.width, "d2h_bytes_per_step": 4 * g.width,
                     "ms_per_step": e2e_s * 1000, "same_result_as_device_run": same},

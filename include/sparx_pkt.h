@@ -71,6 +71,8 @@ typedef struct sparx_pkt_stats {
   uint64_t peel_hits;         /* triangles found by the peel (processed or skipped) */
   uint64_t peel_scanned;      /* active-list entries read by level scans */
   uint64_t peel_edges;        /* frontier edges processed (= m minus zero-support edges) */
+  uint32_t compactions;       /* rebuilds of the peel's working rows */
+  uint32_t reserved;
 } sparx_pkt_stats;
 
 /* Fill `opts` with defaults (wide support, u8 output, device loop). */

@@ -14,8 +14,10 @@
 //   dplus[n], opos[n+1]         degree-ordered out-degree and its prefix
 //   ocol[m], osrc[m]            oriented edge e = (osrc[e] -> ocol[e]); e is the
 //                               undirected edge id; rank(osrc) < rank(ocol)
-//   sup[m] (i32), tag[m]        support / PKT level, and the wave at which the
-//                               edge is processed (0xFFFFFFFF: not yet queued)
+//   es[m] (int2)                per edge {support / PKT level, tag}: the tag is
+//                               the wave at which the edge is processed
+//                               (0xFFFFFFFF: not yet queued); one 8-byte word so
+//                               a triangle's two other edges cost two sectors
 //   act[2][m], q[2][m] (u64)    per-member active lists and frontier queues,
 //                               segment [eb_g, eb_g + m_g) for member g
 //   working CSR (off, row)      the peel's view: row0 at first, then rebuilt
@@ -47,6 +49,7 @@ enum : uint32_t {
   kErrTimeout = 64u,    // device time budget exhausted
   kErrOffsets = 128u,   // offsets not monotone / wrong total
   kErrWaves = 256u,     // wave bound exceeded (no progress)
+  kErrInternal = 512u,  // inconsistent wave layout (a device loop refused to spin)
 };
 
 enum : uint32_t { kPhaseScan0 = 0, kPhaseScan = 1, kPhaseProc = 2, kPhaseDone = 3 };
@@ -57,8 +60,7 @@ struct Union {  // the prepared concatenated graph, as the peel sees it
   const uint32_t* opos;
   const uint32_t* ocol;
   const uint32_t* osrc;
-  int32_t* sup;
-  uint32_t* tag;
+  int2* es;
   uint32_t* act[2];
   unsigned long long* q[2];
   uint32_t n;
@@ -74,14 +76,13 @@ struct UnionRegs {
   const unsigned long long* __restrict__ row;
   const uint32_t* __restrict__ ocol;
   const uint32_t* __restrict__ osrc;
-  int32_t* sup;
-  uint32_t* tag;
+  int2* es;
   uint32_t* act0;
   uint32_t* act1;
   unsigned long long* q0;
   unsigned long long* q1;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
-      : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), sup(p->sup), tag(p->tag),
+      : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]) {}
 };
 
@@ -524,7 +525,7 @@ __device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i,
 __global__ void __launch_bounds__(256) k_support_balanced(
     const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
     const uint32_t* __restrict__ osrc, const unsigned long long* __restrict__ spref, uint32_t m,
-    int32_t* __restrict__ sup, unsigned long long* __restrict__ tri_total) {
+    int2* __restrict__ es, unsigned long long* __restrict__ tri_total) {
   const uint32_t lane = lane_id();
   const unsigned long long total = spref[m];
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -561,8 +562,8 @@ __global__ void __launch_bounds__(256) k_support_balanced(
           hit = ia < ae && __ldg(ocol + ia) == c;
         }
         if (hit) {
-          atomicAdd(sup + ia, 1);
-          atomicAdd(sup + ib, 1);
+          atomicAdd(&es[ia].x, 1);
+          atomicAdd(&es[ib].x, 1);
           found_total++;
         }
       }
@@ -571,7 +572,7 @@ __global__ void __launch_bounds__(256) k_support_balanced(
       const unsigned grp = __match_any_sync(kFull, valid ? e : kInvalid);
       if (valid && lane == (uint32_t)(__ffs(grp) - 1)) {
         const int c = __popc(grp & hits);
-        if (c) atomicAdd(sup + e, c);
+        if (c) atomicAdd(&es[e].x, c);
       }
       i = e_last;
     }
@@ -615,12 +616,11 @@ __global__ void __launch_bounds__(256) k_peel_setup(const Union* __restrict__ Up
       flush_member_stats(cur, sum, mx, mem_tri, mem_maxsup);
       cur = g; sum = 0; mx = 0;
     }
-    int32_t s = U.sup[e];
+    int32_t s = U.es[e].x;
     sum += (unsigned long long)s;
     if (u8mode) s &= 0xFF;
-    U.sup[e] = s;
+    U.es[e] = make_int2(s, (int)kTagActive);
     mx = max(mx, (uint32_t)s);
-    U.tag[e] = kTagActive;
     U.act[0][e] = e - mem[g].eb;
   }
   // warp reduction when every lane ends on the same member
@@ -694,26 +694,27 @@ __device__ __forceinline__ uint32_t edge_work(const UnionRegs& U, uint32_t x) {
 //   only h above l                      -> symmetric
 // A charge that lands on l + 1 queues the edge for the next sub-level; a
 // charge that goes below l is restored to l.
-__device__ __forceinline__ void pkt_rule(const UnionRegs& U, uint32_t e, uint32_t f, uint32_t h, uint32_t l,
-                                         uint32_t W, bool& pf, bool& ph) {
+__device__ __forceinline__ void pkt_rule(const UnionRegs& U, uint32_t e, uint32_t f, int2 es_f, uint32_t h,
+                                         uint32_t l, uint32_t W, bool& pf, bool& ph) {
   pf = ph = false;
-  const uint32_t tf = U.tag[f], th = U.tag[h];
+  const int2 es_h = U.es[h];
+  const uint32_t tf = (uint32_t)es_f.y, th = (uint32_t)es_h.y;
   if (tf < W || th < W) return;
-  const int32_t sf = U.sup[f], sh = U.sup[h];
+  const int32_t sf = es_f.x, sh = es_h.x;
   const int32_t L = (int32_t)l;
   bool df = false, dh = false;
   if (sf > L && sh > L) { df = true; dh = true; }
   else if (sf > L) df = (e < h) || (th != W);
   else if (sh > L) dh = (e < f) || (tf != W);
   if (df) {
-    int32_t prev = atomicSub(U.sup + f, 1);
+    int32_t prev = atomicSub(&U.es[f].x, 1);
     if (prev == L + 1) pf = true;
-    else if (prev <= L) atomicMax(U.sup + f, L);
+    else if (prev <= L) atomicMax(&U.es[f].x, L);
   }
   if (dh) {
-    int32_t prev = atomicSub(U.sup + h, 1);
+    int32_t prev = atomicSub(&U.es[h].x, 1);
     if (prev == L + 1) ph = true;
-    else if (prev <= L) atomicMax(U.sup + h, L);
+    else if (prev <= L) atomicMax(&U.es[h].x, L);
   }
 }
 
@@ -812,7 +813,7 @@ __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, con
   const uint32_t k = __popc(bal);
   if (ps.n + k > kPushBuf) push_flush(ps, M, st, err, qnext);
   if (want) {
-    U.tag[x] = W + 1;
+    U.es[x].y = (int)(W + 1);
     const uint32_t r = __popc(bal & ((1u << lane_id()) - 1));
     ps.buf[ps.n + r] = make_uint2(x, edge_work(U, x));
   }
@@ -853,6 +854,10 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
       while (g + 1 < G && a.wpref[g + 1] <= k) ++g;
       const unsigned long long mbeg = a.wpref[g];
       const unsigned long long seg_end = min(kend, a.wpref[g + 1]);
+      if (seg_end <= k || mbeg > k) {  // layout does not cover k: stop rather than spin
+        if (lane == 0) atomicOr(a.err, kErrInternal);
+        break;
+      }
       const Member M = a.mem[g];
       MemberState* st = a.st + g;
       const uint32_t phase = st->phase, level = st->level, act_sel = st->act_sel, q_sel = st->q_sel;
@@ -860,8 +865,15 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
       if (phase == kPhaseProc) {
         const unsigned long long* q = (q_sel ? U.q1 : U.q0) + M.eb;
         const uint32_t qcount = (uint32_t)(st->curr >> kWorkBits);
+        if (qcount == 0) {
+          if (lane == 0) atomicOr(a.err, kErrInternal);
+          k = seg_end;
+          continue;
+        }
         const QueueStart qs{q};
         uint32_t i = last_entry_le(q, 0, qcount - 1, k - mbeg);
+        // merge cursor carried across iterations that continue the same edge
+        uint32_t m_e = kInvalid, m_next_o = 0, m_cur = 0;
         for (unsigned long long kb = k; kb < seg_end; kb += 32) {
           const unsigned long long kk = kb + lane;
           const bool valid = kk < seg_end;
@@ -869,32 +881,88 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
           const uint32_t x = window_find(qs, i, qcount, j, valid);
           const uint32_t last = (uint32_t)min(31ull, seg_end - 1 - kb);
           const uint32_t x_last = __shfl_sync(kFull, x, last);
-          bool pf = false, ph = false;
-          uint32_t f = 0, h = 0;
+          uint32_t e = 0, o = 0, u = 0, v = 0, sb = 0, slen = 0, lb = 0, le = 0;
           if (valid) {
             const unsigned long long ent = q[x];
-            const uint32_t e = M.eb + (uint32_t)(ent & kEidMask);
-            const uint32_t o = (uint32_t)(j - (ent >> kEidBits));
-            const uint32_t u = __ldg(U.osrc + e), v = __ldg(U.ocol + e);
+            e = M.eb + (uint32_t)(ent & kEidMask);
+            o = (uint32_t)(j - (ent >> kEidBits));
+            u = __ldg(U.osrc + e);
+            v = __ldg(U.ocol + e);
             const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
             const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
-            uint32_t sb, slen, lb, le;
             if (ue - ub <= ve - vb) { sb = ub; slen = ue - ub; lb = vb; le = ve; }
             else { sb = vb; slen = ve - vb; lb = ub; le = ue; }
-            // rows may have been compacted since the entry's work was counted
-            if (o < slen) {
-              const unsigned long long pr = __ldg(U.row + sb + o);
-              const uint32_t w = (uint32_t)pr;
-              f = (uint32_t)(pr >> 32);
-              if (w != u && w != v && f != kInvalid) {
-                const uint32_t p = find_in_row(U.row, lb, le, w);
-                if (p != kInvalid) {
-                  h = (uint32_t)(__ldg(U.row + p) >> 32);
-                  ++hits;
-                  pkt_rule(U, e, f, h, level, W, pf, ph);
+          }
+          // rows may have been compacted since the entry's work was counted
+          const bool el = valid && o < slen;
+          unsigned long long pr = el ? __ldg(U.row + sb + o) : 0ull;
+          const uint32_t w = (uint32_t)pr;
+          uint32_t f = (uint32_t)(pr >> 32), h = 0, p = kInvalid;
+          bool look = el && w != u && w != v && f != kInvalid;
+          // the other edge of the small row: already processed -> no triangle to resolve
+          int2 es_f = make_int2(0, 0);
+          if (look) {
+            es_f = U.es[f];
+            look = (uint32_t)es_f.y >= W;
+          }
+          // lane 0 is always valid: its row bounds decide, so the branch and the
+          // merge below are warp-uniform
+          const uint32_t e0 = __shfl_sync(kFull, e, 0);
+          const uint32_t L_beg = __shfl_sync(kFull, lb, 0), L_end = __shfl_sync(kFull, le, 0);
+          const uint32_t s_len0 = __shfl_sync(kFull, slen, 0);
+          const bool one_edge = __all_sync(kFull, !valid || e == e0);
+          if (one_edge && (L_end - L_beg) <= 8u * s_len0) {
+            // similar row lengths: walk the longer row with a warp-wide cursor;
+            // every chunk of 32 entries is matched against the 32 sorted
+            // elements by a shuffle search
+            const unsigned elb = __ballot_sync(kFull, el);
+            if (elb) {
+              const uint32_t o0 = __shfl_sync(kFull, o, 0);
+              const uint32_t wmax = __shfl_sync(kFull, w, 31 - __clz(elb));
+              uint32_t cur;
+              if (m_e == e0 && m_next_o == o0) {
+                cur = m_cur;
+              } else {
+                const uint32_t wmin = __shfl_sync(kFull, w, __ffs(elb) - 1);
+                uint32_t lo = L_beg, hi = L_end;
+                while (lo < hi) {
+                  const uint32_t mid = lo + ((hi - lo) >> 1);
+                  if ((uint32_t)__ldg(U.row + mid) < wmin) lo = mid + 1; else hi = mid;
                 }
+                cur = lo;
               }
+              for (;;) {
+                const uint32_t idx = cur + lane;
+                const unsigned long long lp = idx < L_end ? __ldg(U.row + idx) : ~0ull;
+                const uint32_t lv = (uint32_t)lp;
+                uint32_t t = 0;
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) {
+                  const uint32_t cand = __shfl_sync(kFull, lv, t + d);
+                  if (cand <= w) t += d;
+                }
+                const uint32_t lvt = __shfl_sync(kFull, lv, t);
+                const uint32_t ht = (uint32_t)(__shfl_sync(kFull, lp, t) >> 32);
+                if (look && lvt == w) { p = cur + t; h = ht; }
+                const uint32_t adv = __popc(__ballot_sync(kFull, lv <= wmax));
+                cur += adv;
+                if (adv < 32) break;
+              }
+              m_e = e0;
+              m_next_o = o0 + 32;
+              m_cur = cur;
             }
+          } else {
+            m_e = kInvalid;
+            if (look) {
+              p = find_in_row(U.row, lb, le, w);
+              if (p != kInvalid) h = (uint32_t)(__ldg(U.row + p) >> 32);
+            }
+          }
+          bool pf = false, ph = false;
+          if (look && p != kInvalid) {
+            ++hits;
+            pkt_rule(U, e, f, es_f, h, level, W, pf, ph);
           }
           push_edge(ps, U, M, st, a.err, qnext, pf, f, W);
           push_edge(ps, U, M, st, a.err, qnext, ph, h, W);
@@ -913,11 +981,12 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
           if (valid) {
             le = act[M.eb + (kk - mbeg)];
             e = M.eb + le;
-            const int32_t s = U.sup[e];
+            const int2 st_e = U.es[e];
+            const int32_t s = st_e.x;
             if (phase == kPhaseScan0) {
-              if (s == 0) { U.tag[e] = 0; zero = true; }
+              if (s == 0) { U.es[e].y = 0; zero = true; }
               else { keep = true; mn = min(mn, (uint32_t)s); }
-            } else if (U.tag[e] == kTagActive) {  // processed edges leave the active list
+            } else if ((uint32_t)st_e.y == kTagActive) {  // processed edges leave the active list
               if (s <= (int32_t)level) queue = true;
               else { keep = true; mn = min(mn, (uint32_t)s); }
             }
@@ -970,7 +1039,7 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
 // processed (tag >= the next wave).  Count, scan (host), fill; warp per vertex.
 __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restrict__ off,
                                                        const unsigned long long* __restrict__ row, uint32_t n,
-                                                       const uint32_t* __restrict__ tag, const Control* ctl,
+                                                       const int2* __restrict__ es, const Control* ctl,
                                                        uint32_t* __restrict__ cnt) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -981,7 +1050,7 @@ __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restric
     uint32_t c = 0;
     for (uint32_t s = b + lane; s < e; s += 32) {
       const uint32_t x = (uint32_t)(__ldg(row + s) >> 32);
-      c += x != kInvalid && __ldg(tag + x) >= W;
+      c += x != kInvalid && (uint32_t)__ldg(&es[x].y) >= W;
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(kFull, c, d);
@@ -991,7 +1060,7 @@ __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restric
 
 __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict__ off,
                                                       const unsigned long long* __restrict__ row, uint32_t n,
-                                                      const uint32_t* __restrict__ tag, const Control* ctl,
+                                                      const int2* __restrict__ es, const Control* ctl,
                                                       const uint32_t* __restrict__ off2,
                                                       unsigned long long* __restrict__ row2) {
   const uint32_t lane = lane_id();
@@ -1008,7 +1077,7 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
       if (s < e) {
         pr = __ldg(row + s);
         const uint32_t x = (uint32_t)(pr >> 32);
-        keep = x != kInvalid && __ldg(tag + x) >= W;
+        keep = x != kInvalid && (uint32_t)__ldg(&es[x].y) >= W;
       }
       const unsigned bal = __ballot_sync(kFull, keep);
       if (keep) row2[at + __popc(bal & ((1u << lane) - 1))] = pr;
@@ -1041,6 +1110,12 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
   if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; s_live_edges = 0; }
   __syncthreads();
   const bool was_done = ctl->done;
+  if (was_done) {
+    // the loop is stopped (host-launched waves keep coming until the host
+    // looks): the planned wave must survive untouched for a resume
+    if (threadIdx.x == 0 && use_handle) cudaGraphSetConditional(handle, 0u);
+    return;
+  }
   unsigned long long carry = 0;
   for (uint32_t b = 0; b < G; b += blockDim.x) {
     const uint32_t g = b + threadIdx.x;
@@ -1130,8 +1205,9 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
       if (e) { done = 1; reason = kExitError; }
       if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; reason = kExitError; }
       if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; reason = kExitError; }
-      // working rows at most half live: stop so the host can compact them
-      if (!done && ctl->csr_slots >= ctl->compact_min && 4 * s_live_edges <= ctl->csr_slots) {
+      // live edges fill at most 70% of the working rows: stop so the host can
+      // compact them (a compaction costs about three passes over the rows)
+      if (!done && ctl->csr_slots >= ctl->compact_min && 20 * s_live_edges <= 7 * ctl->csr_slots) {
         done = 1;
         reason = kExitCompact;
       }
@@ -1144,7 +1220,7 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
 
 // Kernel E: truss per slot = level + 2 (pkt.rs:524-526); self-loop slots 2.
 template <typename OutT>
-__global__ void k_finalize(const unsigned long long* __restrict__ row0, const int32_t* __restrict__ sup,
+__global__ void k_finalize(const unsigned long long* __restrict__ row0, const int2* __restrict__ es,
                            unsigned long long width, OutT* __restrict__ out, int u8mode, int out8,
                            uint32_t* __restrict__ kmax, uint32_t* __restrict__ err) {
   unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1155,7 +1231,7 @@ __global__ void k_finalize(const unsigned long long* __restrict__ row0, const in
     const uint32_t e = (uint32_t)(__ldg(row0 + i) >> 32);
     uint32_t t = 2;
     if (e != kInvalid) {
-      const uint32_t s = (uint32_t)__ldg(sup + e);
+      const uint32_t s = (uint32_t)__ldg(&es[e].x);
       t = s + 2;
       if (u8mode) { ovf |= s >= 255; t &= 0xFFu; }
       else if (out8) ovf |= t > 255;
@@ -1170,13 +1246,13 @@ __global__ void k_finalize(const unsigned long long* __restrict__ row0, const in
 }
 
 // support per slot (Triangles::new layout): sup of the slot's edge, 0 for self-loops
-__global__ void k_support_slots(const unsigned long long* __restrict__ row0, const int32_t* __restrict__ sup,
+__global__ void k_support_slots(const unsigned long long* __restrict__ row0, const int2* __restrict__ es,
                                 unsigned long long width, uint32_t* __restrict__ out, int u8mode) {
   unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (; i < width; i += stride) {
     const uint32_t e = (uint32_t)(__ldg(row0 + i) >> 32);
-    uint32_t s = e == kInvalid ? 0u : (uint32_t)__ldg(sup + e);
+    uint32_t s = e == kInvalid ? 0u : (uint32_t)__ldg(&es[e].x);
     out[i] = u8mode ? (s & 0xFFu) : s;
   }
 }

@@ -52,6 +52,7 @@ int status_from_flags(uint32_t f) {
   if (f & (kErrRange | kErrUnsorted | kErrAsym | kErrOffsets)) return SPARX_E_INVALID_CSR;
   if (f & kErrCapacity) return SPARX_E_TOO_LARGE;
   if (f & (kErrTimeout | kErrWaves)) return SPARX_E_TIMEOUT;
+  if (f & kErrInternal) return SPARX_E_CUDA;
   if (f & kErrOverflowU8) return SPARX_E_OVERFLOW_U8;
   return SPARX_E_CUDA;
 }
@@ -65,7 +66,7 @@ struct Counters {  // device scalars
 };
 
 struct Layout {
-  size_t off, nbr, row0, dplus, opos, ocol, osrc, sup, tag, act0, act1, q0, q1, out, stage0, stage1;
+  size_t off, nbr, row0, dplus, opos, ocol, osrc, es, act0, act1, q0, q1, out, stage0, stage1;
   size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
   size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
   size_t total;
@@ -87,8 +88,7 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   L.opos = take(4 * (N + 1));
   L.ocol = take(4 * M);
   L.osrc = take(4 * M);
-  L.sup = take(4 * M);
-  L.tag = take(4 * M);
+  L.es = take(8 * M);
   L.act0 = take(4 * M);
   L.act1 = take(4 * M);
   L.q0 = take(16 * M + 16);  // q0 and q1 back to back; also the support prefix (M + 1 u64)
@@ -394,7 +394,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   uint32_t* opos = at<uint32_t>(E, L.opos);
   uint32_t* ocol = at<uint32_t>(E, L.ocol);
   uint32_t* osrc = at<uint32_t>(E, L.osrc);
-  int32_t* sup = at<int32_t>(E, L.sup);
+  int2* es = at<int2>(E, L.es);
   Member* dmem = at<Member>(E, L.mem);
   const int vgrid = grid_for((unsigned long long)N * 32, 256, E.sm_count * 32);
 
@@ -432,19 +432,19 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   CU(cudaEventRecord(E.tev[2], s));
 
   // -- support (Kernel C) --
-  CU(cudaMemsetAsync(sup, 0, 4 * std::max<uint64_t>(m, 1), s));
+  CU(cudaMemsetAsync(es, 0, 8 * std::max<uint64_t>(m, 1), s));
   unsigned long long* spref = at<unsigned long long>(E, L.q0);
   if (m > 0) {
     exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, at<unsigned long long>(E, L.tiles),
                                        &cnt->grand, s);
-    k_support_balanced<<<E.sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, sup, &cnt->tri);
+    k_support_balanced<<<E.sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri);
     J.launches += 4;
     CU(cudaMemcpyAsync(&J.support_elements, spref + m, 8, cudaMemcpyDeviceToHost, s));
   }
   CU(cudaEventRecord(E.tev[3], s));
 
   if (J.support_only) {
-    k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(row0, sup, W, J.support_out,
+    k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(row0, es, W, J.support_out,
                                                                        O.support_mode == SPARX_SUPPORT_U8);
     J.launches += 1;
     CU(cudaEventRecord(E.tev[4], s));
@@ -457,8 +457,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     U.opos = opos;
     U.ocol = ocol;
     U.osrc = osrc;
-    U.sup = sup;
-    U.tag = at<uint32_t>(E, L.tag);
+    U.es = es;
     U.act[0] = at<uint32_t>(E, L.act0);
     U.act[1] = at<uint32_t>(E, L.act1);
     U.q[0] = at<unsigned long long>(E, L.q0);
@@ -521,10 +520,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       // drop processed edges from the working rows, then resume the loop
       uint32_t* off2 = at<uint32_t>(E, next_buf ? L.offB : L.offA);
       unsigned long long* row2 = at<unsigned long long>(E, next_buf ? L.rowB : L.rowA);
-      const uint32_t* tag = at<uint32_t>(E, L.tag);
-      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, tag, wa.ctl, dplus);
+      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, es, wa.ctl, dplus);
       exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
-      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, tag, wa.ctl, off2, row2);
+      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, es, wa.ctl, off2, row2);
       k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + N, wa.ctl);
       J.launches += 6;
       cur_off = off2;
@@ -537,9 +535,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     const int u8 = O.support_mode == SPARX_SUPPORT_U8;
     if (W > 0) {
       if (O.out_bits == 8)
-        k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(row0, sup, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err);
+        k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(row0, es, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err);
       else
-        k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(row0, sup, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err);
+        k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(row0, es, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err);
       J.launches += 1;
     }
   }
@@ -593,6 +591,7 @@ void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
     st->peel_hits = J.ctl.hits;
     st->peel_scanned = J.ctl.el_scan;
     st->peel_edges = J.ctl.edges_proc;
+    st->compactions = J.ctl.compactions;
   }
   st->ms_orient = J.ms_orient;
   st->ms_support = J.ms_support;
@@ -1085,8 +1084,7 @@ Layout make_noalloc_layout(uint64_t N, uint64_t W) {
   L.opos = take(4 * (N + 1));
   L.ocol = take(4 * M);
   L.osrc = take(4 * M);
-  L.sup = take(4 * M);
-  L.tag = take(4 * M);
+  L.es = take(8 * M);
   L.act0 = take(4 * M);
   L.act1 = take(4 * M);
   L.q0 = take(16 * M + 16);
@@ -1130,7 +1128,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   uint32_t* opos = (uint32_t*)P(L.opos);
   uint32_t* ocol = (uint32_t*)P(L.ocol);
   uint32_t* osrc = (uint32_t*)P(L.osrc);
-  int32_t* sup = (int32_t*)P(L.sup);
+  int2* es = (int2*)P(L.es);
   Counters* cnt = (Counters*)P(L.cnt);
   uint32_t* err = &cnt->err;
   int sm = 148, per_sm = 1;
@@ -1163,12 +1161,12 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, row0);
   k_orient_reverse<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, row0, err);
 
-  CU(cudaMemsetAsync(sup, 0, 4 * std::max<uint64_t>(m, 1), s));
+  CU(cudaMemsetAsync(es, 0, 8 * std::max<uint64_t>(m, 1), s));
   unsigned long long* spref = (unsigned long long*)P(L.q0);
   if (m > 0) {
     exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, (unsigned long long*)P(L.tiles),
                                        &cnt->grand, s);
-    k_support_balanced<<<sm * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, sup, &cnt->tri);
+    k_support_balanced<<<sm * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri);
   }
 
   Union U;
@@ -1177,8 +1175,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   U.opos = opos;
   U.ocol = ocol;
   U.osrc = osrc;
-  U.sup = sup;
-  U.tag = (uint32_t*)P(L.tag);
+  U.es = es;
   U.act[0] = (uint32_t*)P(L.act0);
   U.act[1] = (uint32_t*)P(L.act1);
   U.q[0] = (unsigned long long*)P(L.q0);
@@ -1227,7 +1224,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
     if (done) break;
   }
   if (width)
-    k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(row0, sup, width, d_out, 0, 0, &cnt->kmax, err);
+    k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(row0, es, width, d_out, 0, 0, &cnt->kmax, err);
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   CU(cudaGetLastError());

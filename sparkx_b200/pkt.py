@@ -71,7 +71,7 @@ class _Stats(ctypes.Structure):
         ("ms_total", ctypes.c_double),
         ("support_elements", ctypes.c_uint64), ("peel_elements", ctypes.c_uint64),
         ("peel_hits", ctypes.c_uint64), ("peel_scanned", ctypes.c_uint64),
-        ("peel_edges", ctypes.c_uint64),
+        ("peel_edges", ctypes.c_uint64), ("compactions", ctypes.c_uint32), ("reserved2", ctypes.c_uint32),
     ]
 
 
@@ -174,6 +174,7 @@ class PktStats:
     peel_hits: int = 0
     peel_scanned: int = 0
     peel_edges: int = 0
+    compactions: int = 0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "PktStats":

@@ -253,3 +253,16 @@ def test_batch_isolates_bad_members_and_budget():
         assert r[2] == 0 and np.array_equal(r[0], O.pkt(g.offsets, g.neighbours))
     res = run_batch([(gs[0].offsets, gs[0].neighbours)], O32, hbm_budget_bytes=1 << 20)
     assert res[0][2] == P.E_OOM
+
+
+@pytest.mark.parametrize("loop", [P.LOOP_GRAPH, LOOP_HOST])
+def test_compaction_in_both_loops(loop):
+    """Graphs above the compaction threshold rebuild the working rows mid-peel;
+    host-launched waves must resume the planned wave unchanged after each rebuild."""
+    fx = fixtures()
+    for name in ("rmat16", "rmat18"):
+        p = fx[name]["params"]
+        g = gen.rmat(p["scale"], p["ef"], seed=p["seed"])
+        t, st = run_pkt(g.offsets, g.neighbours, PktOptions(out_bits=32, loop=loop, timeout_ms=120_000))
+        assert truss_sha(t) == fx[name]["modes"]["0"]["truss_sha256"]
+        assert st.compactions >= 1
