@@ -178,6 +178,8 @@ def main():
                     help="device steps only (warm-up and steps as given), for profiler captures")
     ap.add_argument("--loop", choices=["graph", "host"], default="graph",
                     help="peel loop: CUDA-graph WHILE node (default) or host-launched waves")
+    ap.add_argument("--support-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="0 auto, 1 balanced edge form, 2 vertex form")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -207,7 +209,8 @@ def main():
     d_nbr = torch.from_numpy(g.neighbours.view(np.int32)).to(dev)
     # 32-bit truss output: R-MAT-22's truss numbers exceed the reference's u8 layout (k_max 543)
     d_out = torch.empty(g.width, dtype=torch.int32, device=dev)
-    opts = PktOptions(out_bits=32, device=local, loop=0 if args.loop == "graph" else 1)
+    opts = PktOptions(out_bits=32, device=local, loop=0 if args.loop == "graph" else 1,
+                      support_kernel=args.support_kernel)
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -221,7 +224,8 @@ def main():
         print(json.dumps({"profile": args.workload, "waves": st.waves, "ms_support": st.ms_support,
                           "ms_peel": st.ms_peel, "launches": st.launches, "peel_elements": st.peel_elements,
                           "peel_hits": st.peel_hits, "peel_scanned": st.peel_scanned,
-                          "compactions": st.compactions}), flush=True)
+                          "compactions": st.compactions, "merge_iters": st.merge_iters,
+                          "lane_iters": st.lane_iters, "merge_chunks": st.merge_chunks}), flush=True)
         return 0
     for _ in range(max(3, args.warmup)):
         st = step()
@@ -327,7 +331,9 @@ def main():
                           "finalize": last.ms_finalize, "upload": last.ms_upload},
             "work": {"support_elements": last.support_elements, "peel_elements": last.peel_elements,
                      "peel_hits": last.peel_hits, "peel_scanned": last.peel_scanned,
-                     "peel_edges": last.peel_edges, "compactions": last.compactions},
+                     "peel_edges": last.peel_edges, "compactions": last.compactions,
+                     "merge_iters": last.merge_iters, "lane_iters": last.lane_iters,
+                     "merge_chunks": last.merge_chunks},
             "e2e": {"value": world * g.width / e2e_s, "unit": "edges/s",
                     "h2d_bytes_per_step": 8 * n1 + 8 * g.width, "d2h_bytes_per_step": 4 * g.width,
                     "ms_per_step": e2e_s * 1000, "same_result_as_device_run": same},

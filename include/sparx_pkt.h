@@ -73,6 +73,9 @@ typedef struct sparx_pkt_stats {
   uint64_t peel_edges;        /* frontier edges processed (= m minus zero-support edges) */
   uint32_t compactions;       /* rebuilds of the peel's working rows */
   uint32_t reserved;
+  uint64_t merge_iters;       /* peel warp iterations resolved by a row merge */
+  uint64_t lane_iters;        /* peel warp iterations resolved by per-lane searches */
+  uint64_t merge_chunks;      /* 32-entry chunks of longer rows read by the merges */
 } sparx_pkt_stats;
 
 /* Fill `opts` with defaults (wide support, u8 output, device loop). */
@@ -132,7 +135,7 @@ int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64
  * scratch lives in one fixed file-scope device array of
  * SPARX_NOALLOC_SCRATCH_BYTES per device (present on every GPU that loads the
  * library, until exit); graphs needing more get SPARX_E_TOO_LARGE (roughly
- * 2.5 M CSR slots).  The call allocates no device or pinned memory, streams or
+ * 1.4 M CSR slots).  The call allocates no device or pinned memory, streams or
  * events.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress), so make it before any stream capture begins.  All
  * calls on a device share the array and it keeps the previous call's

@@ -19,7 +19,8 @@ class NativeLibraryMissing(RuntimeError):
 
 
 def library_path(name: str) -> str:
-    return os.path.join(_HERE, name)
+    """In-tree library; SPARX_LIB_DIR points at another build of the same sources."""
+    return os.path.join(os.environ.get("SPARX_LIB_DIR", _HERE), name)
 
 
 def load_library(name: str) -> ctypes.CDLL:

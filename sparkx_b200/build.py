@@ -51,7 +51,8 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
     target = os.path.join(HERE, "libsparx_pkt.so")
     deps = _sources((".cu", ".cuh", ".h"))
     if force or _stale(target, deps):
-        cmd = [_nvcc(), *NVCC_FLAGS, "-o", target, os.path.join(CSRC, "sparx_pkt.cu"), "-lgomp"]
+        extra = os.environ.get("SPARX_NVCC_FLAGS", "").split()
+        cmd = [_nvcc(), *NVCC_FLAGS, *extra, "-o", target, os.path.join(CSRC, "sparx_pkt.cu"), "-lgomp"]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)

@@ -63,6 +63,7 @@ struct Union {  // the prepared concatenated graph, as the peel sees it
   int2* es;
   uint32_t* act[2];
   unsigned long long* q[2];
+  uint4* qd[2];                    // per queue entry {short row start, length, long row begin, end}
   uint32_t n;
   uint32_t m;
   uint32_t width;
@@ -81,9 +82,12 @@ struct UnionRegs {
   uint32_t* act1;
   unsigned long long* q0;
   unsigned long long* q1;
+  uint4* qd0;
+  uint4* qd1;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
       : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
-        act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]) {}
+        act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]),
+        qd0(p->qd[0]), qd1(p->qd[1]) {}
 };
 
 struct Member {  // static per-member ranges
@@ -122,6 +126,9 @@ struct Control {
   unsigned long long compact_min; // do not compact working rows smaller than this
   uint32_t exit_reason;           // why the loop stopped: kExit*
   uint32_t compactions;
+  unsigned long long merge_iters; // warp iterations resolved by the row merge
+  unsigned long long lane_iters;  // warp iterations resolved by per-lane searches
+  unsigned long long merge_chunks;// 32-entry chunks of longer rows read by merges
 };
 
 enum : uint32_t { kExitNone = 0, kExitDone = 1, kExitCompact = 2, kExitError = 3 };
@@ -196,6 +203,16 @@ __device__ __forceinline__ uint32_t last_entry_le(const unsigned long long* __re
     if ((q[mid] >> kEidBits) <= k) lo = mid; else hi = mid - 1;
   }
   return lo;
+}
+
+__device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long v) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
+  }
+  return v;
 }
 
 // Segmented inclusive warp scan; segments are runs of equal `key`, which is
@@ -296,11 +313,12 @@ __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict
                                                       const uint32_t* __restrict__ nbr, uint32_t n,
                                                       uint32_t* __restrict__ dplus,
                                                       unsigned long long* __restrict__ self_loops,
-                                                      uint32_t* __restrict__ err) {
+                                                      uint32_t* __restrict__ err,
+                                                      uint32_t* __restrict__ max_dplus) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  uint32_t flags = 0;
+  uint32_t flags = 0, mxd = 0;
   unsigned long long selfc = 0;
   for (uint32_t u = warp; u < n; u += nwarps) {
     const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
@@ -320,12 +338,16 @@ __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) cnt += __shfl_down_sync(kFull, cnt, d);
-    if (lane == 0) dplus[u] = cnt;
+    if (lane == 0) {
+      dplus[u] = cnt;
+      mxd = max(mxd, cnt);
+    }
   }
   if (flags) atomicOr(err, flags);
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) selfc += __shfl_down_sync(kFull, selfc, d);
   if (lane == 0 && selfc) atomicAdd(self_loops, selfc);
+  if (lane == 0 && mxd) atomicMax(max_dplus, mxd);
 }
 
 // Kernel B2: fill oriented lists (kept in id order) and, for each vertex's
@@ -525,7 +547,7 @@ __device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i,
 __global__ void __launch_bounds__(256) k_support_balanced(
     const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
     const uint32_t* __restrict__ osrc, const unsigned long long* __restrict__ spref, uint32_t m,
-    int2* __restrict__ es, unsigned long long* __restrict__ tri_total) {
+    int2* __restrict__ es, unsigned long long* __restrict__ tri_total, uint32_t* __restrict__ err) {
   const uint32_t lane = lane_id();
   const unsigned long long total = spref[m];
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -543,36 +565,33 @@ __global__ void __launch_bounds__(256) k_support_balanced(
       const uint32_t e = window_find(ps, i, m, k, valid);
       const uint32_t last = (uint32_t)min(31ull, kend - 1 - kb);
       const uint32_t e_last = __shfl_sync(kFull, e, last);
-      bool hit = false;
+      uint32_t o = 0, sb = 0, lb = 0, le = 0;
       if (valid) {
-        const uint32_t o = (uint32_t)(k - spref[e]);
+        o = (uint32_t)(k - spref[e]);
         const uint32_t a = __ldg(osrc + e), b = __ldg(ocol + e);
         const uint32_t ab = __ldg(opos + a), ae = __ldg(opos + a + 1);
         const uint32_t bb = __ldg(opos + b), be = __ldg(opos + b + 1);
-        uint32_t ia, ib;
-        if (ae - ab <= be - bb) {
-          ia = ab + o;
-          const uint32_t c = __ldg(ocol + ia);
-          ib = lower_bound_u32(ocol, bb, be, c);
-          hit = ib < be && __ldg(ocol + ib) == c;
-        } else {
-          ib = bb + o;
-          const uint32_t c = __ldg(ocol + ib);
-          ia = lower_bound_u32(ocol, ab, ae, c);
-          hit = ia < ae && __ldg(ocol + ia) == c;
-        }
-        if (hit) {
-          atomicAdd(&es[ia].x, 1);
-          atomicAdd(&es[ib].x, 1);
-          found_total++;
-        }
+        if (ae - ab <= be - bb) { sb = ab; lb = bb; le = be; }
+        else { sb = bb; lb = ab; le = ae; }
+      }
+      uint32_t p = kInvalid;  // position of c in the longer list
+      if (valid) {
+        const uint32_t c = __ldg(ocol + sb + o);
+        const uint32_t q = lower_bound_u32(ocol, lb, le, c);
+        if (q < le && __ldg(ocol + q) == c) p = q;
+      }
+      const bool hit = valid && p != kInvalid;
+      if (hit) {
+        atomicAdd(&es[sb + o].x, 1);
+        atomicAdd(&es[p].x, 1);
+        found_total++;
       }
       // credit e once per run of lanes sharing it
       const unsigned hits = __ballot_sync(kFull, hit);
       const unsigned grp = __match_any_sync(kFull, valid ? e : kInvalid);
       if (valid && lane == (uint32_t)(__ffs(grp) - 1)) {
-        const int c = __popc(grp & hits);
-        if (c) atomicAdd(&es[e].x, c);
+        const int cnt = __popc(grp & hits);
+        if (cnt) atomicAdd(&es[e].x, cnt);
       }
       i = e_last;
     }
@@ -580,6 +599,240 @@ __global__ void __launch_bounds__(256) k_support_balanced(
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) found_total += __shfl_down_sync(kFull, found_total, d);
   if (lane == 0 && found_total) atomicAdd(tri_total, found_total);
+}
+
+// ---------------------------------------------------------------------------
+// Kernel C (vertex form).  Each triangle a < b < c (orientation rank) is found
+// once, from its lowest vertex a: N+(a) is hashed into shared memory, then the
+// out-lists N+(b) of every b in N+(a) are streamed with coalesced loads and
+// probed against the table.  Of the three credits, (a -> b) and (a -> c) land
+// in shared-memory counters for a's out-list, flushed once per vertex; only
+// (b -> c) is a global atomic.  Light vertices (out-degree <= kLightMax) take
+// one warp each; heavier ones one CTA each (k_support_heavy).
+constexpr int kLightMax = 64;
+constexpr int kLightSlots = 128;
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t c, uint32_t shift) {
+  return (c * 0x9E3779B1u) >> shift;
+}
+
+// insert key c -> j (table has >= 2x slots, so a free slot always exists)
+__device__ __forceinline__ void table_insert(uint32_t* keys, uint16_t* vals, uint32_t mask, uint32_t shift,
+                                             uint32_t c, uint32_t j) {
+  uint32_t h = hash_slot(c, shift);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t old = atomicCAS(keys + h, kInvalid, c);
+    if (old == kInvalid) { vals[h] = (uint16_t)j; return; }
+    h = (h + 1) & mask;
+  }
+}
+
+__device__ __forceinline__ uint32_t table_find(const uint32_t* keys, const uint16_t* vals, uint32_t mask,
+                                               uint32_t shift, uint32_t c) {
+  uint32_t h = hash_slot(c, shift);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t k = keys[h];
+    if (k == c) return vals[h];
+    if (k == kInvalid) return kInvalid;
+    h = (h + 1) & mask;
+  }
+  return kInvalid;
+}
+
+__device__ __forceinline__ uint32_t log2_pow2(uint32_t t) { return 31 - __clz(t); }
+
+__global__ void __launch_bounds__(256) k_support_light(const uint32_t* __restrict__ opos,
+                                                       const uint32_t* __restrict__ ocol, uint32_t n,
+                                                       int2* __restrict__ es, unsigned long long* __restrict__ tri_total,
+                                                       uint32_t* __restrict__ heavy_list,
+                                                       uint32_t* __restrict__ heavy_count,
+                                                       uint32_t* __restrict__ vcursor) {
+  __shared__ uint32_t s_key[8][kLightSlots];
+  __shared__ uint16_t s_val[8][kLightSlots];
+  __shared__ uint32_t s_cnt[8][kLightMax];
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  uint32_t* keys = s_key[wib];
+  uint16_t* vals = s_val[wib];
+  uint32_t* cnt = s_cnt[wib];
+  unsigned long long tri = 0;
+  for (;;) {
+    uint32_t v0 = 0;
+    if (lane == 0) v0 = atomicAdd(vcursor, 32u);
+    v0 = __shfl_sync(kFull, v0, 0);
+    if (v0 >= n) break;
+    const uint32_t va = v0 + lane;
+    const uint32_t dv = va < n ? __ldg(opos + va + 1) - __ldg(opos + va) : 0u;
+    const bool heavy = dv > (uint32_t)kLightMax;
+    const unsigned hb = __ballot_sync(kFull, heavy);
+    if (hb) {
+      uint32_t at = 0;
+      if (lane == 0) at = atomicAdd(heavy_count, (uint32_t)__popc(hb));
+      at = __shfl_sync(kFull, at, 0);
+      if (heavy) heavy_list[at + __popc(hb & ((1u << lane) - 1))] = va;
+    }
+    unsigned todo = __ballot_sync(kFull, dv >= 2 && !heavy);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t a = v0 + src;
+      const uint32_t da = __shfl_sync(kFull, dv, src);
+      const uint32_t base = __ldg(opos + a);
+      uint32_t T = 8;
+      while (T < 2 * da) T <<= 1;
+      const uint32_t mask = T - 1, shift = 32 - log2_pow2(T);
+      for (uint32_t s = lane; s < T; s += 32) keys[s] = kInvalid;
+      if (lane < da) cnt[lane] = 0;
+      if (lane + 32 < da) cnt[lane + 32] = 0;
+      __syncwarp();
+      const uint32_t b0 = lane < da ? __ldg(ocol + base + lane) : kInvalid;
+      const uint32_t b1 = lane + 32 < da ? __ldg(ocol + base + lane + 32) : kInvalid;
+      if (b0 != kInvalid) table_insert(keys, vals, mask, shift, b0, lane);
+      if (b1 != kInvalid) table_insert(keys, vals, mask, shift, b1, lane + 32);
+      // out-lists of the b's: start and length, exclusive prefix over lengths
+      const uint32_t p0 = b0 != kInvalid ? __ldg(opos + b0) : 0u;
+      const uint32_t l0 = b0 != kInvalid ? __ldg(opos + b0 + 1) - p0 : 0u;
+      const uint32_t p1 = b1 != kInvalid ? __ldg(opos + b1) : 0u;
+      const uint32_t l1 = b1 != kInvalid ? __ldg(opos + b1 + 1) - p1 : 0u;
+      const uint32_t i0 = (uint32_t)warp_incl_scan(l0), t0 = __shfl_sync(kFull, i0, 31);
+      const uint32_t i1 = (uint32_t)warp_incl_scan(l1) + t0, total = __shfl_sync(kFull, i1, 31);
+      // exclusive starts; entries past the list never match (start = max)
+      const uint32_t x0 = lane < da ? i0 - l0 : kInvalid;
+      const uint32_t x1 = lane + 32 < da ? i1 - l1 : kInvalid;
+      __syncwarp();
+      for (uint32_t f0 = 0; f0 < total; f0 += 32) {
+        const uint32_t f = f0 + lane;
+        // entry owning f: largest index with start <= f, over 64 entries
+        uint32_t t = 0;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+          const uint32_t cand = __shfl_sync(kFull, x0, t + d);
+          if (cand <= f) t += d;
+        }
+        uint32_t u = 0;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+          const uint32_t cand = __shfl_sync(kFull, x1, u + d);
+          if (cand <= f) u += d;
+        }
+        const uint32_t x1_0 = __shfl_sync(kFull, x1, 0);
+        const uint32_t xt = __shfl_sync(kFull, x0, t), pt = __shfl_sync(kFull, p0, t);
+        const uint32_t xu = __shfl_sync(kFull, x1, u), pu = __shfl_sync(kFull, p1, u);
+        const bool hi = x1_0 <= f;  // entry index >= 32
+        const uint32_t i = hi ? 32 + u : t;
+        const uint32_t start = hi ? xu : xt, pos = hi ? pu : pt;
+        bool hit = false;
+        if (f < total) {
+          const uint32_t at = pos + (f - start);
+          const uint32_t c = __ldg(ocol + at);
+          const uint32_t j = table_find(keys, vals, mask, shift, c);
+          if (j != kInvalid) {
+            hit = true;
+            atomicAdd(cnt + j, 1u);    // a -> c
+            atomicAdd(cnt + i, 1u);    // a -> b
+            atomicAdd(&es[at].x, 1);   // b -> c
+          }
+        }
+        tri += hit;
+      }
+      __syncwarp();
+      if (lane < da && cnt[lane]) atomicAdd(&es[base + lane].x, (int)cnt[lane]);
+      if (lane + 32 < da && cnt[lane + 32]) atomicAdd(&es[base + lane + 32].x, (int)cnt[lane + 32]);
+      __syncwarp();
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) tri += __shfl_down_sync(kFull, tri, d);
+  if (lane == 0 && tri) atomicAdd(tri_total, tri);
+}
+
+// Heavy vertices: one CTA each, table of `slots` entries in dynamic shared
+// memory (slots >= 2 * max out-degree), lists of the b's staged in shared memory.
+__global__ void __launch_bounds__(256) k_support_heavy(const uint32_t* __restrict__ opos,
+                                                       const uint32_t* __restrict__ ocol,
+                                                       int2* __restrict__ es, unsigned long long* __restrict__ tri_total,
+                                                       const uint32_t* __restrict__ heavy_list,
+                                                       const uint32_t* __restrict__ heavy_count,
+                                                       uint32_t* __restrict__ hcursor, uint32_t slots,
+                                                       uint32_t max_deg) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* keys = (uint32_t*)smem;                       // slots
+  uint32_t* cnt = keys + slots;                           // max_deg
+  uint32_t* pre = cnt + max_deg;                          // max_deg + 1 exclusive starts
+  uint32_t* bpos = pre + max_deg + 1;                     // max_deg list starts
+  uint16_t* vals = (uint16_t*)(bpos + max_deg);           // slots
+  __shared__ uint32_t s_a, s_sum[32];
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t nheavy = *heavy_count;
+  unsigned long long tri = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t h = atomicAdd(hcursor, 1u);
+      s_a = h < nheavy ? heavy_list[h] : kInvalid;
+    }
+    __syncthreads();
+    const uint32_t a = s_a;
+    if (a == kInvalid) break;
+    const uint32_t base = __ldg(opos + a), d = __ldg(opos + a + 1) - base;
+    uint32_t T = 8;
+    while (T < 2 * d) T <<= 1;
+    const uint32_t mask = T - 1, shift = 32 - log2_pow2(T);
+    for (uint32_t s = threadIdx.x; s < T; s += blockDim.x) keys[s] = kInvalid;
+    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    // insert N+(a), record the b lists, exclusive prefix of their lengths
+    uint32_t carry = 0;
+    for (uint32_t i0 = 0; i0 < d; i0 += blockDim.x) {
+      const uint32_t i = i0 + threadIdx.x;
+      uint32_t len = 0;
+      if (i < d) {
+        const uint32_t b = __ldg(ocol + base + i);
+        table_insert(keys, vals, mask, shift, b, i);
+        const uint32_t pb = __ldg(opos + b);
+        len = __ldg(opos + b + 1) - pb;
+        bpos[i] = pb;
+      }
+      uint32_t total;
+      const uint32_t ex = block_exclusive_scan<uint32_t>(len, s_sum, total);
+      if (i < d) pre[i] = carry + ex;
+      carry += total;
+    }
+    if (threadIdx.x == 0) pre[d] = carry;
+    __syncthreads();
+    const uint32_t total = carry;
+    for (uint32_t f0 = wid * 32; f0 < total; f0 += nw * 32) {
+      const uint32_t f = f0 + lane;
+      if (f < total) {
+        // entry owning f: largest i with pre[i] <= f (entries with no out-list
+        // share their start with the next entry and are skipped)
+        uint32_t lo = 0, hi = d - 1;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi + 1) >> 1;
+          if (pre[mid] <= f) lo = mid; else hi = mid - 1;
+        }
+        const uint32_t at = bpos[lo] + (f - pre[lo]);
+        const uint32_t c = __ldg(ocol + at);
+        const uint32_t j = table_find(keys, vals, mask, shift, c);
+        if (j != kInvalid) {
+          atomicAdd(cnt + j, 1u);
+          atomicAdd(cnt + lo, 1u);
+          atomicAdd(&es[at].x, 1);
+          ++tri;
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x)
+      if (cnt[i]) atomicAdd(&es[base + i].x, (int)cnt[i]);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int dd = 16; dd > 0; dd >>= 1) tri += __shfl_down_sync(kFull, tri, dd);
+  if (lane == 0 && tri) atomicAdd(tri_total, tri);
+}
+
+// dynamic shared memory of k_support_heavy for a given max out-degree
+__host__ __device__ inline size_t heavy_smem_bytes(uint32_t slots, uint32_t max_deg) {
+  return (size_t)slots * 4 + (size_t)max_deg * 4 * 3 + 4 + (size_t)slots * 2;
 }
 
 // ---------------------------------------------------------------------------
@@ -679,10 +932,13 @@ struct WaveArgs {
   uint32_t* err;
 };
 
-// work of pushing edge x (union eid): the shorter working row of its endpoints
-__device__ __forceinline__ uint32_t edge_work(const UnionRegs& U, uint32_t x) {
+// Rows of frontier edge x in the working CSR: {shorter row start, its length,
+// longer row begin, longer row end}.  The length is the edge's work.
+__device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x) {
   const uint32_t u = __ldg(U.osrc + x), v = __ldg(U.ocol + x);
-  return min(deg_of(U.off, u), deg_of(U.off, v));
+  const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
+  const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
+  return (ue - ub <= ve - vb) ? make_uint4(ub, ue - ub, vb, ve) : make_uint4(vb, ve - vb, ub, ue);
 }
 
 // PKT sub-level rule for one triangle (e, f, h) of frontier edge e at level l,
@@ -752,36 +1008,32 @@ struct QueueStart {
   __device__ __forceinline__ unsigned long long operator()(uint32_t x) const { return q[x] >> kEidBits; }
 };
 
-__device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long v) {
-  const uint32_t lane = lane_id();
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const unsigned long long o = __shfl_up_sync(kFull, v, d);
-    if (lane >= (uint32_t)d) v += o;
-  }
-  return v;
-}
-
 // Per-warp staging of frontier pushes in shared memory: entries are gathered
 // across iterations and published with one 64-bit atomic (count and work) per
 // kPushBuf entries, instead of one per iteration on a single hot counter.
 constexpr int kPushBuf = 64;
 constexpr int kWaveThreads = 256;
+#ifndef SPARX_WAVE_MINB
+#define SPARX_WAVE_MINB 6  // resident 256-thread blocks per SM the register budget targets
+#endif
 constexpr int kWaveWarps = kWaveThreads / 32;
 
 struct PushStage {
-  uint2* buf;   // this warp's kPushBuf (edge, work) slots
-  uint32_t n;   // warp-uniform fill
+  uint32_t* eid;  // this warp's kPushBuf staged edges
+  uint4* desc;    // and their row descriptors (desc.y = work)
+  uint32_t n;     // warp-uniform fill
 };
 
 __device__ __forceinline__ void push_flush(PushStage& ps, const Member& M, MemberState* st, uint32_t* err,
-                                           unsigned long long* qnext) {
+                                           unsigned long long* qnext, uint4* qdnext) {
   __syncwarp();
   const uint32_t n = ps.n;
   if (n == 0) return;
   const uint32_t lane = lane_id();
-  const uint2 e0 = lane < n ? ps.buf[lane] : make_uint2(0, 0);
-  const uint2 e1 = lane + 32 < n ? ps.buf[lane + 32] : make_uint2(0, 0);
+  const uint4 d0 = lane < n ? ps.desc[lane] : make_uint4(0, 0, 0, 0);
+  const uint4 d1 = lane + 32 < n ? ps.desc[lane + 32] : make_uint4(0, 0, 0, 0);
+  const uint2 e0 = make_uint2(lane < n ? ps.eid[lane] : 0u, d0.y);
+  const uint2 e1 = make_uint2(lane + 32 < n ? ps.eid[lane + 32] : 0u, d1.y);
   const unsigned long long p0 = warp_incl_scan(e0.y), p1 = warp_incl_scan(e1.y);
   const unsigned long long t0 = __shfl_sync(kFull, p0, 31), t1 = __shfl_sync(kFull, p1, 31);
   unsigned long long old = 0;
@@ -792,13 +1044,20 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const Member& M, Membe
   old = __shfl_sync(kFull, old, 0);
   const unsigned long long pos = old >> kWorkBits, ws = old & kWorkMask;
   if (lane < n) {
-    if (pos + lane < M.m) qnext[M.eb + pos + lane] = ((ws + p0 - e0.y) << kEidBits) | (e0.x - M.eb);
-    else atomicOr(err, kErrCapacity);
+    if (pos + lane < M.m) {
+      qnext[M.eb + pos + lane] = ((ws + p0 - e0.y) << kEidBits) | (e0.x - M.eb);
+      qdnext[M.eb + pos + lane] = d0;
+    } else {
+      atomicOr(err, kErrCapacity);
+    }
   }
   if (lane + 32 < n) {
-    if (pos + 32 + lane < M.m)
+    if (pos + 32 + lane < M.m) {
       qnext[M.eb + pos + 32 + lane] = ((ws + t0 + p1 - e1.y) << kEidBits) | (e1.x - M.eb);
-    else atomicOr(err, kErrCapacity);
+      qdnext[M.eb + pos + 32 + lane] = d1;
+    } else {
+      atomicOr(err, kErrCapacity);
+    }
   }
   ps.n = 0;
   __syncwarp();
@@ -806,16 +1065,17 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const Member& M, Membe
 
 // Queue edge x (union eid) for wave W + 1.  All lanes call it.
 __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, const Member& M, MemberState* st,
-                                          uint32_t* err, unsigned long long* qnext, bool want, uint32_t x,
-                                          uint32_t W) {
+                                          uint32_t* err, unsigned long long* qnext, uint4* qdnext, bool want,
+                                          uint32_t x, uint32_t W) {
   const unsigned bal = __ballot_sync(kFull, want);
   if (!bal) return;
   const uint32_t k = __popc(bal);
-  if (ps.n + k > kPushBuf) push_flush(ps, M, st, err, qnext);
+  if (ps.n + k > kPushBuf) push_flush(ps, M, st, err, qnext, qdnext);
   if (want) {
     U.es[x].y = (int)(W + 1);
     const uint32_t r = __popc(bal & ((1u << lane_id()) - 1));
-    ps.buf[ps.n + r] = make_uint2(x, edge_work(U, x));
+    ps.eid[ps.n + r] = x;
+    ps.desc[ps.n + r] = edge_desc(U, x);
   }
   ps.n += k;
 }
@@ -828,8 +1088,9 @@ __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, con
 //                       <= level -> queued for this level; else kept
 //   frontier element j  element o of the shorter working row of frontier
 //                       edge e, searched in the longer row; a hit is a triangle
-__global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
-  __shared__ uint2 s_push[kWaveWarps][kPushBuf];
+__global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs a) {
+  __shared__ uint4 s_push_desc[kWaveWarps][kPushBuf];
+  __shared__ uint32_t s_push_eid[kWaveWarps][kPushBuf];
   __shared__ uint32_t s_keep[kWaveWarps][kPushBuf];
   const Control* ctl = a.ctl;
   if (ctl->done) return;
@@ -843,8 +1104,8 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
   const UnionRegs U(a.Up);
   unsigned long long ch = total / (nwarps * 4);
   ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
-  uint32_t hits = 0;
-  PushStage ps{s_push[wib], 0};
+  uint32_t hits = 0, n_merge = 0, n_lane = 0, n_chunk = 0;
+  PushStage ps{s_push_eid[wib], s_push_desc[wib], 0};
 
   for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
     const unsigned long long kend = min(c0 + ch, total);
@@ -862,15 +1123,16 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
       MemberState* st = a.st + g;
       const uint32_t phase = st->phase, level = st->level, act_sel = st->act_sel, q_sel = st->q_sel;
       unsigned long long* qnext = q_sel ? U.q0 : U.q1;
+      uint4* qdnext = q_sel ? U.qd0 : U.qd1;
       if (phase == kPhaseProc) {
         const unsigned long long* q = (q_sel ? U.q1 : U.q0) + M.eb;
+        const uint4* qd = (q_sel ? U.qd1 : U.qd0) + M.eb;
         const uint32_t qcount = (uint32_t)(st->curr >> kWorkBits);
         if (qcount == 0) {
           if (lane == 0) atomicOr(a.err, kErrInternal);
           k = seg_end;
           continue;
         }
-        const QueueStart qs{q};
         uint32_t i = last_entry_le(q, 0, qcount - 1, k - mbeg);
         // merge cursor carried across iterations that continue the same edge
         uint32_t m_e = kInvalid, m_next_o = 0, m_cur = 0;
@@ -878,34 +1140,44 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
           const unsigned long long kk = kb + lane;
           const bool valid = kk < seg_end;
           const unsigned long long j = kk - mbeg;
-          const uint32_t x = window_find(qs, i, qcount, j, valid);
+          // the window's entries, loaded once: each lane picks its own by a
+          // shuffle search on the work starts (entries own >= 1 element, so
+          // 32 consecutive elements span at most 32 entries)
+          const unsigned long long qv = (i + lane < qcount) ? q[i + lane] : ~0ull;
+          uint32_t t = 0;
+#pragma unroll
+          for (int d = 16; d > 0; d >>= 1) {
+            const unsigned long long cand = __shfl_sync(kFull, qv, t + d) >> kEidBits;
+            if (cand <= j) t += d;
+          }
+          const unsigned long long ent = __shfl_sync(kFull, qv, t);
+          const uint32_t x = i + t;
           const uint32_t last = (uint32_t)min(31ull, seg_end - 1 - kb);
           const uint32_t x_last = __shfl_sync(kFull, x, last);
-          uint32_t e = 0, o = 0, u = 0, v = 0, sb = 0, slen = 0, lb = 0, le = 0;
+          uint32_t e = 0, o = 0, sb = 0, slen = 0, lb = 0, le = 0;
           if (valid) {
-            const unsigned long long ent = q[x];
             e = M.eb + (uint32_t)(ent & kEidMask);
             o = (uint32_t)(j - (ent >> kEidBits));
-            u = __ldg(U.osrc + e);
-            v = __ldg(U.ocol + e);
-            const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
-            const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
-            if (ue - ub <= ve - vb) { sb = ub; slen = ue - ub; lb = vb; le = ve; }
-            else { sb = vb; slen = ve - vb; lb = ub; le = ue; }
+            const uint4 dsc = qd[x];
+            sb = dsc.x;
+            slen = dsc.y;
+            lb = dsc.z;
+            le = dsc.w;
           }
           // rows may have been compacted since the entry's work was counted
           const bool el = valid && o < slen;
           unsigned long long pr = el ? __ldg(U.row + sb + o) : 0ull;
           const uint32_t w = (uint32_t)pr;
-          uint32_t f = (uint32_t)(pr >> 32), h = 0, p = kInvalid;
-          bool look = el && w != u && w != v && f != kInvalid;
-          // the other edge of the small row: already processed -> no triangle to resolve
+          uint32_t f = (uint32_t)(pr >> 32), h = kInvalid, p = kInvalid;
+          // f == kInvalid: a self-loop entry; f == e: the frontier edge itself
+          bool look = el && f != kInvalid && f != e;
+          // the other edge of the short row: already processed -> nothing to resolve
           int2 es_f = make_int2(0, 0);
           if (look) {
             es_f = U.es[f];
             look = (uint32_t)es_f.y >= W;
           }
-          // lane 0 is always valid: its row bounds decide, so the branch and the
+          // lane 0 is always valid: its rows decide, so the branch and the
           // merge below are warp-uniform
           const uint32_t e0 = __shfl_sync(kFull, e, 0);
           const uint32_t L_beg = __shfl_sync(kFull, lb, 0), L_end = __shfl_sync(kFull, le, 0);
@@ -931,28 +1203,36 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
                 }
                 cur = lo;
               }
-              for (;;) {
+              const uint32_t cap = (L_end - L_beg) / 32 + 2;
+              for (uint32_t it = 0;; ++it) {
+                if (it > cap) {
+                  if (lane == 0) atomicOr(a.err, kErrInternal);
+                  break;
+                }
                 const uint32_t idx = cur + lane;
                 const unsigned long long lp = idx < L_end ? __ldg(U.row + idx) : ~0ull;
                 const uint32_t lv = (uint32_t)lp;
-                uint32_t t = 0;
+                uint32_t tt = 0;
 #pragma unroll
                 for (int d = 16; d > 0; d >>= 1) {
-                  const uint32_t cand = __shfl_sync(kFull, lv, t + d);
-                  if (cand <= w) t += d;
+                  const uint32_t cand = __shfl_sync(kFull, lv, tt + d);
+                  if (cand <= w) tt += d;
                 }
-                const uint32_t lvt = __shfl_sync(kFull, lv, t);
-                const uint32_t ht = (uint32_t)(__shfl_sync(kFull, lp, t) >> 32);
-                if (look && lvt == w) { p = cur + t; h = ht; }
+                const uint32_t lvt = __shfl_sync(kFull, lv, tt);
+                const uint32_t ht = (uint32_t)(__shfl_sync(kFull, lp, tt) >> 32);
+                if (look && lvt == w) { p = cur + tt; h = ht; }
                 const uint32_t adv = __popc(__ballot_sync(kFull, lv <= wmax));
                 cur += adv;
+                ++n_chunk;
                 if (adv < 32) break;
               }
               m_e = e0;
               m_next_o = o0 + 32;
               m_cur = cur;
             }
+            ++n_merge;
           } else {
+            ++n_lane;
             m_e = kInvalid;
             if (look) {
               p = find_in_row(U.row, lb, le, w);
@@ -960,12 +1240,13 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
             }
           }
           bool pf = false, ph = false;
-          if (look && p != kInvalid) {
+          // h == kInvalid: w was the long row's own vertex (a self-loop entry)
+          if (look && p != kInvalid && h != kInvalid) {
             ++hits;
             pkt_rule(U, e, f, es_f, h, level, W, pf, ph);
           }
-          push_edge(ps, U, M, st, a.err, qnext, pf, f, W);
-          push_edge(ps, U, M, st, a.err, qnext, ph, h, W);
+          push_edge(ps, U, M, st, a.err, qnext, qdnext, pf, f, W);
+          push_edge(ps, U, M, st, a.err, qnext, qdnext, ph, h, W);
           i = x_last;
         }
       } else if (phase == kPhaseScan0 || phase == kPhaseScan) {
@@ -991,7 +1272,7 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
               else { keep = true; mn = min(mn, (uint32_t)s); }
             }
           }
-          push_edge(ps, U, M, st, a.err, qnext, queue, e, W);
+          push_edge(ps, U, M, st, a.err, qnext, qdnext, queue, e, W);
           const unsigned kb_bal = __ballot_sync(kFull, keep);
           if (kb_bal) {
             const uint32_t kc = __popc(kb_bal);
@@ -1026,13 +1307,18 @@ __global__ void __launch_bounds__(kWaveThreads, 5) k_wave(WaveArgs a) {
         }
         __syncwarp();
       }
-      push_flush(ps, M, st, a.err, qnext);  // entries belong to this member: publish before moving on
+      push_flush(ps, M, st, a.err, qnext, qdnext);  // entries belong to this member: publish before moving on
       k = seg_end;
     }
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) hits += __shfl_xor_sync(kFull, hits, d);
-  if (lane == 0 && hits) atomicAdd(&a.ctl->hits, (unsigned long long)hits);
+  if (lane == 0) {
+    if (hits) atomicAdd(&a.ctl->hits, (unsigned long long)hits);
+    if (n_merge) atomicAdd(&a.ctl->merge_iters, (unsigned long long)n_merge);
+    if (n_lane) atomicAdd(&a.ctl->lane_iters, (unsigned long long)n_lane);
+    if (n_chunk) atomicAdd(&a.ctl->merge_chunks, (unsigned long long)n_chunk);
+  }
 }
 
 // Working-row compaction (between waves): keep the entries whose edge is not
@@ -1083,6 +1369,23 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
       if (keep) row2[at + __popc(bal & ((1u << lane) - 1))] = pr;
       at += __popc(bal);
     }
+  }
+}
+
+// After a compaction the rows moved: rebuild the descriptors of every queued
+// frontier (block per member).
+__global__ void k_refresh_desc(const Union* __restrict__ Up, const Member* __restrict__ mem,
+                               const MemberState* __restrict__ st, uint32_t G) {
+  const UnionRegs U(Up);
+  for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
+    const MemberState s = st[g];
+    if (s.phase != kPhaseProc) continue;
+    const uint32_t cnt = (uint32_t)(s.curr >> kWorkBits);
+    const Member M = mem[g];
+    const unsigned long long* q = (s.q_sel ? U.q1 : U.q0) + M.eb;
+    uint4* qd = (s.q_sel ? U.qd1 : U.qd0) + M.eb;
+    for (uint32_t x = threadIdx.x; x < cnt; x += blockDim.x)
+      qd[x] = edge_desc(U, M.eb + (uint32_t)(q[x] & kEidMask));
   }
 }
 

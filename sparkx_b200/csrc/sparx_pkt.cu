@@ -63,10 +63,16 @@ struct Counters {  // device scalars
   unsigned long long self_loops;
   unsigned long long tri;
   unsigned long long grand;
+  uint32_t max_dplus;    // largest oriented out-degree
+  uint32_t vcursor;      // vertex-form support: next light vertex batch
+  uint32_t hcursor;      //                      next heavy vertex
+  uint32_t heavy_count;  //                      heavy vertices listed
 };
 
+
+
 struct Layout {
-  size_t off, nbr, row0, dplus, opos, ocol, osrc, es, act0, act1, q0, q1, out, stage0, stage1;
+  size_t off, nbr, row0, dplus, opos, ocol, osrc, es, act0, act1, q0, q1, qd0, qd1, out, stage0, stage1;
   size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
   size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
   size_t total;
@@ -93,6 +99,8 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   L.act1 = take(4 * M);
   L.q0 = take(16 * M + 16);  // q0 and q1 back to back; also the support prefix (M + 1 u64)
   L.q1 = L.q0 + 8 * M;
+  L.qd0 = take(16 * M);
+  L.qd1 = take(16 * M);
   L.out = take(out_bytes);
   L.offA = take(4 * (N + 1));
   L.offB = take(4 * (N + 1));
@@ -277,6 +285,39 @@ void exclusive_scan(F f, unsigned long long count, T* out, T* tiles, T* grand, c
   k_scan_apply<T, F><<<(unsigned)ntiles, kScanThreads, 0, s>>>(f, count, tiles, out);
 }
 
+// Triangle support per oriented edge into es[].x (zeroed by the caller).
+// The vertex form needs a shared-memory table of 2x the largest out-degree;
+// beyond what a CTA can hold the balanced form runs instead.
+constexpr size_t kHeavySmemLimit = 160u << 10;
+
+int launch_support(int sm_count, uint32_t support_kernel, uint32_t n, uint64_t m, uint32_t max_dplus,
+                   const uint32_t* opos, const uint32_t* ocol, const uint32_t* osrc, int2* es,
+                   unsigned long long* spref, unsigned long long* tiles, Counters* cnt, uint32_t* heavy_list,
+                   cudaStream_t s, uint32_t* launches, unsigned long long* support_elements) {
+  if (m == 0) return SPARX_OK;
+  uint32_t slots = 8;
+  while (slots < 2 * max_dplus) slots <<= 1;
+  const size_t hsmem = heavy_smem_bytes(slots, max_dplus);
+  // auto picks the balanced form: on R-MAT-22 it runs in 131 ms against 221 ms
+  // for the vertex form (B200, measured)
+  const bool vertex_form = support_kernel == 2;
+  if (vertex_form && hsmem <= kHeavySmemLimit) {
+    k_support_light<<<sm_count * 8, 256, 0, s>>>(opos, ocol, n, es, &cnt->tri, heavy_list, &cnt->heavy_count,
+                                                 &cnt->vcursor);
+    CU(cudaFuncSetAttribute(k_support_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+    k_support_heavy<<<sm_count * 4, 256, hsmem, s>>>(opos, ocol, es, &cnt->tri, heavy_list, &cnt->heavy_count,
+                                                     &cnt->hcursor, slots, max_dplus);
+    *launches += 2;
+    *support_elements = 0;
+    return SPARX_OK;
+  }
+  exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, tiles, &cnt->grand, s);
+  k_support_balanced<<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri, &cnt->err);
+  *launches += 4;
+  CU(cudaMemcpyAsync(support_elements, spref + m, 8, cudaMemcpyDeviceToHost, s));
+  return SPARX_OK;
+}
+
 __global__ void k_member_edges(Member* mem, uint32_t G, const uint32_t* opos) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
     const uint32_t eb = opos[mem[g].vb];
@@ -408,7 +449,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     if (*herr) { J.err = *herr; return status_from_flags(*herr); }
   }
   // -- orientation (Kernel B) --
-  k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err);
+  k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus);
   exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
   J.launches += 4;
   CU(cudaMemcpyAsync(dmem, J.members.data(), sizeof(Member) * G, cudaMemcpyHostToDevice, s));
@@ -433,13 +474,11 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
 
   // -- support (Kernel C) --
   CU(cudaMemsetAsync(es, 0, 8 * std::max<uint64_t>(m, 1), s));
-  unsigned long long* spref = at<unsigned long long>(E, L.q0);
-  if (m > 0) {
-    exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, at<unsigned long long>(E, L.tiles),
-                                       &cnt->grand, s);
-    k_support_balanced<<<E.sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri);
-    J.launches += 4;
-    CU(cudaMemcpyAsync(&J.support_elements, spref + m, 8, cudaMemcpyDeviceToHost, s));
+  {
+    int rc = launch_support(E.sm_count, O.support_kernel, N, m, hc.max_dplus, opos, ocol, osrc, es,
+                            at<unsigned long long>(E, L.q0), at<unsigned long long>(E, L.tiles), cnt,
+                            at<uint32_t>(E, L.act0), s, &J.launches, &J.support_elements);
+    if (rc) return rc;
   }
   CU(cudaEventRecord(E.tev[3], s));
 
@@ -462,6 +501,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     U.act[1] = at<uint32_t>(E, L.act1);
     U.q[0] = at<unsigned long long>(E, L.q0);
     U.q[1] = at<unsigned long long>(E, L.q1);
+    U.qd[0] = at<uint4>(E, L.qd0);
+    U.qd[1] = at<uint4>(E, L.qd1);
     U.n = N;
     U.m = (uint32_t)m;
     U.width = (uint32_t)W;
@@ -471,7 +512,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaMemsetAsync(at<uint32_t>(E, L.mem_maxsup), 0, 4ull * G, s));
     Control c0{};
     c0.G = G;
-    c0.max_waves = 2ull * m + 64;
+    c0.max_waves = 3ull * m + 64;  // each frontier wave processes >= 1 edge; <= 2 scans per level
     c0.timeout_ns = O.timeout_ms * 1000000ull;
     c0.csr_slots = W;
     c0.compact_min = kCompactMinSlots;
@@ -524,7 +565,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
       k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, es, wa.ctl, off2, row2);
       k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + N, wa.ctl);
-      J.launches += 6;
+      k_refresh_desc<<<std::min<uint32_t>(G, 1024), 256, 0, s>>>(wa.Up, dmem, wa.st, G);
+      J.launches += 7;
       cur_off = off2;
       cur_row = row2;
       next_buf ^= 1;
@@ -592,6 +634,9 @@ void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
     st->peel_scanned = J.ctl.el_scan;
     st->peel_edges = J.ctl.edges_proc;
     st->compactions = J.ctl.compactions;
+    st->merge_iters = J.ctl.merge_iters;
+    st->lane_iters = J.ctl.lane_iters;
+    st->merge_chunks = J.ctl.merge_chunks;
   }
   st->ms_orient = J.ms_orient;
   st->ms_support = J.ms_support;
@@ -1089,6 +1134,8 @@ Layout make_noalloc_layout(uint64_t N, uint64_t W) {
   L.act1 = take(4 * M);
   L.q0 = take(16 * M + 16);
   L.q1 = L.q0 + 8 * M;
+  L.qd0 = take(16 * M);
+  L.qd1 = take(16 * M);
   const uint64_t tiles = (std::max<uint64_t>(N + 1, M + 1) + kScanTile - 1) / kScanTile + 2;
   L.tiles = take(8 * tiles);
   L.ctl = take(sizeof(Control));
@@ -1118,7 +1165,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   const Layout L = make_noalloc_layout(n, width);
   if (L.total > kNoAllocScratchBytes) {
     set_error("graph needs " + std::to_string(L.total) + " bytes of scratch; the allocation-free entry point has " +
-              std::to_string(kNoAllocScratchBytes) + " (about 2.5 M CSR slots); use sparx_pkt_run_device");
+              std::to_string(kNoAllocScratchBytes) + " (about 1.4 M CSR slots); use sparx_pkt_run_device");
     return SPARX_E_TOO_LARGE;
   }
   auto P = [&](size_t off) { return base + off; };
@@ -1148,7 +1195,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   if (hc.err) return status_from_flags(hc.err);
 
   const int vgrid = grid_for((unsigned long long)N * 32, 256, sm * 32);
-  k_orient_count<<<vgrid, 256, 0, s>>>(off, d_nbr, N, dplus, &cnt->self_loops, err);
+  k_orient_count<<<vgrid, 256, 0, s>>>(off, d_nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus);
   exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, (uint32_t*)P(L.tiles), (uint32_t*)&cnt->grand, s);
   uint32_t m32 = 0;
   CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
@@ -1162,11 +1209,12 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   k_orient_reverse<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, row0, err);
 
   CU(cudaMemsetAsync(es, 0, 8 * std::max<uint64_t>(m, 1), s));
-  unsigned long long* spref = (unsigned long long*)P(L.q0);
-  if (m > 0) {
-    exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, (unsigned long long*)P(L.tiles),
-                                       &cnt->grand, s);
-    k_support_balanced<<<sm * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri);
+  {
+    uint32_t launches = 0;
+    unsigned long long elements = 0;
+    rc = launch_support(sm, 0, N, m, hc.max_dplus, opos, ocol, osrc, es, (unsigned long long*)P(L.q0),
+                        (unsigned long long*)P(L.tiles), cnt, (uint32_t*)P(L.act0), s, &launches, &elements);
+    if (rc) return rc;
   }
 
   Union U;
@@ -1180,6 +1228,8 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   U.act[1] = (uint32_t*)P(L.act1);
   U.q[0] = (unsigned long long*)P(L.q0);
   U.q[1] = (unsigned long long*)P(L.q1);
+  U.qd[0] = (uint4*)P(L.qd0);
+  U.qd[1] = (uint4*)P(L.qd1);
   U.n = N;
   U.m = (uint32_t)m;
   U.width = (uint32_t)width;
@@ -1187,7 +1237,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   const Member M0{0, N, 0, (uint32_t)width, 0, (uint32_t)m};
   Control c0{};
   c0.G = 1;
-  c0.max_waves = 2ull * m + 64;
+  c0.max_waves = 3ull * m + 64;
   c0.timeout_ns = kDefaultTimeoutMs * 1000000ull;
   c0.csr_slots = width;
   c0.compact_min = ~0ull;  // no compaction buffers in the fixed scratch

@@ -72,6 +72,7 @@ class _Stats(ctypes.Structure):
         ("support_elements", ctypes.c_uint64), ("peel_elements", ctypes.c_uint64),
         ("peel_hits", ctypes.c_uint64), ("peel_scanned", ctypes.c_uint64),
         ("peel_edges", ctypes.c_uint64), ("compactions", ctypes.c_uint32), ("reserved2", ctypes.c_uint32),
+        ("merge_iters", ctypes.c_uint64), ("lane_iters", ctypes.c_uint64), ("merge_chunks", ctypes.c_uint64),
     ]
 
 
@@ -175,6 +176,9 @@ class PktStats:
     peel_scanned: int = 0
     peel_edges: int = 0
     compactions: int = 0
+    merge_iters: int = 0
+    lane_iters: int = 0
+    merge_chunks: int = 0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "PktStats":

@@ -39,7 +39,7 @@ def test_status_codes_and_defaults(lib):
     o = pkt._Opts()
     assert lib.sparx_pkt_default_opts(ctypes.byref(o)) == 0
     assert o.struct_size == ctypes.sizeof(pkt._Opts) and o.out_bits == 8 and o.device == -1
-    assert ctypes.sizeof(pkt._Stats) == 8 * 6 + 4 * 4 + 8 * 7 + 8 * 5 + 8
+    assert ctypes.sizeof(pkt._Stats) == 8 * 6 + 4 * 4 + 8 * 7 + 8 * 5 + 8 + 8 * 3
 
 
 def test_sm100a_build_flags():

@@ -266,3 +266,16 @@ def test_compaction_in_both_loops(loop):
         t, st = run_pkt(g.offsets, g.neighbours, PktOptions(out_bits=32, loop=loop, timeout_ms=120_000))
         assert truss_sha(t) == fx[name]["modes"]["0"]["truss_sha256"]
         assert st.compactions >= 1
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_support_kernel_forms_agree(kernel):
+    """Balanced (edge) and vertex (shared-memory hash) support forms give the same
+    per-slot support and the same truss numbers."""
+    for g in (gen.rmat(14, 16, seed=2), gen.erdos_renyi(20000, 300000, 9), kn(90), book(300),
+              gen.debruijn(20000, 7, 20, 500, 0.05, 9)):
+        ref = O.triangles(g.offsets, g.neighbours)
+        sup, st = run_triangles(g.offsets, g.neighbours.astype(np.uint64), PktOptions(support_kernel=kernel))
+        assert np.array_equal(sup, ref)
+        t, _ = run_pkt(g.offsets, g.neighbours, PktOptions(out_bits=32, support_kernel=kernel))
+        assert np.array_equal(t, O.pkt(g.offsets, g.neighbours, threads=4))
