@@ -134,6 +134,120 @@ def cpu_pkt_sample(threads: int):
     return g.width / dt, dt, sample
 
 
+def run_mix(args):
+    """Config 4: a sample of the batched mix, batched vs one decomposition per call."""
+    import torch  # noqa: F401  (initialises the device first)
+    from sparkx_b200 import gen
+    from sparkx_b200.pkt import PktOptions, run_batch, run_pkt
+    t0 = time.perf_counter()
+    members = [gen.mix_member(i) for i in range(args.mix_count)]
+    graphs = [gen.mix_graph(m) for m in members]
+    log(f"mix: {len(graphs)} graphs, {sum(g.width for g in graphs)} slots, generated in "
+        f"{time.perf_counter() - t0:.1f}s")
+    opts = PktOptions(out_bits=32)
+    pairs = [(g.offsets, g.neighbours) for g in graphs]
+    run_batch(pairs[: min(8, len(pairs))], opts)  # warm-up
+    run_pkt(*pairs[0], opts)
+    tb = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        res = run_batch(pairs, opts)
+        tb.append(time.perf_counter() - t1)
+    assert all(r[2] == 0 for r in res)
+    tp = []
+    for _ in range(max(1, args.steps // 2)):
+        t1 = time.perf_counter()
+        solo = [run_pkt(o, n, opts)[0] for o, n in pairs]
+        tp.append(time.perf_counter() - t1)
+    same = all(np.array_equal(r[0], s) for r, s in zip(res, solo))
+    small = [i for i, g in enumerate(graphs) if g.n < 10_000]
+    tps = []
+    if small:
+        sp = [pairs[i] for i in small]
+        t1 = time.perf_counter()
+        run_batch(sp, opts)
+        tb_small = time.perf_counter() - t1
+        t1 = time.perf_counter()
+        for o, n in sp:
+            run_pkt(o, n, opts)
+        tps = [tb_small, time.perf_counter() - t1]
+    b = statistics.median(tb)
+    p = statistics.median(tp)
+    out = {"metric": "PKT batched mix graphs/s", "value": len(graphs) / b, "unit": "graphs/s",
+           "per_graph_value": len(graphs) / p, "batched_speedup": p / b, "n_graphs": len(graphs),
+           "slots": sum(g.width for g in graphs), "same_results_as_per_graph": same,
+           "edges_per_s_batched": sum(g.width for g in graphs) / b,
+           "small_graphs": {"count": len(small), "batched_graphs_per_s": len(small) / tps[0] if tps else None,
+                            "per_graph_graphs_per_s": len(small) / tps[1] if tps else None,
+                            "speedup": tps[1] / tps[0] if tps else None},
+           "config": {"workload": f"first {len(graphs)} members of the batched mix (config 4 distribution: "
+                                  "ER or R-MAT, n log-uniform in [1e3,1e6], avg degree uniform [4,64], "
+                                  "seeds 1000+i)"}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """Config 5: Poisson arrivals served with continuous batching vs plain per-graph calls."""
+    import threading as th
+    import torch  # noqa: F401
+    from sparkx_b200 import gen
+    from sparkx_b200.pkt import PktOptions, run_pkt
+    from sparkx_b200.serve import PktServer
+    rng = np.random.default_rng(5)
+    graphs = [gen.mix_graph(gen.mix_member(i)) for i in range(args.mix_count)]
+    if args.tail:
+        ntail = max(1, len(graphs) // 100)
+        for j in range(ntail):
+            graphs.insert(int(rng.integers(0, len(graphs))), gen.rmat(24, 16, seed=100 + j))
+    n = len(graphs)
+    opts = PktOptions(out_bits=32)
+    run_pkt(graphs[0].offsets, graphs[0].neighbours, opts)
+    rows = []
+    for rate in args.rates:
+        gaps = rng.exponential(1.0 / rate, size=n)
+        # served
+        lat = [0.0] * n
+        with PktServer(0, opts) as srv:
+            t0 = time.perf_counter()
+            tickets = []
+            sched = np.cumsum(gaps)
+            for i, g in enumerate(graphs):
+                d = t0 + sched[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets.append((srv.submit(g.offsets, g.neighbours), time.perf_counter()))
+            for i, (t, ts) in enumerate(tickets):
+                r = srv.wait(t, timeout_ms=600_000)
+                assert r.status == 0
+                lat[i] = r.latency_ms
+            span = time.perf_counter() - t0
+        # plain: one call at a time in arrival order (FIFO, single stream)
+        plain_lat = []
+        t0 = time.perf_counter()
+        sched = np.cumsum(gaps)
+        for i, g in enumerate(graphs):
+            arrive = t0 + sched[i]
+            d = arrive - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            run_pkt(g.offsets, g.neighbours, opts)
+            plain_lat.append((time.perf_counter() - arrive) * 1000)
+        span_plain = time.perf_counter() - t0
+        rows.append({"rate_per_s": rate, "served_graphs_per_s": n / span, "plain_graphs_per_s": n / span_plain,
+                     "served_p50_ms": float(np.percentile(lat, 50)), "served_p99_ms": float(np.percentile(lat, 99)),
+                     "plain_p50_ms": float(np.percentile(plain_lat, 50)),
+                     "plain_p99_ms": float(np.percentile(plain_lat, 99))})
+        log(json.dumps(rows[-1]))
+    out = {"metric": "PKT served stream latency/throughput", "n_requests": n, "tail_rmat24": bool(args.tail),
+           "rows": rows,
+           "config": {"workload": f"{n} requests: first {args.mix_count} members of the config-4 mix"
+                                  + (" + 1% R-MAT-24 tail" if args.tail else "") + ", Poisson arrivals",
+                      "budget": "150 GB (4 lanes)"}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def host_threads() -> int:
     return max(1, min(os.cpu_count() or 1, 255))
 
@@ -171,7 +285,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["mix", "serve"], default="rmat22")
+    ap.add_argument("--mix-count", type=int, default=256)
+    ap.add_argument("--rates", type=float, nargs="*", default=[50.0, 200.0, 1000.0])
+    ap.add_argument("--tail", action="store_true", help="serve: add the 1% R-MAT-24 tail")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -187,6 +304,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "mix":
+        return run_mix(args)
+    if args.workload == "serve":
+        return run_serve(args)
 
     import torch
     from sparkx_b200 import pkt

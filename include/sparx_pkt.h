@@ -174,6 +174,33 @@ typedef struct sparx_graph_view {
 int sparx_pkt_run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
                         const sparx_pkt_opts* opts, int* status_out, sparx_pkt_stats* stats_out);
 
+/* ---- serving: continuous batching ------------------------------------ */
+typedef struct sparx_server sparx_server;
+
+/* Create a server on opts->device with an HBM budget (0 = 150 GB, capped at the
+ * device's free memory).  The budget is split over 4 execution lanes; a request
+ * needing more than one lane's share completes with SPARX_E_OOM.  Requests stay
+ * addressable by ticket until sparx_server_destroy. */
+int sparx_server_create(sparx_server** out, uint64_t hbm_budget_bytes, const sparx_pkt_opts* opts);
+
+/* Queue a decomposition; the arrays must stay valid until sparx_server_poll
+ * reports it done.  *ticket identifies the request. */
+int sparx_server_submit(sparx_server* s, const sparx_graph_view* graph, uint64_t* ticket);
+
+/* Non-blocking: *done = 1 once finished; *status is that request's status. */
+int sparx_server_poll(sparx_server* s, uint64_t ticket, int* done, int* status,
+                      sparx_pkt_stats* stats);
+
+/* Block until the request finishes (timeout_ms 0 = forever). */
+int sparx_server_wait(sparx_server* s, uint64_t ticket, uint64_t timeout_ms, int* status,
+                      sparx_pkt_stats* stats);
+
+/* Cancel a queued (not yet admitted) request. */
+int sparx_server_cancel(sparx_server* s, uint64_t ticket);
+
+/* Drain and free. */
+int sparx_server_destroy(sparx_server* s);
+
 #ifdef __cplusplus
 }
 #endif

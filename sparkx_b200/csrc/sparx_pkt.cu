@@ -959,6 +959,143 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
   return first_fail;
 }
 
+// ---------------------------------------------------------------------------
+// Serving: continuous batching over execution lanes.  Each lane is a private
+// engine (stream, workspace, staging, cached peel graph).  An idle lane takes
+// every queued request that fits its share of the HBM budget (FIFO), packs
+// them into one union and runs it; requests that arrive while other lanes are
+// busy start on the next free lane at once, so their work overlaps on the
+// device with the unions already running.
+
+constexpr int kServerLanes = 4;
+constexpr size_t kServerMaxMembers = 4096;
+
+struct ServerReq {
+  uint64_t ticket = 0;
+  HostMember h;
+  int status = SPARX_OK;
+  bool running = false, done = false, cancelled = false;
+  sparx_pkt_stats st{};
+  std::chrono::steady_clock::time_point t_submit, t_start, t_done;
+};
+
+void engine_release(Engine* E) {
+  if (!E) return;
+  cudaSetDevice(E->device);
+  if (E->stream) cudaStreamSynchronize(E->stream);
+  if (E->peel.exec) { cudaGraphExecDestroy(E->peel.exec); cudaGraphDestroy(E->peel.graph); }
+  if (E->ws) cudaFree(E->ws);
+  for (int i = 0; i < 2; ++i) {
+    if (E->pinned[i]) cudaFreeHost(E->pinned[i]);
+    if (E->pin_ev[i]) cudaEventDestroy(E->pin_ev[i]);
+  }
+  for (auto& e : E->tev) if (e) cudaEventDestroy(e);
+  if (E->pinned_small) cudaFreeHost(E->pinned_small);
+  if (E->stream) cudaStreamDestroy(E->stream);
+  if (E->capture) cudaStreamDestroy(E->capture);
+  delete E;
+}
+
+}  // namespace
+
+struct sparx_server {
+  int device = 0;
+  Opts O;
+  uint64_t lane_budget = 0;
+  std::vector<Engine*> lanes;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ServerReq*> queue;
+  std::unordered_map<uint64_t, ServerReq*> reqs;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+};
+
+namespace {
+
+void server_finish(sparx_server* S, ServerReq* r, int status) {
+  r->status = status;
+  r->done = true;
+  r->running = false;
+  r->t_done = std::chrono::steady_clock::now();
+  r->st.ms_total = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+  (void)S;
+}
+
+void server_worker(sparx_server* S, int lane) {
+  Engine& E = *S->lanes[lane];
+  cudaSetDevice(S->device);
+  const size_t esz = S->O.out_bits / 8;
+  for (;;) {
+    std::vector<ServerReq*> batch;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
+      if (S->queue.empty()) {
+        if (S->stop) return;
+        continue;
+      }
+      uint64_t N = 0, W = 0;
+      while (!S->queue.empty() && batch.size() < kServerMaxMembers) {
+        ServerReq* r = S->queue.front();
+        const uint64_t N2 = N + r->h.n, W2 = W + r->h.w;
+        const size_t bytes = make_layout(N2, W2, (uint32_t)batch.size() + 1, true, esz * W2).total;
+        const bool fits = bytes <= S->lane_budget && N2 < 0xFFFFFFFFull && W2 < 0xFFFFFFFFull;
+        if (!fits) {
+          if (batch.empty()) {  // never fits a lane on its own
+            S->queue.pop_front();
+            server_finish(S, r, SPARX_E_OOM);
+            S->cv_done.notify_all();
+            continue;
+          }
+          break;
+        }
+        S->queue.pop_front();
+        r->running = true;
+        r->t_start = std::chrono::steady_clock::now();
+        batch.push_back(r);
+        N = N2;
+        W = W2;
+      }
+    }
+    if (batch.empty()) continue;
+    // host checks, then one union for the valid requests
+    std::vector<HostMember> hm;
+    std::vector<size_t> which;
+    std::vector<int> status(batch.size(), SPARX_OK);
+    for (size_t i = 0; i < batch.size(); ++i) {
+      HostMember h = batch[i]->h;
+      status[i] = host_validate(h);
+      if (status[i] == SPARX_OK && h.w / 2 > kEidMask) status[i] = SPARX_E_TOO_LARGE;
+      if (status[i] == SPARX_OK) {
+        h.index = hm.size();
+        hm.push_back(h);
+        which.push_back(i);
+      }
+    }
+    std::vector<int> st2(hm.size(), SPARX_OK);
+    std::vector<sparx_pkt_stats> stats(hm.size());
+    int first_fail = SPARX_OK;
+    if (!hm.empty()) run_batch_union(E, hm, S->O, st2.data(), stats.data(), &first_fail);
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      for (size_t k = 0; k < which.size(); ++k) {
+        status[which[k]] = st2[k];
+        batch[which[k]]->st = stats[k];
+      }
+      for (size_t i = 0; i < batch.size(); ++i) server_finish(S, batch[i], status[i]);
+    }
+    S->cv_done.notify_all();
+  }
+}
+
+int server_result(ServerReq* r, int* status, sparx_pkt_stats* stats) {
+  if (status) *status = r->status;
+  if (stats) *stats = r->st;
+  return SPARX_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -967,6 +1104,125 @@ int sparx_pkt_run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t
                         const sparx_pkt_opts* opts, int* status_out, sparx_pkt_stats* stats_out) {
   return run_batch(graphs, count, hbm_budget_bytes, opts, status_out, stats_out);
 }
+
+int sparx_server_create(sparx_server** out, uint64_t hbm_budget_bytes, const sparx_pkt_opts* opts) {
+  g_last_error.clear();
+  if (!out) { set_error("null server pointer"); return SPARX_E_ARG; }
+  Opts O;
+  int rc = read_opts(opts, &O);
+  if (rc) return rc;
+  int device = O.device;
+  if (device < 0) CU(cudaGetDevice(&device));
+  CU(cudaSetDevice(device));
+  if (!hbm_budget_bytes) hbm_budget_bytes = 150ull << 30;
+  size_t free_b = 0, total_b = 0;
+  CU(cudaMemGetInfo(&free_b, &total_b));
+  const uint64_t usable = free_b > (2ull << 30) ? free_b - (2ull << 30) : free_b / 2;
+  const uint64_t budget = std::min<uint64_t>(hbm_budget_bytes, usable);
+  auto* S = new sparx_server();
+  S->device = device;
+  S->O = O;
+  S->lane_budget = budget / kServerLanes;
+  for (int i = 0; i < kServerLanes; ++i) {
+    Engine* E = new Engine();
+    rc = engine_init(*E, device);
+    if (rc) {
+      engine_release(E);
+      for (Engine* L : S->lanes) engine_release(L);
+      delete S;
+      return rc;
+    }
+    S->lanes.push_back(E);
+  }
+  for (int i = 0; i < kServerLanes; ++i) S->workers.emplace_back(server_worker, S, i);
+  *out = S;
+  return SPARX_OK;
+}
+
+int sparx_server_submit(sparx_server* S, const sparx_graph_view* v, uint64_t* ticket) {
+  g_last_error.clear();
+  if (!S || !v || !ticket) { set_error("null argument"); return SPARX_E_ARG; }
+  if (!v->offsets || v->n_plus_1 < 1 || (v->width && (!v->neighbours || !v->truss_out)) ||
+      (v->neighbour_bits != 32 && v->neighbour_bits != 64)) {
+    set_error("bad graph view");
+    return SPARX_E_ARG;
+  }
+  int rc = check_dims(v->n_plus_1, v->width);
+  if (rc) return rc;
+  auto* r = new ServerReq();
+  r->h.off = v->offsets;
+  r->h.n = v->n_plus_1 - 1;
+  r->h.nbr = v->neighbours;
+  r->h.bits = v->neighbour_bits == 32 ? 32 : 64;
+  r->h.w = v->width;
+  r->h.out = v->truss_out;
+  r->t_submit = std::chrono::steady_clock::now();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) { delete r; set_error("server is shutting down"); return SPARX_E_ARG; }
+    r->ticket = S->next_ticket++;
+    S->reqs[r->ticket] = r;
+    S->queue.push_back(r);
+  }
+  S->cv_work.notify_one();
+  *ticket = r->ticket;
+  return SPARX_OK;
+}
+
+int sparx_server_poll(sparx_server* S, uint64_t ticket, int* done, int* status, sparx_pkt_stats* stats) {
+  if (!S || !done) return SPARX_E_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(ticket);
+  if (it == S->reqs.end()) return SPARX_E_NOT_FOUND;
+  *done = it->second->done ? 1 : 0;
+  if (it->second->done) server_result(it->second, status, stats);
+  return SPARX_OK;
+}
+
+int sparx_server_wait(sparx_server* S, uint64_t ticket, uint64_t timeout_ms, int* status, sparx_pkt_stats* stats) {
+  if (!S) return SPARX_E_ARG;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(ticket);
+  if (it == S->reqs.end()) return SPARX_E_NOT_FOUND;
+  ServerReq* r = it->second;
+  auto pred = [&] { return r->done; };
+  if (timeout_ms) {
+    if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) return SPARX_E_TIMEOUT;
+  } else {
+    S->cv_done.wait(lk, pred);
+  }
+  return server_result(r, status, stats);
+}
+
+int sparx_server_cancel(sparx_server* S, uint64_t ticket) {
+  if (!S) return SPARX_E_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(ticket);
+  if (it == S->reqs.end()) return SPARX_E_NOT_FOUND;
+  ServerReq* r = it->second;
+  if (r->running || r->done) { set_error("request already admitted"); return SPARX_E_ARG; }
+  for (auto q = S->queue.begin(); q != S->queue.end(); ++q)
+    if (*q == r) { S->queue.erase(q); break; }
+  r->cancelled = true;
+  server_finish(S, r, SPARX_E_CANCELLED);
+  S->cv_done.notify_all();
+  return SPARX_OK;
+}
+
+int sparx_server_destroy(sparx_server* S) {
+  if (!S) return SPARX_E_ARG;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv_work.notify_all();
+  for (auto& t : S->workers) t.join();
+  for (Engine* E : S->lanes) engine_release(E);
+  for (auto& kv : S->reqs) delete kv.second;
+  delete S;
+  return SPARX_OK;
+}
+
 
 int sparx_pkt_default_opts(sparx_pkt_opts* o) {
   if (!o) return SPARX_E_ARG;

@@ -1,0 +1,75 @@
+"""Continuous-batching service: every request's result equals its solo
+decomposition (and the oracle), whatever else is in flight."""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import kn, random_graph
+from oracle import oracle as O
+from sparkx_b200 import gen
+import sparkx_b200.pkt as P
+from sparkx_b200.serve import PktServer
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _engine():
+    import torch
+    assert torch.cuda.is_available(), "needs a CUDA device"
+    from sparkx_b200 import build
+    build.build_engine()
+
+
+def workload():
+    rng = np.random.default_rng(23)
+    gs = [random_graph(rng, n_max=60) for _ in range(25)]
+    gs += [gen.mix_graph(gen.mix_member(i)) for i in range(20) if gen.mix_member(i).n < 40_000]
+    gs += [gen.rmat(13, 16, seed=3), gen.rmat(14, 16, seed=4), kn(40), gen.from_edges(5, [])]
+    return gs
+
+
+def test_alone_equals_in_mix():
+    gs = workload()
+    solo = [P.run_pkt(g.offsets, g.neighbours, P.PktOptions(out_bits=32))[0] for g in gs]
+    with PktServer(8 << 30) as srv:
+        tickets = [srv.submit(g.offsets, g.neighbours) for g in gs]
+        res = [srv.wait(t, timeout_ms=120_000) for t in tickets]
+    for g, r, s in zip(gs, res, solo):
+        assert r.status == P.OK
+        assert np.array_equal(r.truss, s)
+        assert r.latency_ms > 0
+    for g, r in list(zip(gs, res))[:12]:
+        assert np.array_equal(r.truss, O.pkt(g.offsets, g.neighbours, threads=2))
+
+
+def test_staggered_arrivals_overlap():
+    gs = workload()
+    with PktServer(8 << 30) as srv:
+        first = [srv.submit(g.offsets, g.neighbours) for g in gs[:10]]
+        time.sleep(0.01)
+        second = [srv.submit(g.offsets, g.neighbours) for g in gs[10:]]
+        out = {t: srv.wait(t, timeout_ms=120_000) for t in first + second}
+    for g, t in zip(gs, first + second):
+        assert out[t].status == P.OK
+        assert np.array_equal(out[t].truss, P.run_pkt(g.offsets, g.neighbours, P.PktOptions(out_bits=32))[0])
+
+
+def test_errors_cancel_and_budget():
+    good = gen.rmat(12, 16, seed=5)
+    bad = (np.array([0, 1, 3, 4, 4], np.uint64), np.array([1, 0, 2, 3], np.uint32))
+    with PktServer(1 << 30) as srv:
+        tb = srv.submit(*bad)
+        tg = [srv.submit(good.offsets, good.neighbours) for _ in range(30)]
+        cancelled = srv.cancel(tg[-1])
+        rb = srv.wait(tb, timeout_ms=60_000)
+        assert rb.status == P.E_INVALID_CSR
+        for t in tg[:-1]:
+            r = srv.wait(t, timeout_ms=60_000)
+            assert r.status == P.OK and np.array_equal(r.truss, O.pkt(good.offsets, good.neighbours))
+        last = srv.wait(tg[-1], timeout_ms=60_000)
+        assert last.status == (P.E_CANCELLED if cancelled else P.OK)
+        big = gen.rmat(20, 16, seed=1)  # needs more than a quarter of a 1 GiB budget
+        r = srv.wait(srv.submit(big.offsets, big.neighbours), timeout_ms=60_000)
+        assert r.status == P.E_OOM
