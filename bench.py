@@ -342,7 +342,8 @@ def main():
         for _ in range(args.warmup + args.steps):
             st = step()
         torch.cuda.synchronize(dev)
-        print(json.dumps({"profile": args.workload, "waves": st.waves, "ms_support": st.ms_support,
+        print(json.dumps({"profile": args.workload, "waves": st.waves, "ms_total": st.ms_total,
+                          "ms_orient": st.ms_orient, "ms_support": st.ms_support,
                           "ms_peel": st.ms_peel, "launches": st.launches, "peel_elements": st.peel_elements,
                           "peel_hits": st.peel_hits, "peel_scanned": st.peel_scanned,
                           "compactions": st.compactions, "merge_iters": st.merge_iters,

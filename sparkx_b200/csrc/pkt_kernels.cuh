@@ -129,6 +129,10 @@ struct Control {
   unsigned long long merge_iters; // warp iterations resolved by the row merge
   unsigned long long lane_iters;  // warp iterations resolved by per-lane searches
   unsigned long long merge_chunks;// 32-entry chunks of longer rows read by merges
+  // optional wave trace: per planned wave {start time (ns), work, members in
+  // a frontier step, members in a scan}; nullptr = off
+  ulonglong4* trace;
+  unsigned long long trace_cap;
 };
 
 enum : uint32_t { kExitNone = 0, kExitDone = 1, kExitCompact = 2, kExitError = 3 };
@@ -170,9 +174,10 @@ __device__ __forceinline__ uint32_t find_in_row(const unsigned long long* __rest
   for (int it = 0; it < 3 && hi - lo > 48; ++it) {
     const uint32_t a = (uint32_t)__ldg(row + lo), b = (uint32_t)__ldg(row + hi - 1);
     if (w < a || w > b) return kInvalid;
-    // g in [lo, hi - 1] because w - a <= b - a
-    const uint32_t g =
-        lo + (uint32_t)(((unsigned long long)(w - a) * (hi - 1 - lo)) / ((unsigned long long)(b - a) + 1));
+    // fraction in [0, 1); the clamp keeps g in [lo, hi - 1] whatever the rounding
+    const float frac = __fdividef((float)(w - a), (float)(b - a) + 1.0f);
+    const uint32_t span = hi - 1 - lo;
+    const uint32_t g = lo + min(span, (uint32_t)(frac * (float)span));
     const uint32_t x = (uint32_t)__ldg(row + g);
     if (x == w) return g;
     if (x < w) lo = g + 1; else hi = g;
@@ -185,25 +190,63 @@ __device__ __forceinline__ uint32_t find_in_row(const unsigned long long* __rest
   return (lo < end && (uint32_t)__ldg(row + lo) == w) ? lo : kInvalid;
 }
 
-// largest i in [lo, hi] with pref[i] <= k (pref non-decreasing, pref[lo] <= k)
-__device__ __forceinline__ uint32_t last_le_u64(const unsigned long long* __restrict__ pref,
-                                                uint32_t lo, uint32_t hi, unsigned long long k) {
-  while (lo < hi) {
-    uint32_t mid = lo + ((hi - lo + 1) >> 1);
-    if (pref[mid] <= k) lo = mid; else hi = mid - 1;
+// Warp-cooperative searches over a non-decreasing key(x).  Each step gathers
+// 32 evenly spaced keys with one load per lane and keeps the stretch between
+// the two samples that bracket the target, so a span of n entries costs
+// ceil(log32 n) + 1 dependent gathers instead of log2 n dependent loads.  All
+// lanes must call them with the same arguments.
+
+// largest x in [lo, hi] with key(x) <= t; requires key(lo) <= t
+template <class KeyF>
+__device__ __forceinline__ uint32_t warp_last_le(const KeyF& key, uint32_t lo, uint32_t hi,
+                                                 unsigned long long t) {
+  const uint32_t lane = lane_id();
+  while (hi - lo >= 32) {
+    const uint32_t step = (hi - lo) / 32 + 1;
+    const unsigned long long s = (unsigned long long)lo + (unsigned long long)lane * step;
+    const bool le = s <= hi && key((uint32_t)s) <= t;
+    const uint32_t b = __ballot_sync(kFull, le) | 1u;  // key(lo) <= t
+    const uint32_t tl = 31 - __clz(b);
+    lo += tl * step;
+    hi = min(hi, lo + step - 1);
   }
-  return lo;
+  const bool le = lo + lane <= hi && key(lo + lane) <= t;
+  const uint32_t b = __ballot_sync(kFull, le) | 1u;
+  return lo + 31 - __clz(b);
 }
 
-// largest i in [lo, hi] with (q[i] >> 28) <= k
-__device__ __forceinline__ uint32_t last_entry_le(const unsigned long long* __restrict__ q,
-                                                  uint32_t lo, uint32_t hi, unsigned long long k) {
-  while (lo < hi) {
-    uint32_t mid = lo + ((hi - lo + 1) >> 1);
-    if ((q[mid] >> kEidBits) <= k) lo = mid; else hi = mid - 1;
+// first x in [lo, hi) with key(x) >= t, or hi
+template <class KeyF>
+__device__ __forceinline__ uint32_t warp_lower_bound(const KeyF& key, uint32_t lo, uint32_t hi,
+                                                     unsigned long long t) {
+  const uint32_t lane = lane_id();
+  while (hi - lo > 32) {
+    const uint32_t step = (hi - lo + 31) / 32;
+    const unsigned long long s = (unsigned long long)lo + (unsigned long long)lane * step;
+    const bool lt = s < hi && key((uint32_t)s) < t;
+    const uint32_t b = __ballot_sync(kFull, lt);
+    if (b == 0) return lo;
+    const uint32_t tl = 31 - __clz(b);
+    // key(lo + tl*step) < t <= key(lo + (tl+1)*step) (or past hi)
+    const uint32_t nlo = lo + tl * step + 1;
+    hi = min(hi, lo + (tl + 1) * step);
+    lo = nlo;
   }
-  return lo;
+  const bool lt = lo + lane < hi && key(lo + lane) < t;
+  return lo + __popc(__ballot_sync(kFull, lt));
 }
+
+struct PrefKey {
+  const unsigned long long* p;
+  __device__ __forceinline__ unsigned long long operator()(uint32_t x) const { return p[x]; }
+};
+
+struct RowIdKey {
+  const unsigned long long* row;
+  __device__ __forceinline__ unsigned long long operator()(uint32_t x) const {
+    return (uint32_t)__ldg(row + x);
+  }
+};
 
 __device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long v) {
   const uint32_t lane = lane_id();
@@ -213,39 +256,6 @@ __device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long 
     if (lane >= (uint32_t)d) v += o;
   }
   return v;
-}
-
-// Segmented inclusive warp scan; segments are runs of equal `key`, which is
-// non-decreasing across lanes.
-__device__ __forceinline__ void seg_scan(uint32_t key, unsigned long long& v, uint32_t& c) {
-  const uint32_t lane = lane_id();
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    unsigned long long ov = __shfl_up_sync(kFull, v, d);
-    uint32_t oc = __shfl_up_sync(kFull, c, d);
-    uint32_t ok = __shfl_up_sync(kFull, key, d);
-    if (lane >= (uint32_t)d && ok == key) { v += ov; c += oc; }
-  }
-}
-
-__device__ __forceinline__ void seg_min(uint32_t key, uint32_t& v) {
-  const uint32_t lane = lane_id();
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    uint32_t ov = __shfl_up_sync(kFull, v, d);
-    uint32_t ok = __shfl_up_sync(kFull, key, d);
-    if (lane >= (uint32_t)d && ok == key) v = min(v, ov);
-  }
-}
-
-__device__ __forceinline__ int seg_tail(uint32_t key) {
-  unsigned grp = __match_any_sync(kFull, key);
-  return 31 - __clz(grp);
-}
-
-__device__ __forceinline__ int seg_head(uint32_t key) {
-  unsigned grp = __match_any_sync(kFull, key);
-  return __ffs(grp) - 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -558,7 +568,7 @@ __global__ void __launch_bounds__(256) k_support_balanced(
   unsigned long long found_total = 0;
   for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
     const unsigned long long kend = min(c0 + ch, total);
-    uint32_t i = last_le_u64(spref, 0, m - 1, c0);
+    uint32_t i = warp_last_le(PrefKey{spref}, 0, m - 1, c0);
     for (unsigned long long kb = c0; kb < kend; kb += 32) {
       const unsigned long long k = kb + lane;
       const bool valid = k < kend;
@@ -1008,33 +1018,38 @@ struct QueueStart {
   __device__ __forceinline__ unsigned long long operator()(uint32_t x) const { return q[x] >> kEidBits; }
 };
 
-// Per-warp staging of frontier pushes in shared memory: entries are gathered
+// Per-warp staging of frontier pushes in shared memory: edge ids are gathered
 // across iterations and published with one 64-bit atomic (count and work) per
-// kPushBuf entries, instead of one per iteration on a single hot counter.
+// kPushBuf entries, instead of one per iteration on a single hot counter.  The
+// row descriptors of the staged edges are looked up at publication, all lanes
+// at once, so those dependent loads stay off the per-iteration path.
 constexpr int kPushBuf = 64;
 constexpr int kWaveThreads = 256;
 #ifndef SPARX_WAVE_MINB
 #define SPARX_WAVE_MINB 6  // resident 256-thread blocks per SM the register budget targets
 #endif
 constexpr int kWaveWarps = kWaveThreads / 32;
+#ifndef SPARX_MERGE_CHUNKS
+#define SPARX_MERGE_CHUNKS 2  // long-row chunks of 32 entries loaded per merge round
+#endif
+constexpr int kMergeChunks = SPARX_MERGE_CHUNKS;
 
 struct PushStage {
   uint32_t* eid;  // this warp's kPushBuf staged edges
-  uint4* desc;    // and their row descriptors (desc.y = work)
   uint32_t n;     // warp-uniform fill
 };
 
-__device__ __forceinline__ void push_flush(PushStage& ps, const Member& M, MemberState* st, uint32_t* err,
-                                           unsigned long long* qnext, uint4* qdnext) {
+__device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, const Member& M,
+                                           MemberState* st, uint32_t* err, unsigned long long* qnext,
+                                           uint4* qdnext) {
   __syncwarp();
   const uint32_t n = ps.n;
   if (n == 0) return;
   const uint32_t lane = lane_id();
-  const uint4 d0 = lane < n ? ps.desc[lane] : make_uint4(0, 0, 0, 0);
-  const uint4 d1 = lane + 32 < n ? ps.desc[lane + 32] : make_uint4(0, 0, 0, 0);
-  const uint2 e0 = make_uint2(lane < n ? ps.eid[lane] : 0u, d0.y);
-  const uint2 e1 = make_uint2(lane + 32 < n ? ps.eid[lane + 32] : 0u, d1.y);
-  const unsigned long long p0 = warp_incl_scan(e0.y), p1 = warp_incl_scan(e1.y);
+  const uint32_t x0 = lane < n ? ps.eid[lane] : 0u, x1 = lane + 32 < n ? ps.eid[lane + 32] : 0u;
+  const uint4 d0 = lane < n ? edge_desc(U, x0) : make_uint4(0, 0, 0, 0);
+  const uint4 d1 = lane + 32 < n ? edge_desc(U, x1) : make_uint4(0, 0, 0, 0);
+  const unsigned long long p0 = warp_incl_scan(d0.y), p1 = warp_incl_scan(d1.y);
   const unsigned long long t0 = __shfl_sync(kFull, p0, 31), t1 = __shfl_sync(kFull, p1, 31);
   unsigned long long old = 0;
   if (lane == 0) {
@@ -1045,7 +1060,7 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const Member& M, Membe
   const unsigned long long pos = old >> kWorkBits, ws = old & kWorkMask;
   if (lane < n) {
     if (pos + lane < M.m) {
-      qnext[M.eb + pos + lane] = ((ws + p0 - e0.y) << kEidBits) | (e0.x - M.eb);
+      qnext[M.eb + pos + lane] = ((ws + p0 - d0.y) << kEidBits) | (x0 - M.eb);
       qdnext[M.eb + pos + lane] = d0;
     } else {
       atomicOr(err, kErrCapacity);
@@ -1053,7 +1068,7 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const Member& M, Membe
   }
   if (lane + 32 < n) {
     if (pos + 32 + lane < M.m) {
-      qnext[M.eb + pos + 32 + lane] = ((ws + t0 + p1 - e1.y) << kEidBits) | (e1.x - M.eb);
+      qnext[M.eb + pos + 32 + lane] = ((ws + t0 + p1 - d1.y) << kEidBits) | (x1 - M.eb);
       qdnext[M.eb + pos + 32 + lane] = d1;
     } else {
       atomicOr(err, kErrCapacity);
@@ -1070,12 +1085,10 @@ __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, con
   const unsigned bal = __ballot_sync(kFull, want);
   if (!bal) return;
   const uint32_t k = __popc(bal);
-  if (ps.n + k > kPushBuf) push_flush(ps, M, st, err, qnext, qdnext);
+  if (ps.n + k > kPushBuf) push_flush(ps, U, M, st, err, qnext, qdnext);
   if (want) {
     U.es[x].y = (int)(W + 1);
-    const uint32_t r = __popc(bal & ((1u << lane_id()) - 1));
-    ps.eid[ps.n + r] = x;
-    ps.desc[ps.n + r] = edge_desc(U, x);
+    ps.eid[ps.n + __popc(bal & ((1u << lane_id()) - 1))] = x;
   }
   ps.n += k;
 }
@@ -1089,7 +1102,6 @@ __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, con
 //   frontier element j  element o of the shorter working row of frontier
 //                       edge e, searched in the longer row; a hit is a triangle
 __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs a) {
-  __shared__ uint4 s_push_desc[kWaveWarps][kPushBuf];
   __shared__ uint32_t s_push_eid[kWaveWarps][kPushBuf];
   __shared__ uint32_t s_keep[kWaveWarps][kPushBuf];
   const Control* ctl = a.ctl;
@@ -1102,15 +1114,15 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   const UnionRegs U(a.Up);
-  unsigned long long ch = total / (nwarps * 4);
+  unsigned long long ch = total / (nwarps * 2);
   ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
   uint32_t hits = 0, n_merge = 0, n_lane = 0, n_chunk = 0;
-  PushStage ps{s_push_eid[wib], s_push_desc[wib], 0};
+  PushStage ps{s_push_eid[wib], 0};
 
   for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
     const unsigned long long kend = min(c0 + ch, total);
     unsigned long long k = c0;
-    uint32_t g = G > 1 ? last_le_u64(a.wpref, 0, G - 1, k) : 0;
+    uint32_t g = G > 1 ? warp_last_le(PrefKey{a.wpref}, 0, G - 1, k) : 0;
     while (k < kend) {
       while (g + 1 < G && a.wpref[g + 1] <= k) ++g;
       const unsigned long long mbeg = a.wpref[g];
@@ -1133,7 +1145,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           k = seg_end;
           continue;
         }
-        uint32_t i = last_entry_le(q, 0, qcount - 1, k - mbeg);
+        uint32_t i = warp_last_le(QueueStart{q}, 0, qcount - 1, k - mbeg);
         // merge cursor carried across iterations that continue the same edge
         uint32_t m_e = kInvalid, m_next_o = 0, m_cur = 0;
         for (unsigned long long kb = k; kb < seg_end; kb += 32) {
@@ -1196,35 +1208,41 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
                 cur = m_cur;
               } else {
                 const uint32_t wmin = __shfl_sync(kFull, w, __ffs(elb) - 1);
-                uint32_t lo = L_beg, hi = L_end;
-                while (lo < hi) {
-                  const uint32_t mid = lo + ((hi - lo) >> 1);
-                  if ((uint32_t)__ldg(U.row + mid) < wmin) lo = mid + 1; else hi = mid;
-                }
-                cur = lo;
+                cur = warp_lower_bound(RowIdKey{U.row}, L_beg, L_end, wmin);
               }
+              // kMergeChunks chunks are loaded per round, so most rows cost
+              // one dependent load instead of one per chunk
               const uint32_t cap = (L_end - L_beg) / 32 + 2;
               for (uint32_t it = 0;; ++it) {
                 if (it > cap) {
                   if (lane == 0) atomicOr(a.err, kErrInternal);
                   break;
                 }
-                const uint32_t idx = cur + lane;
-                const unsigned long long lp = idx < L_end ? __ldg(U.row + idx) : ~0ull;
-                const uint32_t lv = (uint32_t)lp;
-                uint32_t tt = 0;
+                unsigned long long lp[kMergeChunks];
 #pragma unroll
-                for (int d = 16; d > 0; d >>= 1) {
-                  const uint32_t cand = __shfl_sync(kFull, lv, tt + d);
-                  if (cand <= w) tt += d;
+                for (int c = 0; c < kMergeChunks; ++c) {
+                  const uint32_t idx = cur + 32 * c + lane;
+                  lp[c] = idx < L_end ? __ldg(U.row + idx) : ~0ull;
                 }
-                const uint32_t lvt = __shfl_sync(kFull, lv, tt);
-                const uint32_t ht = (uint32_t)(__shfl_sync(kFull, lp, tt) >> 32);
-                if (look && lvt == w) { p = cur + tt; h = ht; }
-                const uint32_t adv = __popc(__ballot_sync(kFull, lv <= wmax));
+                uint32_t adv = 0;
+#pragma unroll
+                for (int c = 0; c < kMergeChunks; ++c) {
+                  if (c > 0 && adv < 32u * c) break;  // the row passed wmax in an earlier chunk
+                  const uint32_t lv = (uint32_t)lp[c];
+                  uint32_t tt = 0;
+#pragma unroll
+                  for (int d = 16; d > 0; d >>= 1) {
+                    const uint32_t cv = __shfl_sync(kFull, lv, tt + d);
+                    if (cv <= w) tt += d;
+                  }
+                  const uint32_t lvt = __shfl_sync(kFull, lv, tt);
+                  const uint32_t ht = (uint32_t)(__shfl_sync(kFull, lp[c], tt) >> 32);
+                  if (look && lvt == w) { p = cur + 32 * c + tt; h = ht; }
+                  adv += __popc(__ballot_sync(kFull, lv <= wmax));
+                  ++n_chunk;
+                }
                 cur += adv;
-                ++n_chunk;
-                if (adv < 32) break;
+                if (adv < 32u * kMergeChunks) break;
               }
               m_e = e0;
               m_next_o = o0 + 32;
@@ -1307,7 +1325,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
         }
         __syncwarp();
       }
-      push_flush(ps, M, st, a.err, qnext, qdnext);  // entries belong to this member: publish before moving on
+      push_flush(ps, U, M, st, a.err, qnext, qdnext);  // entries belong to this member: publish before moving on
       k = seg_end;
     }
   }
@@ -1322,22 +1340,40 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
 }
 
 // Working-row compaction (between waves): keep the entries whose edge is not
-// processed (tag >= the next wave).  Count, scan (host), fill; warp per vertex.
-__global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restrict__ off,
-                                                       const unsigned long long* __restrict__ row, uint32_t n,
-                                                       const int2* __restrict__ es, const Control* ctl,
-                                                       uint32_t* __restrict__ cnt) {
+// processed (tag >= the next wave).  The edges' states are first condensed
+// into a bitmap (one bit per edge, small enough to stay in L2), so the row
+// passes look up a bit instead of a random 8-byte state.  Mark, count, scan
+// (host), fill; warp per vertex for the row passes.
+__global__ void __launch_bounds__(256) k_compact_mark(const int2* __restrict__ es, uint32_t m,
+                                                      const Control* ctl, uint32_t* __restrict__ alive) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t W = ctl->wave;
+  const uint32_t words = (m + 31) / 32;
+  for (uint32_t i = warp; i < words; i += nwarps) {
+    const uint32_t x = i * 32 + lane;
+    const bool live = x < m && (uint32_t)__ldg(&es[x].y) >= W;
+    const uint32_t bits = __ballot_sync(kFull, live);
+    if (lane == 0) alive[i] = bits;
+  }
+}
+
+__device__ __forceinline__ bool is_alive(const uint32_t* __restrict__ alive, uint32_t x) {
+  return x != kInvalid && ((__ldg(alive + (x >> 5)) >> (x & 31)) & 1u);
+}
+
+__global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restrict__ off,
+                                                       const unsigned long long* __restrict__ row, uint32_t n,
+                                                       const uint32_t* __restrict__ alive,
+                                                       uint32_t* __restrict__ cnt) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = warp; u < n; u += nwarps) {
     const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
     uint32_t c = 0;
-    for (uint32_t s = b + lane; s < e; s += 32) {
-      const uint32_t x = (uint32_t)(__ldg(row + s) >> 32);
-      c += x != kInvalid && (uint32_t)__ldg(&es[x].y) >= W;
-    }
+    for (uint32_t s = b + lane; s < e; s += 32) c += is_alive(alive, (uint32_t)(__ldg(row + s) >> 32));
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(kFull, c, d);
     if (lane == 0) cnt[u] = c;
@@ -1346,13 +1382,12 @@ __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restric
 
 __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict__ off,
                                                       const unsigned long long* __restrict__ row, uint32_t n,
-                                                      const int2* __restrict__ es, const Control* ctl,
+                                                      const uint32_t* __restrict__ alive,
                                                       const uint32_t* __restrict__ off2,
                                                       unsigned long long* __restrict__ row2) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t W = ctl->wave;
   for (uint32_t u = warp; u < n; u += nwarps) {
     const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
     uint32_t at = __ldg(off2 + u);
@@ -1362,8 +1397,7 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
       bool keep = false;
       if (s < e) {
         pr = __ldg(row + s);
-        const uint32_t x = (uint32_t)(pr >> 32);
-        keep = x != kInvalid && (uint32_t)__ldg(&es[x].y) >= W;
+        keep = is_alive(alive, (uint32_t)(pr >> 32));
       }
       const unsigned bal = __ballot_sync(kFull, keep);
       if (keep) row2[at + __popc(bal & ((1u << lane) - 1))] = pr;
@@ -1373,20 +1407,23 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
 }
 
 // After a compaction the rows moved: rebuild the descriptors of every queued
-// frontier (block per member).
-__global__ void k_refresh_desc(const Union* __restrict__ Up, const Member* __restrict__ mem,
-                               const MemberState* __restrict__ st, uint32_t G) {
+// frontier.  `per` blocks share a member (block b serves member b / per), so
+// one large frontier is spread over the whole GPU.
+__global__ void __launch_bounds__(256) k_refresh_desc(const Union* __restrict__ Up,
+                                                      const Member* __restrict__ mem,
+                                                      const MemberState* __restrict__ st, uint32_t G,
+                                                      uint32_t per) {
   const UnionRegs U(Up);
-  for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
-    const MemberState s = st[g];
-    if (s.phase != kPhaseProc) continue;
-    const uint32_t cnt = (uint32_t)(s.curr >> kWorkBits);
-    const Member M = mem[g];
-    const unsigned long long* q = (s.q_sel ? U.q1 : U.q0) + M.eb;
-    uint4* qd = (s.q_sel ? U.qd1 : U.qd0) + M.eb;
-    for (uint32_t x = threadIdx.x; x < cnt; x += blockDim.x)
-      qd[x] = edge_desc(U, M.eb + (uint32_t)(q[x] & kEidMask));
-  }
+  const uint32_t g = blockIdx.x / per, part = blockIdx.x % per;
+  if (g >= G) return;
+  const MemberState s = st[g];
+  if (s.phase != kPhaseProc) return;
+  const uint32_t cnt = (uint32_t)(s.curr >> kWorkBits);
+  const Member M = mem[g];
+  const unsigned long long* q = (s.q_sel ? U.q1 : U.q0) + M.eb;
+  uint4* qd = (s.q_sel ? U.qd1 : U.qd0) + M.eb;
+  for (uint32_t x = part * blockDim.x + threadIdx.x; x < cnt; x += per * blockDim.x)
+    qd[x] = edge_desc(U, M.eb + (uint32_t)(q[x] & kEidMask));
 }
 
 // Publish the compacted rows and resume the loop.
@@ -1496,6 +1533,8 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
     wpref[G] = carry;
     uint32_t done = was_done;
     if (!was_done) {
+      if (ctl->trace && ctl->waves_run < ctl->trace_cap)
+        ctl->trace[ctl->waves_run] = make_ulonglong4(globaltimer(), carry, s_proc, s_scan);
       ctl->el_proc += s_proc;
       ctl->el_scan += s_scan;
       ctl->edges_proc += s_edges;
@@ -1508,9 +1547,10 @@ __global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, M
       if (e) { done = 1; reason = kExitError; }
       if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; reason = kExitError; }
       if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; reason = kExitError; }
-      // live edges fill at most 70% of the working rows: stop so the host can
-      // compact them (a compaction costs about three passes over the rows)
-      if (!done && ctl->csr_slots >= ctl->compact_min && 20 * s_live_edges <= 7 * ctl->csr_slots) {
+      // live edges fill at most 78% of the working rows: stop so the host can
+      // compact them (a compaction costs about 1.2 ms on 128 M slots, which the
+      // shorter rows repay at this fill)
+      if (!done && ctl->csr_slots >= ctl->compact_min && 100 * s_live_edges <= 39 * ctl->csr_slots) {
         done = 1;
         reason = kExitCompact;
       }

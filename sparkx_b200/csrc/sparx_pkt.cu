@@ -7,6 +7,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -74,6 +75,7 @@ struct Counters {  // device scalars
 struct Layout {
   size_t off, nbr, row0, dplus, opos, ocol, osrc, es, act0, act1, q0, q1, qd0, qd1, out, stage0, stage1;
   size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
+  size_t alive;                   // compaction: one bit per edge, set while it is unprocessed
   size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
   size_t total;
 };
@@ -106,6 +108,7 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   L.offB = take(4 * (N + 1));
   L.rowA = take(8 * W);
   L.rowB = take(8 * W);
+  L.alive = take(4 * ((M + 31) / 32));
   L.stage0 = take(kStageBytes);
   L.stage1 = take(kStageBytes);
   const uint64_t tiles = (std::max<uint64_t>(N + 1, M + 1) + kScanTile - 1) / kScanTile + 2;
@@ -141,8 +144,11 @@ struct Engine {
   void* pinned_small = nullptr;  // 4 KB for scalar read-backs
   PeelGraph peel;
   int wave_blocks = 0;
+  ulonglong4* trace = nullptr;  // wave trace records (SPARX_TRACE_FILE set)
   std::mutex mu;
 };
+
+constexpr unsigned long long kTraceRecords = 1ull << 20;
 
 std::mutex g_engines_mu;
 std::map<int, Engine*> g_engines;
@@ -516,6 +522,14 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     c0.timeout_ns = O.timeout_ms * 1000000ull;
     c0.csr_slots = W;
     c0.compact_min = kCompactMinSlots;
+    // wave trace: when SPARX_TRACE_FILE names a file, the planner records
+    // each wave's start time and work there (first 2^20 waves)
+    const char* trace_path = std::getenv("SPARX_TRACE_FILE");
+    if (trace_path && *trace_path) {
+      if (!E.trace) CU(cudaMalloc(&E.trace, kTraceRecords * sizeof(ulonglong4)));
+      c0.trace = E.trace;
+      c0.trace_cap = kTraceRecords;
+    }
     CU(cudaMemcpyAsync(at<Control>(E, L.ctl), &c0, sizeof(Control), cudaMemcpyHostToDevice, s));
     if (m > 0)
       k_peel_setup<<<grid_for(m, 256, E.sm_count * 8), 256, 0, s>>>(at<Union>(E, L.uni), dmem,
@@ -561,12 +575,16 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       // drop processed edges from the working rows, then resume the loop
       uint32_t* off2 = at<uint32_t>(E, next_buf ? L.offB : L.offA);
       unsigned long long* row2 = at<unsigned long long>(E, next_buf ? L.rowB : L.rowA);
-      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, es, wa.ctl, dplus);
+      uint32_t* alive = at<uint32_t>(E, L.alive);
+      k_compact_mark<<<grid_for((m + 31) / 32 * 32ull, 256, E.sm_count * 16), 256, 0, s>>>(es, (uint32_t)m,
+                                                                                          wa.ctl, alive);
+      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, dplus);
       exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
-      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, es, wa.ctl, off2, row2);
+      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, off2, row2);
       k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + N, wa.ctl);
-      k_refresh_desc<<<std::min<uint32_t>(G, 1024), 256, 0, s>>>(wa.Up, dmem, wa.st, G);
-      J.launches += 7;
+      const uint32_t per = std::max<uint32_t>(1, (uint32_t)(E.sm_count * 8) / std::max<uint32_t>(G, 1));
+      k_refresh_desc<<<G * per, 256, 0, s>>>(wa.Up, dmem, wa.st, G, per);
+      J.launches += 8;
       cur_off = off2;
       cur_row = row2;
       next_buf ^= 1;
@@ -598,6 +616,18 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   CU(cudaStreamSynchronize(s));
   J.tri = hc.tri;
   J.kmax = hc.kmax;
+  if (!J.support_only && J.ctl.trace) {
+    const char* trace_path = std::getenv("SPARX_TRACE_FILE");
+    const size_t nrec = (size_t)std::min<unsigned long long>(J.ctl.waves_run, J.ctl.trace_cap);
+    std::vector<ulonglong4> rec(nrec);
+    if (nrec) CU(cudaMemcpy(rec.data(), J.ctl.trace, nrec * sizeof(ulonglong4), cudaMemcpyDeviceToHost));
+    if (FILE* f = std::fopen(trace_path, "w")) {
+      std::fprintf(f, "wave,t_ns,work,frontier_elements,scan_elements\n");
+      for (size_t i = 0; i < nrec; ++i)
+        std::fprintf(f, "%zu,%llu,%llu,%llu,%llu\n", i + 1, rec[i].x, rec[i].y, rec[i].z, rec[i].w);
+      std::fclose(f);
+    }
+  }
   // each WHILE-loop iteration is one wave kernel + one planner kernel
   if (!J.support_only && O.loop == SPARX_LOOP_GRAPH)
     J.launches += 2 * (uint32_t)std::max<unsigned long long>(J.ctl.waves_run, 1);
@@ -985,6 +1015,7 @@ void engine_release(Engine* E) {
   if (E->stream) cudaStreamSynchronize(E->stream);
   if (E->peel.exec) { cudaGraphExecDestroy(E->peel.exec); cudaGraphDestroy(E->peel.graph); }
   if (E->ws) cudaFree(E->ws);
+  if (E->trace) cudaFree(E->trace);
   for (int i = 0; i < 2; ++i) {
     if (E->pinned[i]) cudaFreeHost(E->pinned[i]);
     if (E->pin_ev[i]) cudaEventDestroy(E->pin_ev[i]);
