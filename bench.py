@@ -346,7 +346,8 @@ def main():
                           "ms_orient": st.ms_orient, "ms_support": st.ms_support,
                           "ms_peel": st.ms_peel, "launches": st.launches, "peel_elements": st.peel_elements,
                           "peel_hits": st.peel_hits, "peel_scanned": st.peel_scanned,
-                          "compactions": st.compactions, "merge_iters": st.merge_iters,
+                          "compactions": st.compactions, "hub_maps": st.hub_maps,
+                          "merge_iters": st.merge_iters,
                           "lane_iters": st.lane_iters, "merge_chunks": st.merge_chunks}), flush=True)
         return 0
     for _ in range(max(3, args.warmup)):

@@ -72,7 +72,7 @@ typedef struct sparx_pkt_stats {
   uint64_t peel_scanned;      /* active-list entries read by level scans */
   uint64_t peel_edges;        /* frontier edges processed (= m minus zero-support edges) */
   uint32_t compactions;       /* rebuilds of the peel's working rows */
-  uint32_t reserved;
+  uint32_t hub_maps;          /* dense neighbour -> edge maps built for the highest-degree vertices */
   uint64_t merge_iters;       /* peel warp iterations resolved by a row merge */
   uint64_t lane_iters;        /* peel warp iterations resolved by per-lane searches */
   uint64_t merge_chunks;      /* 32-entry chunks of longer rows read by the merges */

@@ -64,6 +64,8 @@ struct Union {  // the prepared concatenated graph, as the peel sees it
   uint32_t* act[2];
   unsigned long long* q[2];
   uint4* qd[2];                    // per queue entry {short row start, length, long row begin, end}
+  const uint32_t* hub_slot;        // vertex -> hub map index or kInvalid; nullptr = no hub maps
+  const uint32_t* hub_map;         // hub k's neighbours: hub_map[k * n + id] = edge id or kInvalid
   uint32_t n;
   uint32_t m;
   uint32_t width;
@@ -84,11 +86,19 @@ struct UnionRegs {
   unsigned long long* q1;
   uint4* qd0;
   uint4* qd1;
+  const uint32_t* __restrict__ hub_slot;
+  const uint32_t* __restrict__ hub_map;
+  uint32_t n;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
       : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]),
-        qd0(p->qd[0]), qd1(p->qd[1]) {}
+        qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), n(p->n) {}
 };
+
+// A queue-entry descriptor whose longer row belongs to a hub carries
+// kHubDesc | hub index in place of the longer row's begin (row positions stay
+// below 2^31 whenever hub maps are built).
+constexpr uint32_t kHubDesc = 0x80000000u;
 
 struct Member {  // static per-member ranges
   uint32_t vb, n;   // vertices [vb, vb + n)
@@ -943,12 +953,18 @@ struct WaveArgs {
 };
 
 // Rows of frontier edge x in the working CSR: {shorter row start, its length,
-// longer row begin, longer row end}.  The length is the edge's work.
+// longer row begin, longer row end}, or {.., .., kHubDesc | hub index, 0} when
+// the longer row's vertex has a hub map.  The length is the edge's work.
 __device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x) {
   const uint32_t u = __ldg(U.osrc + x), v = __ldg(U.ocol + x);
   const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
   const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
-  return (ue - ub <= ve - vb) ? make_uint4(ub, ue - ub, vb, ve) : make_uint4(vb, ve - vb, ub, ue);
+  const bool u_short = ue - ub <= ve - vb;
+  if (U.hub_slot) {
+    const uint32_t hs = __ldg(U.hub_slot + (u_short ? v : u));
+    if (hs != kInvalid) return u_short ? make_uint4(ub, ue - ub, kHubDesc | hs, 0) : make_uint4(vb, ve - vb, kHubDesc | hs, 0);
+  }
+  return u_short ? make_uint4(ub, ue - ub, vb, ve) : make_uint4(vb, ve - vb, ub, ue);
 }
 
 // PKT sub-level rule for one triangle (e, f, h) of frontier edge e at level l,
@@ -1029,6 +1045,9 @@ constexpr int kWaveThreads = 256;
 #define SPARX_WAVE_MINB 6  // resident 256-thread blocks per SM the register budget targets
 #endif
 constexpr int kWaveWarps = kWaveThreads / 32;
+// kept active-list entries staged per warp before one atomic reserves their
+// place: every kept entry of a large scan goes through one counter per member
+constexpr int kKeepBuf = 256;
 #ifndef SPARX_MERGE_CHUNKS
 #define SPARX_MERGE_CHUNKS 2  // long-row chunks of 32 entries loaded per merge round
 #endif
@@ -1103,7 +1122,7 @@ __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, con
 //                       edge e, searched in the longer row; a hit is a triangle
 __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs a) {
   __shared__ uint32_t s_push_eid[kWaveWarps][kPushBuf];
-  __shared__ uint32_t s_keep[kWaveWarps][kPushBuf];
+  __shared__ uint32_t s_keep[kWaveWarps][kKeepBuf];
   const Control* ctl = a.ctl;
   if (ctl->done) return;
   const unsigned long long total = ctl->total_work;
@@ -1114,6 +1133,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   const UnionRegs U(a.Up);
+  const bool hubs = U.hub_map != nullptr;  // descriptors carry kHubDesc only when maps exist
   unsigned long long ch = total / (nwarps * 2);
   ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
   uint32_t hits = 0, n_merge = 0, n_lane = 0, n_chunk = 0;
@@ -1195,7 +1215,8 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           const uint32_t L_beg = __shfl_sync(kFull, lb, 0), L_end = __shfl_sync(kFull, le, 0);
           const uint32_t s_len0 = __shfl_sync(kFull, slen, 0);
           const bool one_edge = __all_sync(kFull, !valid || e == e0);
-          if (one_edge && (L_end - L_beg) <= 8u * s_len0) {
+          const bool hub0 = hubs && (L_beg & kHubDesc);
+          if (one_edge && !hub0 && (L_end - L_beg) <= 8u * s_len0) {
             // similar row lengths: walk the longer row with a warp-wide cursor;
             // every chunk of 32 entries is matched against the 32 sorted
             // elements by a shuffle search
@@ -1253,8 +1274,14 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
             ++n_lane;
             m_e = kInvalid;
             if (look) {
-              p = find_in_row(U.row, lb, le, w);
-              if (p != kInvalid) h = (uint32_t)(__ldg(U.row + p) >> 32);
+              if (hubs && (lb & kHubDesc)) {
+                // the longer row's vertex has a hub map: one lookup
+                h = __ldg(U.hub_map + (unsigned long long)(lb & ~kHubDesc) * U.n + w);
+                p = h != kInvalid ? 0u : kInvalid;
+              } else {
+                p = find_in_row(U.row, lb, le, w);
+                if (p != kInvalid) h = (uint32_t)(__ldg(U.row + p) >> 32);
+              }
             }
           }
           bool pf = false, ph = false;
@@ -1294,13 +1321,12 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           const unsigned kb_bal = __ballot_sync(kFull, keep);
           if (kb_bal) {
             const uint32_t kc = __popc(kb_bal);
-            if (nkeep + kc > kPushBuf) {
+            if (nkeep + kc > kKeepBuf) {
               __syncwarp();
               uint32_t old = 0;
               if (lane == 0) old = atomicAdd(&st->kept, nkeep);
               old = __shfl_sync(kFull, old, 0);
-              if (lane < nkeep) act_out[M.eb + old + lane] = keepbuf[lane];
-              if (lane + 32 < nkeep) act_out[M.eb + old + 32 + lane] = keepbuf[lane + 32];
+              for (uint32_t t = lane; t < nkeep; t += 32) act_out[M.eb + old + t] = keepbuf[t];
               nkeep = 0;
               __syncwarp();
             }
@@ -1314,8 +1340,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           uint32_t old = 0;
           if (lane == 0) old = atomicAdd(&st->kept, nkeep);
           old = __shfl_sync(kFull, old, 0);
-          if (lane < nkeep) act_out[M.eb + old + lane] = keepbuf[lane];
-          if (lane + 32 < nkeep) act_out[M.eb + old + 32 + lane] = keepbuf[lane + 32];
+          for (uint32_t t = lane; t < nkeep; t += 32) act_out[M.eb + old + t] = keepbuf[t];
         }
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
@@ -1329,13 +1354,83 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
       k = seg_end;
     }
   }
+  // work counters: summed per block, then one atomic per counter and block
+  // (per-warp atomics on four addresses serialise on large waves)
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) hits += __shfl_xor_sync(kFull, hits, d);
+  __shared__ uint32_t s_cnt[4][kWaveWarps];
   if (lane == 0) {
-    if (hits) atomicAdd(&a.ctl->hits, (unsigned long long)hits);
-    if (n_merge) atomicAdd(&a.ctl->merge_iters, (unsigned long long)n_merge);
-    if (n_lane) atomicAdd(&a.ctl->lane_iters, (unsigned long long)n_lane);
-    if (n_chunk) atomicAdd(&a.ctl->merge_chunks, (unsigned long long)n_chunk);
+    s_cnt[0][wib] = hits;
+    s_cnt[1][wib] = n_merge;
+    s_cnt[2][wib] = n_lane;
+    s_cnt[3][wib] = n_chunk;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int w = 0; w < kWaveWarps; ++w) sum += s_cnt[threadIdx.x][w];
+    unsigned long long* dst = threadIdx.x == 0 ? &a.ctl->hits
+                              : threadIdx.x == 1 ? &a.ctl->merge_iters
+                              : threadIdx.x == 2 ? &a.ctl->lane_iters
+                                                 : &a.ctl->merge_chunks;
+    if (sum) atomicAdd(dst, sum);
+  }
+}
+
+// Hub maps: the vertices of highest degree (at least `min_deg`, at most the
+// reserved number of maps) get a dense map from neighbour id to edge id, so a
+// frontier element whose longer row is a hub's resolves its triangle with one
+// load instead of a search of the long row.
+//   k_hub_hist    histogram of floor(log2(degree))
+//   k_hub_assign  hub index per vertex (kInvalid below the chosen degree)
+//   k_hub_fill    scatter each hub's row into its map (warp per hub)
+__global__ void __launch_bounds__(256) k_hub_hist(const uint32_t* __restrict__ off, uint32_t n,
+                                                  uint32_t* __restrict__ hist) {
+  __shared__ uint32_t sh[33];
+  if (threadIdx.x < 33) sh[threadIdx.x] = 0;
+  __syncthreads();
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    const uint32_t d = __ldg(off + u + 1) - __ldg(off + u);
+    if (d) atomicAdd(&sh[32 - __clz(d)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 33 && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_hub_assign(const uint32_t* __restrict__ off, uint32_t n,
+                                                    uint32_t min_deg, uint32_t max_hubs,
+                                                    uint32_t* __restrict__ hub_slot,
+                                                    uint32_t* __restrict__ hub_vertex,
+                                                    uint32_t* __restrict__ hub_count) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    const uint32_t d = __ldg(off + u + 1) - __ldg(off + u);
+    uint32_t slot = kInvalid;
+    if (d >= min_deg) {
+      slot = atomicAdd(hub_count, 1u);
+      if (slot < max_hubs) hub_vertex[slot] = u;
+      else slot = kInvalid;  // cannot happen: the host sized max_hubs from the histogram
+    }
+    hub_slot[u] = slot;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_hub_fill(const uint32_t* __restrict__ off,
+                                                  const unsigned long long* __restrict__ row0, uint32_t n,
+                                                  const uint32_t* __restrict__ hub_vertex, uint32_t hubs,
+                                                  uint32_t* __restrict__ hub_map) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t k = warp; k < hubs; k += nwarps) {
+    const uint32_t u = hub_vertex[k];
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    uint32_t* map = hub_map + (unsigned long long)k * n;
+    for (uint32_t s = b + lane; s < e; s += 32) {
+      const unsigned long long pr = __ldg(row0 + s);
+      const uint32_t id = (uint32_t)pr;
+      if (id < n) map[id] = (uint32_t)(pr >> 32);
+    }
   }
 }
 

@@ -68,6 +68,7 @@ struct Counters {  // device scalars
   uint32_t vcursor;      // vertex-form support: next light vertex batch
   uint32_t hcursor;      //                      next heavy vertex
   uint32_t heavy_count;  //                      heavy vertices listed
+  uint32_t hub_count;    // hub maps assigned
 };
 
 
@@ -76,9 +77,24 @@ struct Layout {
   size_t off, nbr, row0, dplus, opos, ocol, osrc, es, act0, act1, q0, q1, qd0, qd1, out, stage0, stage1;
   size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
   size_t alive;                   // compaction: one bit per edge, set while it is unprocessed
+  size_t hub_slot, hub_vertex, hub_hist, hub_map;  // hub maps (hub_cap == 0: none)
+  uint32_t hub_cap;
   size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
   size_t total;
 };
+
+// Hub maps (single-graph launches): at most kHubMaxCount maps of N u32
+// entries within kHubBudgetBytes, for vertices of degree >= kHubMinDegree
+// (so never more than W / kHubMinDegree of them).
+constexpr uint64_t kHubBudgetBytes = 4ull << 30;
+constexpr uint32_t kHubMinDegree = 1024;
+constexpr uint32_t kHubMaxCount = 1024;
+
+uint32_t hub_capacity(uint64_t N, uint64_t W, uint32_t G) {
+  if (G != 1 || N == 0 || W >= (1ull << 31)) return 0;
+  const uint64_t k = std::min<uint64_t>({kHubMaxCount, W / kHubMinDegree, kHubBudgetBytes / (4 * N)});
+  return (uint32_t)k;
+}
 
 Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_bytes) {
   Layout L{};
@@ -109,6 +125,13 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   L.rowA = take(8 * W);
   L.rowB = take(8 * W);
   L.alive = take(4 * ((M + 31) / 32));
+  L.hub_cap = hub_capacity(N, W, G);
+  if (L.hub_cap) {
+    L.hub_slot = take(4 * N);
+    L.hub_vertex = take(4ull * L.hub_cap);
+    L.hub_hist = take(4 * 34);
+    L.hub_map = take(4ull * L.hub_cap * N);
+  }
   L.stage0 = take(kStageBytes);
   L.stage1 = take(kStageBytes);
   const uint64_t tiles = (std::max<uint64_t>(N + 1, M + 1) + kScanTile - 1) / kScanTile + 2;
@@ -380,6 +403,7 @@ struct UnionJob {
   float ms_orient = 0, ms_support = 0, ms_peel = 0, ms_finalize = 0;
   uint32_t launches = 0;
   unsigned long long support_elements = 0;
+  uint32_t hubs = 0;  // hub maps built
   Control ctl{};
 };
 
@@ -455,6 +479,13 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     if (*herr) { J.err = *herr; return status_from_flags(*herr); }
   }
   // -- orientation (Kernel B) --
+  const bool hubs_possible = L.hub_cap > 0 && !J.support_only;
+  uint32_t* hub_hist = hubs_possible ? at<uint32_t>(E, L.hub_hist) : nullptr;
+  if (hubs_possible) {
+    CU(cudaMemsetAsync(hub_hist, 0, 4 * 34, s));
+    k_hub_hist<<<grid_for(N, 256, E.sm_count * 4), 256, 0, s>>>(J.off, N, hub_hist);
+    J.launches += 1;
+  }
   k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus);
   exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
   J.launches += 4;
@@ -466,6 +497,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   uint32_t m32 = 0;
   CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
+  uint32_t hist[34] = {};
+  if (hubs_possible) CU(cudaMemcpyAsync(hist, hub_hist, 4 * 33, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   J.self_loops = hc.self_loops;
   if (hc.err) { J.err = hc.err; return status_from_flags(hc.err); }
@@ -476,6 +509,35 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, row0);
   k_orient_reverse<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, row0, err);
   J.launches += 2;
+  // hub maps: the smallest power-of-two degree bound (>= kHubMinDegree) whose
+  // vertices fit the reserved maps; hist[b] counts degrees in [2^(b-1), 2^b)
+  uint32_t hubs = 0, hub_min_deg = 0;
+  if (hubs_possible) {
+    uint64_t above = 0;
+    for (int b = 32; b >= 1; --b) {
+      const uint64_t lo = 1ull << (b - 1);
+      if (lo < kHubMinDegree || above + hist[b] > L.hub_cap) break;
+      above += hist[b];
+      hub_min_deg = (uint32_t)lo;
+    }
+    hubs = (uint32_t)above;
+  }
+  const uint32_t* d_hub_slot = nullptr;
+  const uint32_t* d_hub_map = nullptr;
+  if (hubs) {
+    uint32_t* hslot = at<uint32_t>(E, L.hub_slot);
+    uint32_t* hvert = at<uint32_t>(E, L.hub_vertex);
+    uint32_t* hmap = at<uint32_t>(E, L.hub_map);
+    CU(cudaMemsetAsync(&cnt->hub_count, 0, 4, s));
+    k_hub_assign<<<grid_for(N, 256, E.sm_count * 8), 256, 0, s>>>(J.off, N, hub_min_deg, hubs, hslot, hvert,
+                                                                  &cnt->hub_count);
+    CU(cudaMemsetAsync(hmap, 0xFF, 4ull * hubs * N, s));
+    k_hub_fill<<<grid_for(32ull * hubs, 256, E.sm_count * 4), 256, 0, s>>>(J.off, row0, N, hvert, hubs, hmap);
+    J.launches += 2;
+    d_hub_slot = hslot;
+    d_hub_map = hmap;
+  }
+  J.hubs = hubs;
   CU(cudaEventRecord(E.tev[2], s));
 
   // -- support (Kernel C) --
@@ -496,7 +558,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaEventRecord(E.tev[5], s));
   } else {
     // -- peel (Kernel D) --
-    Union U;
+    Union U{};
     U.off = J.off;
     U.row = row0;
     U.opos = opos;
@@ -509,6 +571,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     U.q[1] = at<unsigned long long>(E, L.q1);
     U.qd[0] = at<uint4>(E, L.qd0);
     U.qd[1] = at<uint4>(E, L.qd1);
+    U.hub_slot = d_hub_slot;
+    U.hub_map = d_hub_map;
     U.n = N;
     U.m = (uint32_t)m;
     U.width = (uint32_t)W;
@@ -664,6 +728,7 @@ void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
     st->peel_scanned = J.ctl.el_scan;
     st->peel_edges = J.ctl.edges_proc;
     st->compactions = J.ctl.compactions;
+    st->hub_maps = J.hubs;
     st->merge_iters = J.ctl.merge_iters;
     st->lane_iters = J.ctl.lane_iters;
     st->merge_chunks = J.ctl.merge_chunks;
@@ -1504,7 +1569,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
     if (rc) return rc;
   }
 
-  Union U;
+  Union U{};  // no hub maps in the fixed scratch
   U.off = off;
   U.row = row0;
   U.opos = opos;

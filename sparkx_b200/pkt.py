@@ -71,7 +71,7 @@ class _Stats(ctypes.Structure):
         ("ms_total", ctypes.c_double),
         ("support_elements", ctypes.c_uint64), ("peel_elements", ctypes.c_uint64),
         ("peel_hits", ctypes.c_uint64), ("peel_scanned", ctypes.c_uint64),
-        ("peel_edges", ctypes.c_uint64), ("compactions", ctypes.c_uint32), ("reserved2", ctypes.c_uint32),
+        ("peel_edges", ctypes.c_uint64), ("compactions", ctypes.c_uint32), ("hub_maps", ctypes.c_uint32),
         ("merge_iters", ctypes.c_uint64), ("lane_iters", ctypes.c_uint64), ("merge_chunks", ctypes.c_uint64),
     ]
 
@@ -176,6 +176,7 @@ class PktStats:
     peel_scanned: int = 0
     peel_edges: int = 0
     compactions: int = 0
+    hub_maps: int = 0
     merge_iters: int = 0
     lane_iters: int = 0
     merge_chunks: int = 0
