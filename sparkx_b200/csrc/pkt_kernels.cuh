@@ -72,6 +72,25 @@ struct Union {  // the prepared concatenated graph, as the peel sees it
   uint32_t G;
 };
 
+// The peel's arrays that stay where they are for a whole run.  The wave
+// kernel takes them as a by-value parameter, so the compiler can re-read any
+// of them from the parameter bank instead of holding (or spilling) it; only
+// the working rows, which a compaction replaces, are read from the Union.
+struct PeelArrays {
+  const uint32_t* ocol;
+  const uint32_t* osrc;
+  int2* es;
+  uint32_t* act0;
+  uint32_t* act1;
+  unsigned long long* q0;
+  unsigned long long* q1;
+  uint4* qd0;
+  uint4* qd1;
+  const uint32_t* hub_slot;
+  const uint32_t* hub_map;
+  uint32_t n;
+};
+
 // Field-by-field copy of a device-resident Union into registers (a struct
 // copy would land in local memory).
 struct UnionRegs {
@@ -93,6 +112,10 @@ struct UnionRegs {
       : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]),
         qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), n(p->n) {}
+  __device__ __forceinline__ UnionRegs(const Union* p, const PeelArrays& a)
+      : off(p->off), row(p->row), ocol(a.ocol), osrc(a.osrc), es(a.es),
+        act0(a.act0), act1(a.act1), q0(a.q0), q1(a.q1),
+        qd0(a.qd0), qd1(a.qd1), hub_slot(a.hub_slot), hub_map(a.hub_map), n(a.n) {}
 };
 
 // A queue-entry descriptor whose longer row belongs to a hub carries
@@ -135,6 +158,7 @@ struct Control {
   unsigned long long csr_slots;   // entries in the working rows
   unsigned long long compact_min; // do not compact working rows smaller than this
   uint32_t exit_reason;           // why the loop stopped: kExit*
+  uint32_t blocks_done;           // wave blocks finished (the last one plans the next wave)
   uint32_t compactions;
   unsigned long long merge_iters; // warp iterations resolved by the row merge
   unsigned long long lane_iters;  // warp iterations resolved by per-lane searches
@@ -326,7 +350,13 @@ __global__ void k_shift_ids(uint32_t* __restrict__ ids, unsigned long long count
 }
 
 // ---------------------------------------------------------------------------
-// Kernel B1: per-row validation + oriented out-degree.  Warp per vertex.
+// Row kernels take 32 consecutive vertices per warp: a row of at most
+// kLaneRow entries is walked by its own lane, longer rows by the whole warp
+// one at a time, so low-degree vertices (most of a skewed graph) keep all
+// lanes busy.
+constexpr uint32_t kLaneRow = 32;
+
+// Kernel B1: per-row validation + oriented out-degree.
 //   rows strictly ascending (equal -> multigraph), counts self-loops, and
 //   dplus[u] = #{v in N(u): v != u, rank(u) < rank(v)}.
 __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict__ off,
@@ -340,39 +370,66 @@ __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t flags = 0, mxd = 0;
   unsigned long long selfc = 0;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
-    const uint32_t du = e - b;
+  for (uint32_t base = warp * 32; base < n; base += nwarps * 32) {
+    const uint32_t u = base + lane;
+    uint32_t b = 0, e = 0;
+    if (u < n) { b = __ldg(off + u); e = __ldg(off + u + 1); }
     uint32_t cnt = 0;
-    for (uint32_t s = b + lane; s < e; s += 32) {
-      uint32_t v = __ldg(nbr + s);
-      if (v >= n) { flags |= kErrRange; continue; }
-      if (s + 1 < e) {
-        uint32_t nx = __ldg(nbr + s + 1);
-        if (nx == v) flags |= kErrMulti;
-        else if (nx < v) flags |= kErrUnsorted;
+    if (u < n && e - b <= kLaneRow) {
+      uint32_t prev = 0;
+      for (uint32_t s = b; s < e; ++s) {
+        const uint32_t v = __ldg(nbr + s);
+        if (s > b && prev < n) {  // the pair (prev, v), judged as the warp path does
+          if (v == prev) flags |= kErrMulti;
+          else if (v < prev) flags |= kErrUnsorted;
+        }
+        prev = v;
+        if (v >= n) { flags |= kErrRange; continue; }
+        if (v == u) { selfc++; continue; }
+        cnt += rank_less(e - b, u, deg_of(off, v), v);
       }
-      if (v == u) { selfc++; continue; }
-      uint32_t dv = deg_of(off, v);
-      cnt += rank_less(du, u, dv, v);
     }
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    while (big) {
+      const int j = __ffs(big) - 1;
+      big &= big - 1;
+      const uint32_t bu = base + j, bb = __shfl_sync(kFull, b, j), be = __shfl_sync(kFull, e, j);
+      const uint32_t du = be - bb;
+      uint32_t c = 0;
+      for (uint32_t s = bb + lane; s < be; s += 32) {
+        const uint32_t v = __ldg(nbr + s);
+        if (v >= n) { flags |= kErrRange; continue; }
+        if (s + 1 < be) {
+          const uint32_t nx = __ldg(nbr + s + 1);
+          if (nx == v) flags |= kErrMulti;
+          else if (nx < v) flags |= kErrUnsorted;
+        }
+        if (v == bu) { selfc++; continue; }
+        c += rank_less(du, bu, deg_of(off, v), v);
+      }
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) cnt += __shfl_down_sync(kFull, cnt, d);
-    if (lane == 0) {
+      for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(kFull, c, d);
+      if (lane == (uint32_t)j) cnt = c;
+    }
+    if (u < n) {
       dplus[u] = cnt;
       mxd = max(mxd, cnt);
     }
   }
   if (flags) atomicOr(err, flags);
 #pragma unroll
-  for (int d = 16; d > 0; d >>= 1) selfc += __shfl_down_sync(kFull, selfc, d);
+  for (int d = 16; d > 0; d >>= 1) {
+    selfc += __shfl_down_sync(kFull, selfc, d);
+    mxd = max(mxd, __shfl_down_sync(kFull, mxd, d));
+  }
   if (lane == 0 && selfc) atomicAdd(self_loops, selfc);
   if (lane == 0 && mxd) atomicMax(max_dplus, mxd);
 }
 
 // Kernel B2: fill oriented lists (kept in id order) and, for each vertex's
 // out-slots, the (id | edge id << 32) pair of row0; self-loop slots get edge id
-// 0xFFFFFFFF.  Warp per vertex.
+// 0xFFFFFFFF.  In-slots are left to B3: owner[s] = u marks them (kInvalid for
+// the others).
 __device__ __forceinline__ unsigned long long make_pair(uint32_t id, uint32_t e) {
   return (unsigned long long)id | ((unsigned long long)e << 32);
 }
@@ -382,58 +439,88 @@ __global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict_
                                                      const uint32_t* __restrict__ opos,
                                                      uint32_t* __restrict__ ocol,
                                                      uint32_t* __restrict__ osrc,
-                                                     unsigned long long* __restrict__ row0) {
+                                                     unsigned long long* __restrict__ row0,
+                                                     uint32_t* __restrict__ owner) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
-    const uint32_t du = e - b;
-    uint32_t base = __ldg(opos + u);
-    for (uint32_t s0 = b; s0 < e; s0 += 32) {
-      const uint32_t s = s0 + lane;
-      bool out = false;
-      uint32_t v = 0;
-      if (s < e) {
-        v = __ldg(nbr + s);
-        if (v == u || v >= n) row0[s] = make_pair(v, kInvalid);
-        else out = rank_less(du, u, deg_of(off, v), v);
+  for (uint32_t base0 = warp * 32; base0 < n; base0 += nwarps * 32) {
+    const uint32_t u = base0 + lane;
+    uint32_t b = 0, e = 0;
+    if (u < n) { b = __ldg(off + u); e = __ldg(off + u + 1); }
+    if (u < n && e - b <= kLaneRow) {
+      uint32_t p = __ldg(opos + u);
+      for (uint32_t s = b; s < e; ++s) {
+        const uint32_t v = __ldg(nbr + s);
+        uint32_t own = kInvalid;
+        if (v == u || v >= n) {
+          row0[s] = make_pair(v, kInvalid);
+        } else if (rank_less(e - b, u, deg_of(off, v), v)) {
+          ocol[p] = v;
+          osrc[p] = u;
+          row0[s] = make_pair(v, p);
+          ++p;
+        } else {
+          own = u;
+        }
+        owner[s] = own;
       }
-      unsigned bal = __ballot_sync(kFull, out);
-      if (out) {
-        uint32_t p = base + __popc(bal & ((1u << lane) - 1));
-        ocol[p] = v;
-        osrc[p] = u;
-        row0[s] = make_pair(v, p);
+    }
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    while (big) {
+      const int j = __ffs(big) - 1;
+      big &= big - 1;
+      const uint32_t bu = base0 + j, bb = __shfl_sync(kFull, b, j), be = __shfl_sync(kFull, e, j);
+      const uint32_t du = be - bb;
+      uint32_t p0 = __ldg(opos + bu);
+      for (uint32_t s0 = bb; s0 < be; s0 += 32) {
+        const uint32_t s = s0 + lane;
+        bool out = false;
+        uint32_t v = 0;
+        if (s < be) {
+          v = __ldg(nbr + s);
+          uint32_t own = kInvalid;
+          if (v == bu || v >= n) row0[s] = make_pair(v, kInvalid);
+          else if (rank_less(du, bu, deg_of(off, v), v)) out = true;
+          else own = bu;
+          owner[s] = own;
+        }
+        const unsigned bal = __ballot_sync(kFull, out);
+        if (out) {
+          const uint32_t p = p0 + __popc(bal & ((1u << lane) - 1));
+          ocol[p] = v;
+          osrc[p] = bu;
+          row0[s] = make_pair(v, p);
+        }
+        p0 += __popc(bal);
       }
-      base += __popc(bal);
     }
   }
 }
 
-// Kernel B3: in-slots (rank(v) < rank(u)) take the id of v's out-slot to u,
-// found by binary search in v's oriented list.  Missing -> asymmetric.
-__global__ void __launch_bounds__(256) k_orient_reverse(const uint32_t* __restrict__ off,
-                                                        const uint32_t* __restrict__ nbr, uint32_t n,
+// Kernel B3: in-slots (owner[s] = u: rank(v) < rank(u)) take the id of v's
+// out-slot to u, found by binary search in v's oriented list; slot-parallel.
+// Missing -> asymmetric.
+__global__ void __launch_bounds__(256) k_orient_reverse(const uint32_t* __restrict__ nbr,
+                                                        const uint32_t* __restrict__ owner,
+                                                        unsigned long long width,
                                                         const uint32_t* __restrict__ opos,
                                                         const uint32_t* __restrict__ ocol,
                                                         unsigned long long* __restrict__ row0,
                                                         uint32_t* __restrict__ err) {
-  const uint32_t lane = lane_id();
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   bool bad = false;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
-    const uint32_t du = e - b;
-    for (uint32_t s = b + lane; s < e; s += 32) {
-      uint32_t v = __ldg(nbr + s);
-      if (v == u || v >= n) continue;
-      if (rank_less(du, u, deg_of(off, v), v)) continue;
-      uint32_t lo = __ldg(opos + v), hi = __ldg(opos + v + 1);
-      uint32_t p = lower_bound_u32(ocol, lo, hi, u);
-      if (p < hi && __ldg(ocol + p) == u) row0[s] = make_pair(v, p);
-      else { row0[s] = make_pair(v, kInvalid); bad = true; }
+  for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < width;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t u = __ldg(owner + s);
+    if (u == kInvalid) continue;
+    const uint32_t v = __ldg(nbr + s);
+    const uint32_t lo = __ldg(opos + v), hi = __ldg(opos + v + 1);
+    const uint32_t p = lower_bound_u32(ocol, lo, hi, u);
+    if (p < hi && __ldg(ocol + p) == u) {
+      row0[s] = make_pair(v, p);
+    } else {
+      row0[s] = make_pair(v, kInvalid);
+      bad = true;
     }
   }
   if (bad) atomicOr(err, kErrAsym);
@@ -944,12 +1031,15 @@ __global__ void k_peel_init(const Member* __restrict__ mem, MemberState* __restr
 }
 
 struct WaveArgs {
-  const Union* Up;
+  const Union* Up;     // working rows (replaced by compactions)
+  PeelArrays arr;      // everything else the wave reads, by value
   const Member* mem;
   MemberState* st;
   Control* ctl;
-  const unsigned long long* wpref;
+  unsigned long long* wpref;
   uint32_t* err;
+  cudaGraphConditionalHandle handle;  // WHILE condition of the peel graph
+  int use_handle;                     // 0: waves are launched by the host
 };
 
 // Rows of frontier edge x in the working CSR: {shorter row start, its length,
@@ -1112,6 +1202,149 @@ __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, con
   ps.n += k;
 }
 
+// Member state read past L1: the planner runs in the wave kernel's last
+// block, whose L1 may hold lines that other blocks changed by atomics.
+__device__ __forceinline__ MemberState load_state_cg(const MemberState* p) {
+  static_assert(sizeof(MemberState) % 16 == 0, "MemberState is read as uint4 words");
+  MemberState s;
+  const uint4* src = reinterpret_cast<const uint4*>(p);
+  uint4* dst = reinterpret_cast<uint4*>(&s);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(MemberState) / 16); ++i) dst[i] = __ldcg(src + i);
+  return s;
+}
+
+struct PlanShared {
+  unsigned long long sw[32];
+  uint32_t live;
+  unsigned long long proc, scan, edges, live_edges;
+};
+
+// Planner: one block advances every member's state machine after a wave and
+// lays out the next wave's work; sets the CUDA-graph loop condition.  Runs in
+// the last block of each wave (see k_wave), after every other block's writes.
+__device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, MemberState* __restrict__ st,
+                                          Control* ctl, unsigned long long* __restrict__ wpref,
+                                          uint32_t* __restrict__ err, cudaGraphConditionalHandle handle,
+                                          int use_handle, PlanShared& ps) {
+  unsigned long long* sw = ps.sw;
+  uint32_t& s_live = ps.live;
+  unsigned long long &s_proc = ps.proc, &s_scan = ps.scan, &s_edges = ps.edges, &s_live_edges = ps.live_edges;
+  const uint32_t G = ctl->G;
+  if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; s_live_edges = 0; }
+  __syncthreads();
+  const bool was_done = ctl->done;
+  if (was_done) {
+    // the loop is stopped (host-launched waves keep coming until the host
+    // looks): the planned wave must survive untouched for a resume
+    if (threadIdx.x == 0 && use_handle) cudaGraphSetConditional(handle, 0u);
+    return;
+  }
+  unsigned long long carry = 0;
+  for (uint32_t b = 0; b < G; b += blockDim.x) {
+    const uint32_t g = b + threadIdx.x;
+    unsigned long long w = 0;
+    if (g < G && !was_done) {
+      MemberState s = load_state_cg(st + g);
+      const uint32_t m = mem[g].m;
+      switch (s.phase) {
+        case kPhaseScan0:
+          s.act_sel ^= 1u;
+          s.act_count = s.kept;
+          s.kept = 0;
+          if (s.processed >= m) s.phase = kPhaseDone;
+          else { s.level = s.min_kept; s.min_kept = 0xFFFFFFFFu; s.phase = kPhaseScan; }
+          break;
+        case kPhaseScan: {
+          s.act_sel ^= 1u;
+          s.act_count = s.kept;
+          s.kept = 0;
+          const unsigned long long cnt = s.next >> kWorkBits;
+          if (cnt) {
+            s.curr = s.next;
+            s.next = 0;
+            s.q_sel ^= 1u;
+            s.phase = kPhaseProc;
+            s.levels++;
+            s.max_level = s.level;
+          } else if (s.act_count == 0) {
+            s.phase = kPhaseDone;
+          } else {
+            s.level = s.min_kept;  // no edge at this level: jump to the next occupied one
+          }
+          s.min_kept = 0xFFFFFFFFu;
+          break;
+        }
+        case kPhaseProc: {
+          s.processed += (uint32_t)(s.curr >> kWorkBits);
+          const unsigned long long cnt = s.next >> kWorkBits;
+          if (cnt) {
+            s.curr = s.next;
+            s.next = 0;
+            s.q_sel ^= 1u;
+          } else {
+            s.curr = 0;
+            if (s.processed >= m) s.phase = kPhaseDone;
+            else { s.level += 1; s.phase = kPhaseScan; s.min_kept = 0xFFFFFFFFu; }
+          }
+          break;
+        }
+        default:
+          break;
+      }
+      if (s.phase != kPhaseDone) s.waves++;
+      st[g] = s;
+      if (s.phase == kPhaseScan0 || s.phase == kPhaseScan) {
+        w = s.act_count;
+        if (w) atomicAdd(&s_scan, w);
+      } else if (s.phase == kPhaseProc) {
+        w = s.curr & kWorkMask;
+        atomicAdd(&s_proc, w);
+        atomicAdd(&s_edges, s.curr >> kWorkBits);
+      }
+      if (s.phase != kPhaseDone) {
+        atomicAdd(&s_live, 1u);
+        atomicAdd(&s_live_edges, (unsigned long long)(m - s.processed));
+      }
+    }
+    unsigned long long total;
+    unsigned long long ex = block_exclusive_scan<unsigned long long>(w, sw, total);
+    if (g < G) wpref[g] = carry + ex;
+    carry += total;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    wpref[G] = carry;
+    uint32_t done = was_done;
+    if (!was_done) {
+      if (ctl->trace && ctl->waves_run < ctl->trace_cap)
+        ctl->trace[ctl->waves_run] = make_ulonglong4(globaltimer(), carry, s_proc, s_scan);
+      ctl->el_proc += s_proc;
+      ctl->el_scan += s_scan;
+      ctl->edges_proc += s_edges;
+      ctl->total_work = carry;
+      ctl->wave += 1;
+      ctl->waves_run += 1;
+      const uint32_t e = __ldcg(err);
+      uint32_t reason = kExitNone;
+      if (s_live == 0) { done = 1; reason = kExitDone; }
+      if (e) { done = 1; reason = kExitError; }
+      if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; reason = kExitError; }
+      if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; reason = kExitError; }
+      // live edges fill at most 78% of the working rows: stop so the host can
+      // compact them (a compaction costs about 1.2 ms on 128 M slots, which the
+      // shorter rows repay at this fill)
+      if (!done && ctl->csr_slots >= ctl->compact_min && 100 * s_live_edges <= 39 * ctl->csr_slots) {
+        done = 1;
+        reason = kExitCompact;
+      }
+      ctl->done = done;
+      ctl->exit_reason = reason;
+    }
+    if (use_handle) cudaGraphSetConditional(handle, done ? 0u : 1u);
+  }
+}
+
 // Kernel D: one peel wave.  The wave's work (all members' scan elements and
 // frontier elements, laid out by `wpref`) is cut into warp-sized chunks; a
 // warp walks its chunk member by member, 32 consecutive elements per
@@ -1124,15 +1357,16 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
   __shared__ uint32_t s_push_eid[kWaveWarps][kPushBuf];
   __shared__ uint32_t s_keep[kWaveWarps][kKeepBuf];
   const Control* ctl = a.ctl;
-  if (ctl->done) return;
-  const unsigned long long total = ctl->total_work;
+  // a stopped loop (host-launched waves run on until the host looks) does no
+  // work, but its blocks still hand over to the planner
+  const unsigned long long total = ctl->done ? 0ull : ctl->total_work;
   const uint32_t W = ctl->wave;
   const uint32_t G = ctl->G;
   const uint32_t lane = lane_id();
   const uint32_t wib = threadIdx.x >> 5;
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
-  const UnionRegs U(a.Up);
+  const UnionRegs U(a.Up, a.arr);
   const bool hubs = U.hub_map != nullptr;  // descriptors carry kHubDesc only when maps exist
   unsigned long long ch = total / (nwarps * 2);
   ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
@@ -1376,6 +1610,20 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
                                                  : &a.ctl->merge_chunks;
     if (sum) atomicAdd(dst, sum);
   }
+  // the last block to finish plans the next wave (threadfence-reduction
+  // pattern: every thread fences its writes, the block takes a ticket; the
+  // block holding the last ticket sees every other block's writes)
+  __shared__ uint32_t s_last;
+  __shared__ PlanShared s_plan;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&a.ctl->blocks_done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    plan_wave(a.mem, a.st, a.ctl, a.wpref, a.err, a.handle, a.use_handle, s_plan);
+    if (threadIdx.x == 0) a.ctl->blocks_done = 0;
+  }
 }
 
 // Hub maps: the vertices of highest degree (at least `min_deg`, at most the
@@ -1384,7 +1632,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
 // load instead of a search of the long row.
 //   k_hub_hist    histogram of floor(log2(degree))
 //   k_hub_assign  hub index per vertex (kInvalid below the chosen degree)
-//   k_hub_fill    scatter each hub's row into its map (warp per hub)
+//   k_hub_fill    scatter each hub's row into its map (block per hub)
 __global__ void __launch_bounds__(256) k_hub_hist(const uint32_t* __restrict__ off, uint32_t n,
                                                   uint32_t* __restrict__ hist) {
   __shared__ uint32_t sh[33];
@@ -1419,14 +1667,11 @@ __global__ void __launch_bounds__(256) k_hub_fill(const uint32_t* __restrict__ o
                                                   const unsigned long long* __restrict__ row0, uint32_t n,
                                                   const uint32_t* __restrict__ hub_vertex, uint32_t hubs,
                                                   uint32_t* __restrict__ hub_map) {
-  const uint32_t lane = lane_id();
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t k = warp; k < hubs; k += nwarps) {
+  for (uint32_t k = blockIdx.x; k < hubs; k += gridDim.x) {
     const uint32_t u = hub_vertex[k];
     const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
     uint32_t* map = hub_map + (unsigned long long)k * n;
-    for (uint32_t s = b + lane; s < e; s += 32) {
+    for (uint32_t s = b + threadIdx.x; s < e; s += blockDim.x) {
       const unsigned long long pr = __ldg(row0 + s);
       const uint32_t id = (uint32_t)pr;
       if (id < n) map[id] = (uint32_t)(pr >> 32);
@@ -1438,7 +1683,7 @@ __global__ void __launch_bounds__(256) k_hub_fill(const uint32_t* __restrict__ o
 // processed (tag >= the next wave).  The edges' states are first condensed
 // into a bitmap (one bit per edge, small enough to stay in L2), so the row
 // passes look up a bit instead of a random 8-byte state.  Mark, count, scan
-// (host), fill; warp per vertex for the row passes.
+// (host), fill; 32 vertices per warp for the row passes.
 __global__ void __launch_bounds__(256) k_compact_mark(const int2* __restrict__ es, uint32_t m,
                                                       const Control* ctl, uint32_t* __restrict__ alive) {
   const uint32_t lane = lane_id();
@@ -1465,13 +1710,25 @@ __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restric
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+  for (uint32_t base = warp * 32; base < n; base += nwarps * 32) {
+    const uint32_t u = base + lane;
+    uint32_t b = 0, e = 0;
+    if (u < n) { b = __ldg(off + u); e = __ldg(off + u + 1); }
     uint32_t c = 0;
-    for (uint32_t s = b + lane; s < e; s += 32) c += is_alive(alive, (uint32_t)(__ldg(row + s) >> 32));
+    if (u < n && e - b <= kLaneRow)
+      for (uint32_t s = b; s < e; ++s) c += is_alive(alive, (uint32_t)(__ldg(row + s) >> 32));
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    while (big) {
+      const int j = __ffs(big) - 1;
+      big &= big - 1;
+      const uint32_t bb = __shfl_sync(kFull, b, j), be = __shfl_sync(kFull, e, j);
+      uint32_t cc = 0;
+      for (uint32_t s = bb + lane; s < be; s += 32) cc += is_alive(alive, (uint32_t)(__ldg(row + s) >> 32));
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(kFull, c, d);
-    if (lane == 0) cnt[u] = c;
+      for (int d = 16; d > 0; d >>= 1) cc += __shfl_xor_sync(kFull, cc, d);
+      if (lane == (uint32_t)j) c = cc;
+    }
+    if (u < n) cnt[u] = c;
   }
 }
 
@@ -1483,20 +1740,35 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
-    uint32_t at = __ldg(off2 + u);
-    for (uint32_t s0 = b; s0 < e; s0 += 32) {
-      const uint32_t s = s0 + lane;
-      unsigned long long pr = 0;
-      bool keep = false;
-      if (s < e) {
-        pr = __ldg(row + s);
-        keep = is_alive(alive, (uint32_t)(pr >> 32));
+  for (uint32_t base = warp * 32; base < n; base += nwarps * 32) {
+    const uint32_t u = base + lane;
+    uint32_t b = 0, e = 0;
+    if (u < n) { b = __ldg(off + u); e = __ldg(off + u + 1); }
+    if (u < n && e - b <= kLaneRow) {
+      uint32_t at = __ldg(off2 + u);
+      for (uint32_t s = b; s < e; ++s) {
+        const unsigned long long pr = __ldg(row + s);
+        if (is_alive(alive, (uint32_t)(pr >> 32))) row2[at++] = pr;
       }
-      const unsigned bal = __ballot_sync(kFull, keep);
-      if (keep) row2[at + __popc(bal & ((1u << lane) - 1))] = pr;
-      at += __popc(bal);
+    }
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    while (big) {
+      const int j = __ffs(big) - 1;
+      big &= big - 1;
+      const uint32_t bb = __shfl_sync(kFull, b, j), be = __shfl_sync(kFull, e, j);
+      uint32_t at = __ldg(off2 + base + j);
+      for (uint32_t s0 = bb; s0 < be; s0 += 32) {
+        const uint32_t s = s0 + lane;
+        unsigned long long pr = 0;
+        bool keep = false;
+        if (s < be) {
+          pr = __ldg(row + s);
+          keep = is_alive(alive, (uint32_t)(pr >> 32));
+        }
+        const unsigned bal = __ballot_sync(kFull, keep);
+        if (keep) row2[at + __popc(bal & ((1u << lane) - 1))] = pr;
+        at += __popc(bal);
+      }
     }
   }
 }
@@ -1532,129 +1804,6 @@ __global__ void k_compact_commit(Union* U, const uint32_t* off2, const unsigned 
   ctl->done = 0;
 }
 
-// Planner: one block advances every member's state machine after a wave and
-// lays out the next wave's work.  Sets the CUDA-graph loop condition.
-__global__ void __launch_bounds__(1024) k_plan(const Member* __restrict__ mem, MemberState* __restrict__ st,
-                                               Control* ctl, unsigned long long* __restrict__ wpref,
-                                               uint32_t* __restrict__ err, cudaGraphConditionalHandle handle,
-                                               int use_handle) {
-  __shared__ unsigned long long sw[32];
-  __shared__ uint32_t s_live;
-  __shared__ unsigned long long s_proc, s_scan, s_edges, s_live_edges;
-  const uint32_t G = ctl->G;
-  if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; s_live_edges = 0; }
-  __syncthreads();
-  const bool was_done = ctl->done;
-  if (was_done) {
-    // the loop is stopped (host-launched waves keep coming until the host
-    // looks): the planned wave must survive untouched for a resume
-    if (threadIdx.x == 0 && use_handle) cudaGraphSetConditional(handle, 0u);
-    return;
-  }
-  unsigned long long carry = 0;
-  for (uint32_t b = 0; b < G; b += blockDim.x) {
-    const uint32_t g = b + threadIdx.x;
-    unsigned long long w = 0;
-    if (g < G && !was_done) {
-      MemberState s = st[g];
-      const uint32_t m = mem[g].m;
-      switch (s.phase) {
-        case kPhaseScan0:
-          s.act_sel ^= 1u;
-          s.act_count = s.kept;
-          s.kept = 0;
-          if (s.processed >= m) s.phase = kPhaseDone;
-          else { s.level = s.min_kept; s.min_kept = 0xFFFFFFFFu; s.phase = kPhaseScan; }
-          break;
-        case kPhaseScan: {
-          s.act_sel ^= 1u;
-          s.act_count = s.kept;
-          s.kept = 0;
-          const unsigned long long cnt = s.next >> kWorkBits;
-          if (cnt) {
-            s.curr = s.next;
-            s.next = 0;
-            s.q_sel ^= 1u;
-            s.phase = kPhaseProc;
-            s.levels++;
-            s.max_level = s.level;
-          } else if (s.act_count == 0) {
-            s.phase = kPhaseDone;
-          } else {
-            s.level = s.min_kept;  // no edge at this level: jump to the next occupied one
-          }
-          s.min_kept = 0xFFFFFFFFu;
-          break;
-        }
-        case kPhaseProc: {
-          s.processed += (uint32_t)(s.curr >> kWorkBits);
-          const unsigned long long cnt = s.next >> kWorkBits;
-          if (cnt) {
-            s.curr = s.next;
-            s.next = 0;
-            s.q_sel ^= 1u;
-          } else {
-            s.curr = 0;
-            if (s.processed >= m) s.phase = kPhaseDone;
-            else { s.level += 1; s.phase = kPhaseScan; s.min_kept = 0xFFFFFFFFu; }
-          }
-          break;
-        }
-        default:
-          break;
-      }
-      if (s.phase != kPhaseDone) s.waves++;
-      st[g] = s;
-      if (s.phase == kPhaseScan0 || s.phase == kPhaseScan) {
-        w = s.act_count;
-        if (w) atomicAdd(&s_scan, w);
-      } else if (s.phase == kPhaseProc) {
-        w = s.curr & kWorkMask;
-        atomicAdd(&s_proc, w);
-        atomicAdd(&s_edges, s.curr >> kWorkBits);
-      }
-      if (s.phase != kPhaseDone) {
-        atomicAdd(&s_live, 1u);
-        atomicAdd(&s_live_edges, (unsigned long long)(m - s.processed));
-      }
-    }
-    unsigned long long total;
-    unsigned long long ex = block_exclusive_scan<unsigned long long>(w, sw, total);
-    if (g < G) wpref[g] = carry + ex;
-    carry += total;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    wpref[G] = carry;
-    uint32_t done = was_done;
-    if (!was_done) {
-      if (ctl->trace && ctl->waves_run < ctl->trace_cap)
-        ctl->trace[ctl->waves_run] = make_ulonglong4(globaltimer(), carry, s_proc, s_scan);
-      ctl->el_proc += s_proc;
-      ctl->el_scan += s_scan;
-      ctl->edges_proc += s_edges;
-      ctl->total_work = carry;
-      ctl->wave += 1;
-      ctl->waves_run += 1;
-      const uint32_t e = *err;
-      uint32_t reason = kExitNone;
-      if (s_live == 0) { done = 1; reason = kExitDone; }
-      if (e) { done = 1; reason = kExitError; }
-      if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; reason = kExitError; }
-      if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; reason = kExitError; }
-      // live edges fill at most 78% of the working rows: stop so the host can
-      // compact them (a compaction costs about 1.2 ms on 128 M slots, which the
-      // shorter rows repay at this fill)
-      if (!done && ctl->csr_slots >= ctl->compact_min && 100 * s_live_edges <= 39 * ctl->csr_slots) {
-        done = 1;
-        reason = kExitCompact;
-      }
-      ctl->done = done;
-      ctl->exit_reason = reason;
-    }
-    if (use_handle) cudaGraphSetConditional(handle, done ? 0u : 1u);
-  }
-}
 
 // Kernel E: truss per slot = level + 2 (pkt.rs:524-526); self-loop slots 2.
 template <typename OutT>

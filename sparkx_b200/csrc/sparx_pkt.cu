@@ -410,10 +410,36 @@ struct UnionJob {
 template <class T>
 T* at(Engine& E, size_t off) { return reinterpret_cast<T*>(E.ws + off); }
 
-int build_peel_graph(Engine& E, const UnionJob& J, cudaStream_t) {
+PeelArrays peel_arrays(const Union& U) {
+  PeelArrays a{};
+  a.ocol = U.ocol;
+  a.osrc = U.osrc;
+  a.es = U.es;
+  a.act0 = U.act[0];
+  a.act1 = U.act[1];
+  a.q0 = U.q[0];
+  a.q1 = U.q[1];
+  a.qd0 = U.qd[0];
+  a.qd1 = U.qd[1];
+  a.hub_slot = U.hub_slot;
+  a.hub_map = U.hub_map;
+  a.n = U.n;
+  return a;
+}
+
+#ifndef SPARX_WAVES_PER_ITERATION
+#define SPARX_WAVES_PER_ITERATION 4
+#endif
+constexpr int kWavesPerIteration = SPARX_WAVES_PER_ITERATION;
+
+int build_peel_graph(Engine& E, const UnionJob& J, const PeelArrays& arr) {
   const Layout& L = J.L;
   std::vector<size_t> key = {(size_t)E.ws, L.uni, L.mem, L.st, L.ctl, L.wpref, L.cnt, (size_t)J.members.size(),
                              (size_t)E.wave_blocks};
+  // the arrays are baked into the captured kernels' parameters
+  static_assert(sizeof(PeelArrays) % sizeof(size_t) == 0, "PeelArrays is keyed word by word");
+  const size_t* words = reinterpret_cast<const size_t*>(&arr);
+  key.insert(key.end(), words, words + sizeof(PeelArrays) / sizeof(size_t));
   if (E.peel.exec && E.peel.key == key) return SPARX_OK;
   if (E.peel.exec) {
     cudaGraphExecDestroy(E.peel.exec);
@@ -434,14 +460,18 @@ int build_peel_graph(Engine& E, const UnionJob& J, cudaStream_t) {
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   WaveArgs wa;
   wa.Up = at<Union>(E, L.uni);
+  wa.arr = arr;
   wa.mem = at<Member>(E, L.mem);
   wa.st = at<MemberState>(E, L.st);
   wa.ctl = at<Control>(E, L.ctl);
   wa.wpref = at<unsigned long long>(E, L.wpref);
   wa.err = &at<Counters>(E, L.cnt)->err;
+  wa.handle = h;
+  wa.use_handle = 1;
   CU(cudaStreamBeginCaptureToGraph(E.capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-  k_wave<<<E.wave_blocks, 256, 0, E.capture>>>(wa);
-  k_plan<<<1, 1024, 0, E.capture>>>(wa.mem, wa.st, wa.ctl, at<unsigned long long>(E, L.wpref), wa.err, h, 1);
+  // several waves per loop iteration: a wave that finds the loop stopped does
+  // nothing, and the condition is read once per iteration
+  for (int i = 0; i < kWavesPerIteration; ++i) k_wave<<<E.wave_blocks, 256, 0, E.capture>>>(wa);
   cudaGraph_t captured;
   CU(cudaStreamEndCapture(E.capture, &captured));
   cudaGraphExec_t ex;
@@ -467,7 +497,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   uint32_t* osrc = at<uint32_t>(E, L.osrc);
   int2* es = at<int2>(E, L.es);
   Member* dmem = at<Member>(E, L.mem);
-  const int vgrid = grid_for((unsigned long long)N * 32, 256, E.sm_count * 32);
+  const int vgrid = grid_for(N, 256, E.sm_count * 32);  // row kernels: 32 vertices per warp
 
   CU(cudaEventRecord(E.tev[1], s));
   {
@@ -506,8 +536,11 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   if (2 * m + hc.self_loops != W) { J.err = kErrAsym; return SPARX_E_INVALID_CSR; }
   for (const Member& M : J.members)
     if (M.m > kEidMask) { set_error("a graph has >= 2^28 edges"); return SPARX_E_TOO_LARGE; }
-  k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, row0);
-  k_orient_reverse<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, row0, err);
+  {
+    uint32_t* owner = at<uint32_t>(E, L.q0);  // in-slot owners; the q buffers are idle until the peel
+    k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, row0, owner);
+    k_orient_reverse<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(J.nbr, owner, W, opos, ocol, row0, err);
+  }
   J.launches += 2;
   // hub maps: the smallest power-of-two degree bound (>= kHubMinDegree) whose
   // vertices fit the reserved maps; hist[b] counts degrees in [2^(b-1), 2^b)
@@ -532,7 +565,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     k_hub_assign<<<grid_for(N, 256, E.sm_count * 8), 256, 0, s>>>(J.off, N, hub_min_deg, hubs, hslot, hvert,
                                                                   &cnt->hub_count);
     CU(cudaMemsetAsync(hmap, 0xFF, 4ull * hubs * N, s));
-    k_hub_fill<<<grid_for(32ull * hubs, 256, E.sm_count * 4), 256, 0, s>>>(J.off, row0, N, hvert, hubs, hmap);
+    k_hub_fill<<<std::min<uint32_t>(hubs, E.sm_count * 8), 256, 0, s>>>(J.off, row0, N, hvert, hubs, hmap);
     J.launches += 2;
     d_hub_slot = hslot;
     d_hub_map = hmap;
@@ -606,30 +639,29 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaEventRecord(E.tev[4], s));
     WaveArgs wa;
     wa.Up = at<Union>(E, L.uni);
+    wa.arr = peel_arrays(U);
     wa.mem = dmem;
     wa.st = at<MemberState>(E, L.st);
     wa.ctl = at<Control>(E, L.ctl);
     wa.wpref = at<unsigned long long>(E, L.wpref);
     wa.err = err;
+    wa.handle = cudaGraphConditionalHandle{};
+    wa.use_handle = 0;
     Control* hctl = (Control*)E.pinned_small;
     const uint32_t* cur_off = J.off;
     const unsigned long long* cur_row = row0;
     int next_buf = 0;
     for (;;) {
       if (O.loop == SPARX_LOOP_GRAPH) {
-        int rc = build_peel_graph(E, J, s);
+        int rc = build_peel_graph(E, J, wa.arr);
         if (rc) return rc;
         CU(cudaGraphLaunch(E.peel.exec, s));
         CU(cudaMemcpyAsync(hctl, wa.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
       } else {
         for (;;) {
-          for (int i = 0; i < 16; ++i) {
-            k_wave<<<E.wave_blocks, 256, 0, s>>>(wa);
-            k_plan<<<1, 1024, 0, s>>>(wa.mem, wa.st, wa.ctl, at<unsigned long long>(E, L.wpref), err,
-                                      cudaGraphConditionalHandle{}, 0);
-          }
-          J.launches += 32;
+          for (int i = 0; i < 16; ++i) k_wave<<<E.wave_blocks, 256, 0, s>>>(wa);
+          J.launches += 16;
           CU(cudaMemcpyAsync(hctl, wa.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
           CU(cudaStreamSynchronize(s));
           if (hctl->done) break;
@@ -692,9 +724,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       std::fclose(f);
     }
   }
-  // each WHILE-loop iteration is one wave kernel + one planner kernel
+  // each WHILE-loop iteration is one wave kernel (its last block plans)
   if (!J.support_only && O.loop == SPARX_LOOP_GRAPH)
-    J.launches += 2 * (uint32_t)std::max<unsigned long long>(J.ctl.waves_run, 1);
+    J.launches += (uint32_t)std::max<unsigned long long>(J.ctl.waves_run, 1);
   J.err = hc.err;
   CU(cudaEventElapsedTime(&J.ms_orient, E.tev[1], E.tev[2]));
   CU(cudaEventElapsedTime(&J.ms_support, E.tev[2], E.tev[3]));
@@ -1546,7 +1578,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   CU(cudaStreamSynchronize(s));
   if (hc.err) return status_from_flags(hc.err);
 
-  const int vgrid = grid_for((unsigned long long)N * 32, 256, sm * 32);
+  const int vgrid = grid_for(N, 256, sm * 32);  // row kernels: 32 vertices per warp
   k_orient_count<<<vgrid, 256, 0, s>>>(off, d_nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus);
   exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, (uint32_t*)P(L.tiles), (uint32_t*)&cnt->grand, s);
   uint32_t m32 = 0;
@@ -1557,8 +1589,9 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   const uint64_t m = m32;
   if (2 * m + hc.self_loops != width) return SPARX_E_INVALID_CSR;
   if (m > kEidMask) return SPARX_E_TOO_LARGE;
-  k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, row0);
-  k_orient_reverse<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, row0, err);
+  k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, row0, (uint32_t*)P(L.q0));
+  k_orient_reverse<<<grid_for(width, 256, sm * 16), 256, 0, s>>>(d_nbr, (uint32_t*)P(L.q0), width, opos, ocol,
+                                                                row0, err);
 
   CU(cudaMemsetAsync(es, 0, 8 * std::max<uint64_t>(m, 1), s));
   {
@@ -1610,16 +1643,16 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   k_peel_init<<<1, 1024, 0, s>>>(dM, dS, dC, wpref, 1);
   WaveArgs wa;
   wa.Up = dU;
+  wa.arr = peel_arrays(U);
   wa.mem = dM;
   wa.st = dS;
   wa.ctl = dC;
   wa.wpref = wpref;
   wa.err = err;
+  wa.handle = cudaGraphConditionalHandle{};
+  wa.use_handle = 0;
   for (;;) {
-    for (int i = 0; i < 16; ++i) {
-      k_wave<<<wave_blocks, 256, 0, s>>>(wa);
-      k_plan<<<1, 1024, 0, s>>>(dM, dS, dC, wpref, err, cudaGraphConditionalHandle{}, 0);
-    }
+    for (int i = 0; i < 16; ++i) k_wave<<<wave_blocks, 256, 0, s>>>(wa);
     uint32_t done = 0;
     CU(cudaMemcpyAsync(&done, &dC->done, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));

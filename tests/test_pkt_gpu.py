@@ -132,7 +132,7 @@ def test_device_api_matches_host_api():
                         stream.cuda_stream)
     torch.cuda.synchronize()
     assert np.array_equal(d_out.cpu().numpy(), host)
-    assert st.waves > 0 and st.launches > 2 * st.waves
+    assert st.waves > 0 and st.launches > st.waves  # one wave kernel per wave, plus preparation
 
 
 def test_algopkt_api(tmp_path, monkeypatch):
