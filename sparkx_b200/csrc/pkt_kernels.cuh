@@ -350,11 +350,56 @@ __global__ void k_shift_ids(uint32_t* __restrict__ ids, unsigned long long count
 }
 
 // ---------------------------------------------------------------------------
+// Exclusive scan across the block (all threads call it); `total` is the
+// block sum.  smem_warp holds one value per warp.
+template <class T>
+__device__ __forceinline__ T block_exclusive_scan(T x, T* smem_warp, T& total) {
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  T v = x;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    T o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
+  }
+  if (lane == 31) smem_warp[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    T w = lane < (uint32_t)nw ? smem_warp[lane] : T(0);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      T o = __shfl_up_sync(kFull, w, d);
+      if (lane >= (uint32_t)d) w += o;
+    }
+    if (lane < (uint32_t)nw) smem_warp[lane] = w;
+  }
+  __syncthreads();
+  T warp_off = wid ? smem_warp[wid - 1] : T(0);
+  total = smem_warp[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_off + v - x;
+}
+
 // Row kernels take 32 consecutive vertices per warp: a row of at most
 // kLaneRow entries is walked by its own lane, longer rows by the whole warp
 // one at a time, so low-degree vertices (most of a skewed graph) keep all
 // lanes busy.
 constexpr uint32_t kLaneRow = 32;
+
+// Rows longer than kWarpRow entries (by original degree) are oriented and
+// compacted by a block each (the *_big kernels over the list k_big_rows
+// builds); the others by their lane or their warp.
+constexpr uint32_t kWarpRow = 2048;
+
+__device__ __forceinline__ bool big_row(const uint32_t* __restrict__ off0, uint32_t u) {
+  return __ldg(off0 + u + 1) - __ldg(off0 + u) > kWarpRow;
+}
+
+__global__ void __launch_bounds__(256) k_big_rows(const uint32_t* __restrict__ off0, uint32_t n,
+                                                  uint32_t* __restrict__ list, uint32_t* __restrict__ count) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+    if (big_row(off0, u)) list[atomicAdd(count, 1u)] = u;
+}
 
 // Kernel B1: per-row validation + oriented out-degree.
 //   rows strictly ascending (equal -> multigraph), counts self-loops, and
@@ -364,7 +409,9 @@ __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict
                                                       uint32_t* __restrict__ dplus,
                                                       unsigned long long* __restrict__ self_loops,
                                                       uint32_t* __restrict__ err,
-                                                      uint32_t* __restrict__ max_dplus) {
+                                                      uint32_t* __restrict__ max_dplus,
+                                                      const uint32_t* __restrict__ big_list,
+                                                      const uint32_t* __restrict__ big_count) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -389,7 +436,8 @@ __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict
         cnt += rank_less(e - b, u, deg_of(off, v), v);
       }
     }
-    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    const bool blk = u < n && e - b > kWarpRow;  // counted below, a block per row
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow && !blk);
     while (big) {
       const int j = __ffs(big) - 1;
       big &= big - 1;
@@ -411,9 +459,34 @@ __global__ void __launch_bounds__(256) k_orient_count(const uint32_t* __restrict
       for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(kFull, c, d);
       if (lane == (uint32_t)j) cnt = c;
     }
-    if (u < n) {
+    if (u < n && !blk) {
       dplus[u] = cnt;
       mxd = max(mxd, cnt);
+    }
+  }
+  // rows longer than kWarpRow: block-wide, one row at a time
+  __shared__ unsigned long long s_red[32];
+  const uint32_t nbig = *big_count;
+  for (uint32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+    const uint32_t bu = big_list[r];
+    const uint32_t bb = __ldg(off + bu), be = __ldg(off + bu + 1), du = be - bb;
+    unsigned long long c = 0;
+    for (uint32_t s = bb + threadIdx.x; s < be; s += blockDim.x) {
+      const uint32_t v = __ldg(nbr + s);
+      if (v >= n) { flags |= kErrRange; continue; }
+      if (s + 1 < be) {
+        const uint32_t nx = __ldg(nbr + s + 1);
+        if (nx == v) flags |= kErrMulti;
+        else if (nx < v) flags |= kErrUnsorted;
+      }
+      if (v == bu) { selfc++; continue; }
+      c += rank_less(du, bu, deg_of(off, v), v);
+    }
+    unsigned long long total;
+    block_exclusive_scan<unsigned long long>(c, s_red, total);
+    if (threadIdx.x == 0) {
+      dplus[bu] = (uint32_t)total;
+      mxd = max(mxd, (uint32_t)total);
     }
   }
   if (flags) atomicOr(err, flags);
@@ -440,7 +513,9 @@ __global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict_
                                                      uint32_t* __restrict__ ocol,
                                                      uint32_t* __restrict__ osrc,
                                                      unsigned long long* __restrict__ row0,
-                                                     uint32_t* __restrict__ owner) {
+                                                     uint32_t* __restrict__ owner,
+                                                     const uint32_t* __restrict__ big_list,
+                                                     const uint32_t* __restrict__ big_count) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -466,7 +541,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict_
         owner[s] = own;
       }
     }
-    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow && e - b <= kWarpRow);
     while (big) {
       const int j = __ffs(big) - 1;
       big &= big - 1;
@@ -494,6 +569,43 @@ __global__ void __launch_bounds__(256) k_orient_fill(const uint32_t* __restrict_
         }
         p0 += __popc(bal);
       }
+    }
+  }
+  // rows longer than kWarpRow: a block per row, out-slots placed in order by
+  // a block-wide scan over chunks of four consecutive slots per thread
+  __shared__ uint32_t s_scan[32];
+  const uint32_t nbig = *big_count;
+  for (uint32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+    const uint32_t bu = big_list[r];
+    const uint32_t bb = __ldg(off + bu), be = __ldg(off + bu + 1), du = be - bb;
+    uint32_t p0 = __ldg(opos + bu);
+    for (uint32_t base = bb; base < be; base += 4 * blockDim.x) {
+      const uint32_t s0 = base + 4 * threadIdx.x;
+      uint32_t v[4], outm = 0, nout = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        v[i] = 0;
+        const uint32_t s = s0 + i;
+        if (s < be) {
+          v[i] = __ldg(nbr + s);
+          uint32_t own = kInvalid;
+          if (v[i] == bu || v[i] >= n) row0[s] = make_pair(v[i], kInvalid);
+          else if (rank_less(du, bu, deg_of(off, v[i]), v[i])) { outm |= 1u << i; ++nout; }
+          else own = bu;
+          owner[s] = own;
+        }
+      }
+      uint32_t total;
+      uint32_t p = p0 + block_exclusive_scan<uint32_t>(nout, s_scan, total);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (outm & (1u << i)) {
+          ocol[p] = v[i];
+          osrc[p] = bu;
+          row0[s0 + i] = make_pair(v[i], p);
+          ++p;
+        }
+      p0 += total;
     }
   }
 }
@@ -533,33 +645,6 @@ constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-template <class T>
-__device__ __forceinline__ T block_exclusive_scan(T x, T* smem_warp, T& total) {
-  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
-  T v = x;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    T o = __shfl_up_sync(kFull, v, d);
-    if (lane >= (uint32_t)d) v += o;
-  }
-  if (lane == 31) smem_warp[wid] = v;
-  __syncthreads();
-  if (wid == 0) {
-    const int nw = blockDim.x >> 5;
-    T w = lane < (uint32_t)nw ? smem_warp[lane] : T(0);
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      T o = __shfl_up_sync(kFull, w, d);
-      if (lane >= (uint32_t)d) w += o;
-    }
-    if (lane < (uint32_t)nw) smem_warp[lane] = w;
-  }
-  __syncthreads();
-  T warp_off = wid ? smem_warp[wid - 1] : T(0);
-  total = smem_warp[(blockDim.x >> 5) - 1];
-  __syncthreads();
-  return warp_off + v - x;
-}
 
 template <class T, class F>
 __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(F f, unsigned long long count, T* tile_sums) {
@@ -1132,7 +1217,7 @@ struct QueueStart {
 constexpr int kPushBuf = 64;
 constexpr int kWaveThreads = 256;
 #ifndef SPARX_WAVE_MINB
-#define SPARX_WAVE_MINB 6  // resident 256-thread blocks per SM the register budget targets
+#define SPARX_WAVE_MINB 7  // resident 256-thread blocks per SM the register budget targets
 #endif
 constexpr int kWaveWarps = kWaveThreads / 32;
 // kept active-list entries staged per warp before one atomic reserves their
@@ -1706,7 +1791,8 @@ __device__ __forceinline__ bool is_alive(const uint32_t* __restrict__ alive, uin
 __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restrict__ off,
                                                        const unsigned long long* __restrict__ row, uint32_t n,
                                                        const uint32_t* __restrict__ alive,
-                                                       uint32_t* __restrict__ cnt) {
+                                                       uint32_t* __restrict__ cnt,
+                                                       const uint32_t* __restrict__ off0) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1717,7 +1803,8 @@ __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restric
     uint32_t c = 0;
     if (u < n && e - b <= kLaneRow)
       for (uint32_t s = b; s < e; ++s) c += is_alive(alive, (uint32_t)(__ldg(row + s) >> 32));
-    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    const bool blk = u < n && e - b > kLaneRow && big_row(off0, u);
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow && !blk);
     while (big) {
       const int j = __ffs(big) - 1;
       big &= big - 1;
@@ -1728,7 +1815,7 @@ __global__ void __launch_bounds__(256) k_compact_count(const uint32_t* __restric
       for (int d = 16; d > 0; d >>= 1) cc += __shfl_xor_sync(kFull, cc, d);
       if (lane == (uint32_t)j) c = cc;
     }
-    if (u < n) cnt[u] = c;
+    if (u < n && !blk) cnt[u] = c;
   }
 }
 
@@ -1736,7 +1823,8 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
                                                       const unsigned long long* __restrict__ row, uint32_t n,
                                                       const uint32_t* __restrict__ alive,
                                                       const uint32_t* __restrict__ off2,
-                                                      unsigned long long* __restrict__ row2) {
+                                                      unsigned long long* __restrict__ row2,
+                                                      const uint32_t* __restrict__ off0) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1751,7 +1839,7 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
         if (is_alive(alive, (uint32_t)(pr >> 32))) row2[at++] = pr;
       }
     }
-    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow && !big_row(off0, u));
     while (big) {
       const int j = __ffs(big) - 1;
       big &= big - 1;
@@ -1769,6 +1857,63 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
         if (keep) row2[at + __popc(bal & ((1u << lane) - 1))] = pr;
         at += __popc(bal);
       }
+    }
+  }
+}
+
+// Big rows, a block each.  Count: block sum.  Fill: chunks of 1024 entries,
+// four consecutive per thread, placed by a block-wide exclusive scan so the
+// row keeps its order.
+__global__ void __launch_bounds__(256) k_compact_count_big(const uint32_t* __restrict__ off,
+                                                           const unsigned long long* __restrict__ row,
+                                                           const uint32_t* __restrict__ alive,
+                                                           uint32_t* __restrict__ cnt,
+                                                           const uint32_t* __restrict__ list,
+                                                           const uint32_t* __restrict__ count) {
+  __shared__ unsigned long long sw[32];
+  const uint32_t nbig = *count;
+  for (uint32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+    const uint32_t u = list[r];
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    unsigned long long c = 0;
+#pragma unroll 4
+    for (uint32_t s = b + threadIdx.x; s < e; s += blockDim.x) c += is_alive(alive, (uint32_t)(__ldg(row + s) >> 32));
+    unsigned long long total;
+    block_exclusive_scan<unsigned long long>(c, sw, total);
+    if (threadIdx.x == 0) cnt[u] = (uint32_t)total;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_compact_fill_big(const uint32_t* __restrict__ off,
+                                                          const unsigned long long* __restrict__ row,
+                                                          const uint32_t* __restrict__ alive,
+                                                          const uint32_t* __restrict__ off2,
+                                                          unsigned long long* __restrict__ row2,
+                                                          const uint32_t* __restrict__ list,
+                                                          const uint32_t* __restrict__ count) {
+  __shared__ uint32_t sw[32];
+  const uint32_t nbig = *count;
+  for (uint32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+    const uint32_t u = list[r];
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    uint32_t at = __ldg(off2 + u);
+    for (uint32_t base = b; base < e; base += 4 * blockDim.x) {
+      const uint32_t s0 = base + 4 * threadIdx.x;
+      unsigned long long pr[4];
+      uint32_t keep = 0, nk = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        pr[i] = s0 + i < e ? __ldg(row + s0 + i) : 0ull;
+        const bool k = s0 + i < e && is_alive(alive, (uint32_t)(pr[i] >> 32));
+        keep |= (uint32_t)k << i;
+        nk += k;
+      }
+      uint32_t total;
+      uint32_t pos = at + block_exclusive_scan<uint32_t>(nk, sw, total);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (keep & (1u << i)) row2[pos++] = pr[i];
+      at += total;
     }
   }
 }

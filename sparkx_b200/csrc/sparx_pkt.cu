@@ -69,6 +69,7 @@ struct Counters {  // device scalars
   uint32_t hcursor;      //                      next heavy vertex
   uint32_t heavy_count;  //                      heavy vertices listed
   uint32_t hub_count;    // hub maps assigned
+  uint32_t big_count;    // rows compacted by a block each
 };
 
 
@@ -77,6 +78,7 @@ struct Layout {
   size_t off, nbr, row0, dplus, opos, ocol, osrc, es, act0, act1, q0, q1, qd0, qd1, out, stage0, stage1;
   size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
   size_t alive;                   // compaction: one bit per edge, set while it is unprocessed
+  size_t big;                     // compaction: rows longer than kWarpRow (a block each)
   size_t hub_slot, hub_vertex, hub_hist, hub_map;  // hub maps (hub_cap == 0: none)
   uint32_t hub_cap;
   size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
@@ -125,6 +127,7 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   L.rowA = take(8 * W);
   L.rowB = take(8 * W);
   L.alive = take(4 * ((M + 31) / 32));
+  L.big = take(4 * (W / kWarpRow + 1));
   L.hub_cap = hub_capacity(N, W, G);
   if (L.hub_cap) {
     L.hub_slot = take(4 * N);
@@ -516,7 +519,13 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     k_hub_hist<<<grid_for(N, 256, E.sm_count * 4), 256, 0, s>>>(J.off, N, hub_hist);
     J.launches += 1;
   }
-  k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus);
+  // rows orientation and compaction give a block each (listed by original degree)
+  uint32_t* big = at<uint32_t>(E, L.big);
+  CU(cudaMemsetAsync(&cnt->big_count, 0, 4, s));
+  k_big_rows<<<grid_for(N, 256, E.sm_count * 8), 256, 0, s>>>(J.off, N, big, &cnt->big_count);
+  k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus, big,
+                                       &cnt->big_count);
+  J.launches += 1;
   exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
   J.launches += 4;
   CU(cudaMemcpyAsync(dmem, J.members.data(), sizeof(Member) * G, cudaMemcpyHostToDevice, s));
@@ -538,7 +547,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     if (M.m > kEidMask) { set_error("a graph has >= 2^28 edges"); return SPARX_E_TOO_LARGE; }
   {
     uint32_t* owner = at<uint32_t>(E, L.q0);  // in-slot owners; the q buffers are idle until the peel
-    k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, row0, owner);
+    k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, row0, owner, big, &cnt->big_count);
     k_orient_reverse<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(J.nbr, owner, W, opos, ocol, row0, err);
   }
   J.launches += 2;
@@ -674,9 +683,11 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       uint32_t* alive = at<uint32_t>(E, L.alive);
       k_compact_mark<<<grid_for((m + 31) / 32 * 32ull, 256, E.sm_count * 16), 256, 0, s>>>(es, (uint32_t)m,
                                                                                           wa.ctl, alive);
-      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, dplus);
+      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, dplus, J.off);
+      k_compact_count_big<<<E.sm_count * 2, 256, 0, s>>>(cur_off, cur_row, alive, dplus, big, &cnt->big_count);
       exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
-      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, off2, row2);
+      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, off2, row2, J.off);
+      k_compact_fill_big<<<E.sm_count * 2, 256, 0, s>>>(cur_off, cur_row, alive, off2, row2, big, &cnt->big_count);
       k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + N, wa.ctl);
       const uint32_t per = std::max<uint32_t>(1, (uint32_t)(E.sm_count * 8) / std::max<uint32_t>(G, 1));
       k_refresh_desc<<<G * per, 256, 0, s>>>(wa.Up, dmem, wa.st, G, per);
@@ -1520,6 +1531,7 @@ Layout make_noalloc_layout(uint64_t N, uint64_t W) {
   L.q1 = L.q0 + 8 * M;
   L.qd0 = take(16 * M);
   L.qd1 = take(16 * M);
+  L.big = take(4 * (W / kWarpRow + 1));
   const uint64_t tiles = (std::max<uint64_t>(N + 1, M + 1) + kScanTile - 1) / kScanTile + 2;
   L.tiles = take(8 * tiles);
   L.ctl = take(sizeof(Control));
@@ -1579,7 +1591,10 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   if (hc.err) return status_from_flags(hc.err);
 
   const int vgrid = grid_for(N, 256, sm * 32);  // row kernels: 32 vertices per warp
-  k_orient_count<<<vgrid, 256, 0, s>>>(off, d_nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus);
+  uint32_t* big = (uint32_t*)P(L.big);  // big_count was cleared with the counters above
+  k_big_rows<<<grid_for(N, 256, sm * 8), 256, 0, s>>>(off, N, big, &cnt->big_count);
+  k_orient_count<<<vgrid, 256, 0, s>>>(off, d_nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus, big,
+                                       &cnt->big_count);
   exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, (uint32_t*)P(L.tiles), (uint32_t*)&cnt->grand, s);
   uint32_t m32 = 0;
   CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
@@ -1589,7 +1604,8 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   const uint64_t m = m32;
   if (2 * m + hc.self_loops != width) return SPARX_E_INVALID_CSR;
   if (m > kEidMask) return SPARX_E_TOO_LARGE;
-  k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, row0, (uint32_t*)P(L.q0));
+  k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, row0, (uint32_t*)P(L.q0), big,
+                                      &cnt->big_count);
   k_orient_reverse<<<grid_for(width, 256, sm * 16), 256, 0, s>>>(d_nbr, (uint32_t*)P(L.q0), width, opos, ocol,
                                                                 row0, err);
 
