@@ -786,6 +786,33 @@ __global__ void __launch_bounds__(256) k_support_balanced(
         if (cnt) atomicAdd(&es[e].x, cnt);
       }
       i = e_last;
+      // fast path: while the next 32 elements all lie inside edge i, the
+      // lists and the element offsets are the same for the whole warp
+      const unsigned long long nb = kb + 32;
+      const unsigned long long e_end = i + 1 < m ? spref[i + 1] : total;
+      if (nb + 32 <= min(kend, e_end)) {
+        const unsigned long long e_start = spref[i];
+        const uint32_t a = __ldg(osrc + i), b = __ldg(ocol + i);
+        const uint32_t ab = __ldg(opos + a), ae = __ldg(opos + a + 1);
+        const uint32_t bb = __ldg(opos + b), be = __ldg(opos + b + 1);
+        const bool a_short = ae - ab <= be - bb;
+        const uint32_t fsb = a_short ? ab : bb, flb = a_short ? bb : ab, fle = a_short ? be : ae;
+        const unsigned long long stop = min(kend, e_end);
+        do {
+          kb += 32;
+          const uint32_t fo = (uint32_t)(kb + lane - e_start);
+          const uint32_t c = __ldg(ocol + fsb + fo);
+          const uint32_t q = lower_bound_u32(ocol, flb, fle, c);
+          const bool fh = q < fle && __ldg(ocol + q) == c;
+          if (fh) {
+            atomicAdd(&es[fsb + fo].x, 1);
+            atomicAdd(&es[q].x, 1);
+            found_total++;
+          }
+          const int cnt = __popc(__ballot_sync(kFull, fh));
+          if (lane == 0 && cnt) atomicAdd(&es[i].x, cnt);
+        } while (kb + 64 <= stop);
+      }
     }
   }
 #pragma unroll
