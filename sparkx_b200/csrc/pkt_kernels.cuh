@@ -709,6 +709,12 @@ struct LoadU32 {
 };
 
 // support work of oriented edge e = min(d+(src), d+(dst))
+#ifndef SPARX_SAMPLED_LIST
+#define SPARX_SAMPLED_LIST 64
+#endif
+// longer lists from this length on are searched through 32 samples
+constexpr uint32_t kSampledList = SPARX_SAMPLED_LIST;
+
 struct SupportWork {
   const uint32_t* opos;
   const uint32_t* osrc;
@@ -736,7 +742,9 @@ template <class StartF>
 __device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i, uint32_t count,
                                                 unsigned long long j, bool valid);
 
-__global__ void __launch_bounds__(256) k_support_balanced(
+// 8 resident blocks per SM (32 registers): the pass is latency-bound and
+// loses more to fewer warps than to the few spilled values
+__global__ void __launch_bounds__(256, 8) k_support_balanced(
     const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
     const uint32_t* __restrict__ osrc, const unsigned long long* __restrict__ spref, uint32_t m,
     int2* __restrict__ es, unsigned long long* __restrict__ tri_total, uint32_t* __restrict__ err) {
@@ -798,12 +806,28 @@ __global__ void __launch_bounds__(256) k_support_balanced(
         const bool a_short = ae - ab <= be - bb;
         const uint32_t fsb = a_short ? ab : bb, flb = a_short ? bb : ab, fle = a_short ? be : ae;
         const unsigned long long stop = min(kend, e_end);
+        // a long list is narrowed first through 32 evenly spaced samples
+        // (one gather per edge, then shuffles), leaving ~1/32 of it to search
+        const uint32_t flen = fle - flb;
+        const bool sampled = flen >= kSampledList;
+        const uint32_t smp = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)lane * flen) >> 5)) : 0u;
         do {
           kb += 32;
           const uint32_t fo = (uint32_t)(kb + lane - e_start);
           const uint32_t c = __ldg(ocol + fsb + fo);
-          const uint32_t q = lower_bound_u32(ocol, flb, fle, c);
-          const bool fh = q < fle && __ldg(ocol + q) == c;
+          uint32_t lo = flb, hi = fle;
+          if (sampled) {
+            uint32_t t = 0;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+              const uint32_t cand = __shfl_sync(kFull, smp, t + d);
+              if (cand <= c) t += d;
+            }
+            lo = flb + (uint32_t)(((unsigned long long)t * flen) >> 5);
+            hi = t == 31 ? fle : flb + (uint32_t)(((unsigned long long)(t + 1) * flen) >> 5);
+          }
+          const uint32_t q = lower_bound_u32(ocol, lo, hi, c);
+          const bool fh = q < hi && __ldg(ocol + q) == c;
           if (fh) {
             atomicAdd(&es[fsb + fo].x, 1);
             atomicAdd(&es[q].x, 1);
