@@ -1912,10 +1912,10 @@ __global__ void __launch_bounds__(256) k_compact_fill(const uint32_t* __restrict
   }
 }
 
-// Big rows, a block each.  Count: block sum.  Fill: chunks of 1024 entries,
-// four consecutive per thread, placed by a block-wide exclusive scan so the
-// row keeps its order.
-__global__ void __launch_bounds__(256) k_compact_count_big(const uint32_t* __restrict__ off,
+// Big rows, a block of 1024 threads each.  Count: block sum.  Fill: chunks of
+// 4096 entries, four consecutive per thread, placed by a block-wide exclusive
+// scan so the row keeps its order.
+__global__ void __launch_bounds__(1024) k_compact_count_big(const uint32_t* __restrict__ off,
                                                            const unsigned long long* __restrict__ row,
                                                            const uint32_t* __restrict__ alive,
                                                            uint32_t* __restrict__ cnt,
@@ -1935,7 +1935,7 @@ __global__ void __launch_bounds__(256) k_compact_count_big(const uint32_t* __res
   }
 }
 
-__global__ void __launch_bounds__(256) k_compact_fill_big(const uint32_t* __restrict__ off,
+__global__ void __launch_bounds__(1024) k_compact_fill_big(const uint32_t* __restrict__ off,
                                                           const unsigned long long* __restrict__ row,
                                                           const uint32_t* __restrict__ alive,
                                                           const uint32_t* __restrict__ off2,

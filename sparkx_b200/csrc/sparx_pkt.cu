@@ -684,10 +684,11 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       k_compact_mark<<<grid_for((m + 31) / 32 * 32ull, 256, E.sm_count * 16), 256, 0, s>>>(es, (uint32_t)m,
                                                                                           wa.ctl, alive);
       k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, dplus, J.off);
-      k_compact_count_big<<<E.sm_count * 2, 256, 0, s>>>(cur_off, cur_row, alive, dplus, big, &cnt->big_count);
+      k_compact_count_big<<<E.sm_count * 2, 1024, 0, s>>>(cur_off, cur_row, alive, dplus, big, &cnt->big_count);
       exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
       k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, off2, row2, J.off);
-      k_compact_fill_big<<<E.sm_count * 2, 256, 0, s>>>(cur_off, cur_row, alive, off2, row2, big, &cnt->big_count);
+      k_compact_fill_big<<<E.sm_count * 2, 1024, 0, s>>>(cur_off, cur_row, alive, off2, row2, big,
+                                                         &cnt->big_count);
       k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + N, wa.ctl);
       const uint32_t per = std::max<uint32_t>(1, (uint32_t)(E.sm_count * 8) / std::max<uint32_t>(G, 1));
       k_refresh_desc<<<G * per, 256, 0, s>>>(wa.Up, dmem, wa.st, G, per);
