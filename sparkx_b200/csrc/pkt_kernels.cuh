@@ -1467,10 +1467,10 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
       if (e) { done = 1; reason = kExitError; }
       if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; reason = kExitError; }
       if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; reason = kExitError; }
-      // live edges fill at most 78% of the working rows: stop so the host can
-      // compact them (a compaction costs about 1.2 ms on 128 M slots, which the
-      // shorter rows repay at this fill)
-      if (!done && ctl->csr_slots >= ctl->compact_min && 100 * s_live_edges <= 39 * ctl->csr_slots) {
+      // live edges fill at most 85% of the working rows: stop so the host can
+      // compact them (a compaction is a few passes over the rows, which the
+      // shorter rows repay at this fill; 78% and 90% measured slower)
+      if (!done && ctl->csr_slots >= ctl->compact_min && 200 * s_live_edges <= 85 * ctl->csr_slots) {
         done = 1;
         reason = kExitCompact;
       }
@@ -1504,8 +1504,10 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
   const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   const UnionRegs U(a.Up, a.arr);
   const bool hubs = U.hub_map != nullptr;  // descriptors carry kHubDesc only when maps exist
-  unsigned long long ch = total / (nwarps * 2);
-  ch = min(max((ch + 31) & ~31ull, 32ull), 4096ull);
+  // one chunk per warp: finer chunks (and any cap on their size) measured
+  // slower, the search for a chunk's first entry is paid once per warp
+  unsigned long long ch = total / nwarps;
+  ch = max((ch + 31) & ~31ull, 32ull);
   uint32_t hits = 0, n_merge = 0, n_lane = 0, n_chunk = 0;
   PushStage ps{s_push_eid[wib], 0};
 
