@@ -806,11 +806,13 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
         const bool a_short = ae - ab <= be - bb;
         const uint32_t fsb = a_short ? ab : bb, flb = a_short ? bb : ab, fle = a_short ? be : ae;
         const unsigned long long stop = min(kend, e_end);
-        // a long list is narrowed first through 32 evenly spaced samples
-        // (one gather per edge, then shuffles), leaving ~1/32 of it to search
+        // a long list is narrowed first through 64 evenly spaced samples, two
+        // per lane (gathered once per edge, then shuffles), leaving ~1/64 of it
+        // to search
         const uint32_t flen = fle - flb;
         const bool sampled = flen >= kSampledList;
-        const uint32_t smp = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)lane * flen) >> 5)) : 0u;
+        const uint32_t smp = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane) * flen) >> 6)) : 0u;
+        const uint32_t smp1 = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane + 1) * flen) >> 6)) : 0u;
         do {
           kb += 32;
           const uint32_t fo = (uint32_t)(kb + lane - e_start);
@@ -823,8 +825,10 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
               const uint32_t cand = __shfl_sync(kFull, smp, t + d);
               if (cand <= c) t += d;
             }
-            lo = flb + (uint32_t)(((unsigned long long)t * flen) >> 5);
-            hi = t == 31 ? fle : flb + (uint32_t)(((unsigned long long)(t + 1) * flen) >> 5);
+            // sample 2t is the last even one <= c; its odd neighbour decides
+            const uint32_t kk = 2 * t + (__shfl_sync(kFull, smp1, t) <= c ? 1u : 0u);
+            lo = flb + (uint32_t)(((unsigned long long)kk * flen) >> 6);
+            hi = kk == 63 ? fle : flb + (uint32_t)(((unsigned long long)(kk + 1) * flen) >> 6);
           }
           const uint32_t q = lower_bound_u32(ocol, lo, hi, c);
           const bool fh = q < hi && __ldg(ocol + q) == c;
