@@ -1509,13 +1509,19 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
   const UnionRegs U(a.Up, a.arr);
   const bool hubs = U.hub_map != nullptr;  // descriptors carry kHubDesc only when maps exist
   // one chunk per warp: finer chunks (and any cap on their size) measured
-  // slower, the search for a chunk's first entry is paid once per warp
-  unsigned long long ch = total / nwarps;
-  ch = max((ch + 31) & ~31ull, 32ull);
-  uint32_t hits = 0, n_merge = 0, n_lane = 0, n_chunk = 0;
+  // slower, the search for a chunk's first entry is paid once per warp;
+  // ch * nwarps >= total, so the chunk below is the warp's only one
+  const unsigned long long ch = max(((total + nwarps - 1) / nwarps + 31) & ~31ull, 32ull);
+  // work counters live in shared memory (per warp: hits, merge iterations,
+  // lane iterations, merge chunks) rather than in four registers held across
+  // the loop; lane 0 adds to them
+  __shared__ uint32_t s_cnt[4][kWaveWarps];
+  if (lane < 4) s_cnt[lane][wib] = 0;
+  __syncwarp();
   PushStage ps{s_push_eid[wib], 0};
 
-  for (unsigned long long c0 = warp * ch; c0 < total; c0 += nwarps * ch) {
+  if (warp * ch < total) {
+    const unsigned long long c0 = warp * ch;
     const unsigned long long kend = min(c0 + ch, total);
     unsigned long long k = c0;
     uint32_t g = G > 1 ? warp_last_le(PrefKey{a.wpref}, 0, G - 1, k) : 0;
@@ -1610,6 +1616,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
               // kMergeChunks chunks are loaded per round, so most rows cost
               // one dependent load instead of one per chunk
               const uint32_t cap = (L_end - L_beg) / 32 + 2;
+              uint32_t nch = 0;  // chunks matched (work counter)
               for (uint32_t it = 0;; ++it) {
                 if (it > cap) {
                   if (lane == 0) atomicOr(a.err, kErrInternal);
@@ -1636,18 +1643,19 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
                   const uint32_t ht = (uint32_t)(__shfl_sync(kFull, lp[c], tt) >> 32);
                   if (look && lvt == w) { p = cur + 32 * c + tt; h = ht; }
                   adv += __popc(__ballot_sync(kFull, lv <= wmax));
-                  ++n_chunk;
+                  ++nch;
                 }
                 cur += adv;
                 if (adv < 32u * kMergeChunks) break;
               }
+              if (lane == 0) s_cnt[3][wib] += nch;
               m_e = e0;
               m_next_o = o0 + 32;
               m_cur = cur;
             }
-            ++n_merge;
+            if (lane == 0) s_cnt[1][wib]++;
           } else {
-            ++n_lane;
+            if (lane == 0) s_cnt[2][wib]++;
             m_e = kInvalid;
             if (look) {
               if (hubs && (lb & kHubDesc)) {
@@ -1662,10 +1670,10 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           }
           bool pf = false, ph = false;
           // h == kInvalid: w was the long row's own vertex (a self-loop entry)
-          if (look && p != kInvalid && h != kInvalid) {
-            ++hits;
-            pkt_rule(U, e, f, es_f, h, level, W, pf, ph);
-          }
+          const bool hit = look && p != kInvalid && h != kInvalid;
+          const uint32_t nhit = __popc(__ballot_sync(kFull, hit));
+          if (lane == 0) s_cnt[0][wib] += nhit;
+          if (hit) pkt_rule(U, e, f, es_f, h, level, W, pf, ph);
           push_edge(ps, U, M, st, a.err, qnext, qdnext, pf, f, W);
           push_edge(ps, U, M, st, a.err, qnext, qdnext, ph, h, W);
           i = x_last;
@@ -1732,15 +1740,6 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
   }
   // work counters: summed per block, then one atomic per counter and block
   // (per-warp atomics on four addresses serialise on large waves)
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) hits += __shfl_xor_sync(kFull, hits, d);
-  __shared__ uint32_t s_cnt[4][kWaveWarps];
-  if (lane == 0) {
-    s_cnt[0][wib] = hits;
-    s_cnt[1][wib] = n_merge;
-    s_cnt[2][wib] = n_lane;
-    s_cnt[3][wib] = n_chunk;
-  }
   __syncthreads();
   if (threadIdx.x < 4) {
     unsigned long long sum = 0;
