@@ -1289,8 +1289,10 @@ struct PushStage {
 };
 
 __device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, const Member& M,
-                                           MemberState* st, uint32_t* err, unsigned long long* qnext,
-                                           uint4* qdnext) {
+                                           MemberState* st, uint32_t* err, uint32_t q_sel) {
+  // the queue being built (q_sel names the one being processed)
+  unsigned long long* qnext = q_sel ? U.q0 : U.q1;
+  uint4* qdnext = q_sel ? U.qd0 : U.qd1;
   __syncwarp();
   const uint32_t n = ps.n;
   if (n == 0) return;
@@ -1329,12 +1331,12 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, co
 
 // Queue edge x (union eid) for wave W + 1.  All lanes call it.
 __device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, const Member& M, MemberState* st,
-                                          uint32_t* err, unsigned long long* qnext, uint4* qdnext, bool want,
+                                          uint32_t* err, uint32_t q_sel, bool want,
                                           uint32_t x, uint32_t W) {
   const unsigned bal = __ballot_sync(kFull, want);
   if (!bal) return;
   const uint32_t k = __popc(bal);
-  if (ps.n + k > kPushBuf) push_flush(ps, U, M, st, err, qnext, qdnext);
+  if (ps.n + k > kPushBuf) push_flush(ps, U, M, st, err, q_sel);
   if (want) {
     U.es[x].y = (int)(W + 1);
     ps.eid[ps.n + __popc(bal & ((1u << lane_id()) - 1))] = x;
@@ -1536,8 +1538,6 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
       const Member M = a.mem[g];
       MemberState* st = a.st + g;
       const uint32_t phase = st->phase, level = st->level, act_sel = st->act_sel, q_sel = st->q_sel;
-      unsigned long long* qnext = q_sel ? U.q0 : U.q1;
-      uint4* qdnext = q_sel ? U.qd0 : U.qd1;
       if (phase == kPhaseProc) {
         const unsigned long long* q = (q_sel ? U.q1 : U.q0) + M.eb;
         const uint4* qd = (q_sel ? U.qd1 : U.qd0) + M.eb;
@@ -1674,8 +1674,8 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           const uint32_t nhit = __popc(__ballot_sync(kFull, hit));
           if (lane == 0) s_cnt[0][wib] += nhit;
           if (hit) pkt_rule(U, e, f, es_f, h, level, W, pf, ph);
-          push_edge(ps, U, M, st, a.err, qnext, qdnext, pf, f, W);
-          push_edge(ps, U, M, st, a.err, qnext, qdnext, ph, h, W);
+          push_edge(ps, U, M, st, a.err, q_sel, pf, f, W);
+          push_edge(ps, U, M, st, a.err, q_sel, ph, h, W);
           i = x_last;
         }
       } else if (phase == kPhaseScan0 || phase == kPhaseScan) {
@@ -1701,7 +1701,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
               else { keep = true; mn = min(mn, (uint32_t)s); }
             }
           }
-          push_edge(ps, U, M, st, a.err, qnext, qdnext, queue, e, W);
+          push_edge(ps, U, M, st, a.err, q_sel, queue, e, W);
           const unsigned kb_bal = __ballot_sync(kFull, keep);
           if (kb_bal) {
             const uint32_t kc = __popc(kb_bal);
@@ -1734,7 +1734,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
         }
         __syncwarp();
       }
-      push_flush(ps, U, M, st, a.err, qnext, qdnext);  // entries belong to this member: publish before moving on
+      push_flush(ps, U, M, st, a.err, q_sel);  // entries belong to this member: publish before moving on
       k = seg_end;
     }
   }
