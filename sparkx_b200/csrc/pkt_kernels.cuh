@@ -342,12 +342,6 @@ __global__ void k_narrow_offsets(const unsigned long long* __restrict__ src, uin
   if (bad) atomicOr(err, kErrOffsets);
 }
 
-// shift a member's local vertex ids into union ids
-__global__ void k_shift_ids(uint32_t* __restrict__ ids, unsigned long long count, uint32_t base) {
-  unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  for (; i < count; i += stride) ids[i] += base;
-}
 
 // ---------------------------------------------------------------------------
 // Exclusive scan across the block (all threads call it); `total` is the
@@ -1530,7 +1524,8 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
     while (k < kend) {
       while (g + 1 < G && a.wpref[g + 1] <= k) ++g;
       const unsigned long long mbeg = a.wpref[g];
-      const unsigned long long seg_end = min(kend, a.wpref[g + 1]);
+      // a segment spans < 2^31 elements, so offsets inside it are 32-bit
+      const unsigned long long seg_end = min(min(kend, a.wpref[g + 1]), k + (1ull << 31));
       if (seg_end <= k || mbeg > k) {  // layout does not cover k: stop rather than spin
         if (lane == 0) atomicOr(a.err, kErrInternal);
         break;
@@ -1550,10 +1545,12 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
         uint32_t i = warp_last_le(QueueStart{q}, 0, qcount - 1, k - mbeg);
         // merge cursor carried across iterations that continue the same edge
         uint32_t m_e = kInvalid, m_next_o = 0, m_cur = 0;
-        for (unsigned long long kb = k; kb < seg_end; kb += 32) {
-          const unsigned long long kk = kb + lane;
-          const bool valid = kk < seg_end;
-          const unsigned long long j = kk - mbeg;
+        // element j (member-relative) = jb + r + lane; r counts the segment
+        const unsigned long long jb = k - mbeg;
+        const uint32_t seg_len = (uint32_t)(seg_end - k);
+        for (uint32_t r = 0; r < seg_len; r += 32) {
+          const bool valid = r + lane < seg_len;
+          const unsigned long long j = jb + r + lane;
           // the window's entries, loaded once: each lane picks its own by a
           // shuffle search on the work starts (entries own >= 1 element, so
           // 32 consecutive elements span at most 32 entries)
@@ -1566,7 +1563,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           }
           const unsigned long long ent = __shfl_sync(kFull, qv, t);
           const uint32_t x = i + t;
-          const uint32_t last = (uint32_t)min(31ull, seg_end - 1 - kb);
+          const uint32_t last = min(31u, seg_len - 1 - r);
           const uint32_t x_last = __shfl_sync(kFull, x, last);
           uint32_t e = 0, o = 0, sb = 0, slen = 0, lb = 0, le = 0;
           if (valid) {
