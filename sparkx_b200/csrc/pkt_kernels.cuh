@@ -1680,13 +1680,14 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
         uint32_t* act_out = act_sel ? U.act0 : U.act1;
         uint32_t* keepbuf = s_keep[wib];
         uint32_t nkeep = 0, nzero = 0, mn = 0xFFFFFFFFu;
-        for (unsigned long long kb = k; kb < seg_end; kb += 32) {
-          const unsigned long long kk = kb + lane;
-          const bool valid = kk < seg_end;
+        // active-list positions are below the member's edge count (< 2^28)
+        const uint32_t a0 = (uint32_t)(k - mbeg), seg_len = (uint32_t)(seg_end - k);
+        for (uint32_t r = 0; r < seg_len; r += 32) {
+          const bool valid = r + lane < seg_len;
           bool keep = false, zero = false, queue = false;
           uint32_t le = 0, e = 0;
           if (valid) {
-            le = act[M.eb + (kk - mbeg)];
+            le = act[M.eb + a0 + r + lane];
             e = M.eb + le;
             const int2 st_e = U.es[e];
             const int32_t s = st_e.x;
