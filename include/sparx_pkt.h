@@ -124,6 +124,22 @@ int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64
                         sparx_pkt_stats* stats);
 
 /*
+ * Local clustering coefficient of every vertex, graph transitivity and the
+ * average local coefficient, from the triangle supports.  Replaces
+ * ClusteringCoefficient::new / compute (clustering_coefficient.rs:41-52,93-190)
+ * with its definitions: for vertex u with d distinct neighbours (a self-loop
+ * counts as one), local[u] = ceil(sum of u's slot supports / 2) / (d(d-1)/2),
+ * or 0 when d < 2; *transitivity = (sum of all slot supports / 3) / 2 /
+ * (sum of d(d-1)/2); *average = sum of local / n.  In SPARX_SUPPORT_U8 mode the
+ * slot supports are reduced mod 256 like the reference's AtomicU8 counts.  The
+ * reference divides by 3 per worker thread; this is its one-thread value.
+ * local_out is f64[n]; transitivity and average may be NULL.
+ */
+int sparx_clustering_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours,
+                         uint64_t width, double* local_out, double* transitivity, double* average,
+                         const sparx_pkt_opts* opts, sparx_pkt_stats* stats);
+
+/*
  * Allocation-free PKT decomposition of one graph in DEVICE memory.  No
  * counterpart in the reference.
  *

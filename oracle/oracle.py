@@ -96,6 +96,43 @@ def triangles(off, nbr, mode=MODE_WIDE, threads=1, hash_map=False, eo_er=None):
     return sup
 
 
+def clustering(off, nbr, mode=MODE_WIDE, threads=1):
+    """Local clustering coefficients, transitivity and their average as
+    k_truss/clustering_coefficient.rs:93-190 computes them, with one worker (the reference
+    divides the triangle total by 3 per worker thread, clustering_coefficient.rs:157, so its
+    transitivity depends on the thread count; one worker is the exact value).
+
+    For u with d distinct neighbours (the row's HashSet, clustering_coefficient.rs:140-155):
+    possible = d(d-1)/2 if d > 1 else 0; t = ceil(row support sum / 2); local = t / possible
+    when possible is a normal float, else 0 (:160-172).  transitivity = (sum of all slot
+    supports // 3) / 2 / sum(possible) (:157,178-181); average = sum(local) / n (:177).
+    Slot supports come from ``triangles`` (AtomicU8 counts in MODE_U8)."""
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    nbr = np.ascontiguousarray(nbr, dtype=np.int64)
+    n = len(off) - 1
+    sup = triangles(off.astype(np.uint64), nbr.astype(np.uint64), mode=mode, threads=threads)
+    sup = sup.astype(np.uint64)
+    if mode == MODE_U8:
+        sup &= np.uint64(0xFF)
+    rows = np.repeat(np.arange(n), np.diff(off))
+    same = np.zeros(len(nbr), dtype=bool)
+    if len(nbr) > 1:
+        same[1:] = (nbr[1:] == nbr[:-1]) & (rows[1:] == rows[:-1])
+    deg = np.diff(off) - np.bincount(rows[same], minlength=n) if n else np.zeros(0, np.int64)
+    possible = np.where(deg > 1, deg.astype(np.float64) * (deg - 1).astype(np.float64) / 2.0, 0.0)
+    cs = np.concatenate([[0], np.cumsum(sup, dtype=np.uint64)]).astype(np.uint64)
+    row_sum = cs[off[1:]] - cs[off[:-1]]
+    tri = ((row_sum + np.uint64(1)) // np.uint64(2)).astype(np.float64)
+    local = np.zeros(n, dtype=np.float64)
+    pos = possible > 0
+    local[pos] = tri[pos] / possible[pos]
+    total_triangles = int(sup.sum()) // 3
+    with np.errstate(divide="ignore", invalid="ignore"):
+        transitivity = float(np.float64(total_triangles) / 2.0 / np.float64(possible.sum()))
+        average = float(np.float64(local.sum()) / np.float64(n))
+    return local, transitivity, average
+
+
 def pkt(off, nbr, mode=MODE_WIDE, threads=1, hash_map=False, return_stats=False):
     """Truss per slot (u32) by the PKT restatement of k_truss/pkt.rs:216-563."""
     off, nbr, n = _csr(off, nbr)

@@ -3,8 +3,12 @@
 Public surface mirrors the reference's ``AlgoPKT`` (``src/k_truss/pkt.rs:29-123``):
 ``AlgoPKT.new(graph)``, ``trussness(e)``, ``k_trusses()``, ``drop_cache()``; the
 graph is a memory-mapped CSR like ``GraphMemoryMap`` (``src/graph/mod.rs:365-378``).
+``AlgoBurkhardtEtAl`` (the default ``k_truss``), ``Triangles`` and
+``ClusteringCoefficient`` run on the same GPU engine.
 """
 from .graph import GraphMemoryMap  # noqa: F401
-from .pkt import AlgoPKT, PktError, PktOptions, PktStats, Triangles  # noqa: F401
+from .pkt import (AlgoBurkhardtEtAl, AlgoPKT, ClusteringCoefficient, PktError,  # noqa: F401
+                  PktOptions, PktStats, Triangles)
 
-__all__ = ["GraphMemoryMap", "AlgoPKT", "Triangles", "PktOptions", "PktStats", "PktError"]
+__all__ = ["GraphMemoryMap", "AlgoPKT", "AlgoBurkhardtEtAl", "Triangles", "ClusteringCoefficient",
+           "PktOptions", "PktStats", "PktError"]

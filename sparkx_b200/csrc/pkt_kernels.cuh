@@ -19,10 +19,14 @@
 //                               (0xFFFFFFFF: not yet queued); one 8-byte word so
 //                               a triangle's two other edges cost two sectors
 //   act[2][m], q[2][m] (u64)    per-member active lists and frontier queues,
+//   qd[2][m] (uint4)            with each queued edge's row descriptor;
 //                               segment [eb_g, eb_g + m_g) for member g
 //   working CSR (off, row)      the peel's view: row0 at first, then rebuilt
 //                               without processed edges whenever the live
-//                               edges halve (two ping-pong buffers)
+//                               edges fill at most 85% of it (two ping-pong
+//                               buffers)
+//   hub maps                    single-graph launches: neighbour id -> edge id
+//                               for the highest-degree vertices
 #pragma once
 
 #include <cstdint>
@@ -2032,6 +2036,73 @@ __global__ void k_finalize(const unsigned long long* __restrict__ row0, const in
 }
 
 // support per slot (Triangles::new layout): sup of the slot's edge, 0 for self-loops
+// Local clustering coefficient per vertex, and the sums behind the average and
+// the transitivity, from the edge supports (clustering_coefficient.rs:93-190
+// restated): with d = |N(u)| (distinct neighbours; a self-loop counts),
+// possible(u) = d(d - 1)/2 for d > 1, t(u) = ceil(sum of u's slot supports /
+// 2) = triangles at u, local(u) = t(u) / possible(u) or 0.  Slot supports are
+// reduced mod 256 in u8 mode, as the reference's AtomicU8 counts are.  Rows
+// of up to kLaneRow entries per lane, longer rows per warp.
+__device__ __forceinline__ uint32_t slot_support(unsigned long long pr, const int2* __restrict__ es,
+                                                 int u8mode) {
+  const uint32_t e = (uint32_t)(pr >> 32);
+  const uint32_t s = e == kInvalid ? 0u : (uint32_t)__ldg(&es[e].x);
+  return u8mode ? (s & 0xFFu) : s;
+}
+
+__global__ void __launch_bounds__(256) k_clustering(const uint32_t* __restrict__ off,
+                                                    const unsigned long long* __restrict__ row0,
+                                                    const int2* __restrict__ es, uint32_t n, int u8mode,
+                                                    double* __restrict__ local, double* __restrict__ sum_possible,
+                                                    double* __restrict__ sum_local,
+                                                    unsigned long long* __restrict__ sum_slots) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc_p = 0.0, acc_l = 0.0;
+  unsigned long long acc_s = 0;
+  for (uint32_t base = warp * 32; base < n; base += nwarps * 32) {
+    const uint32_t u = base + lane;
+    uint32_t b = 0, e = 0;
+    if (u < n) { b = __ldg(off + u); e = __ldg(off + u + 1); }
+    unsigned long long ts = 0;
+    if (u < n && e - b <= kLaneRow)
+      for (uint32_t s = b; s < e; ++s) ts += slot_support(__ldg(row0 + s), es, u8mode);
+    unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
+    while (big) {
+      const int j = __ffs(big) - 1;
+      big &= big - 1;
+      const uint32_t bb = __shfl_sync(kFull, b, j), be = __shfl_sync(kFull, e, j);
+      unsigned long long c = 0;
+      for (uint32_t s = bb + lane; s < be; s += 32) c += slot_support(__ldg(row0 + s), es, u8mode);
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(kFull, c, d);
+      if (lane == (uint32_t)j) ts = c;
+    }
+    if (u < n) {
+      const uint32_t d = e - b;
+      const double possible = d > 1 ? (double)d * (double)(d - 1) / 2.0 : 0.0;
+      const double tri = (double)((ts + 1) / 2);
+      const double loc = possible > 0.0 ? tri / possible : 0.0;
+      local[u] = loc;
+      acc_p += possible;
+      acc_l += loc;
+      acc_s += ts;
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    acc_p += __shfl_xor_sync(kFull, acc_p, d);
+    acc_l += __shfl_xor_sync(kFull, acc_l, d);
+    acc_s += __shfl_xor_sync(kFull, acc_s, d);
+  }
+  if (lane == 0) {
+    if (acc_p != 0.0) atomicAdd(sum_possible, acc_p);
+    if (acc_l != 0.0) atomicAdd(sum_local, acc_l);
+    if (acc_s) atomicAdd(sum_slots, acc_s);
+  }
+}
+
 __global__ void k_support_slots(const unsigned long long* __restrict__ row0, const int2* __restrict__ es,
                                 unsigned long long width, uint32_t* __restrict__ out, int u8mode) {
   unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,7 +1,7 @@
 // Host side of the B200 PKT k-truss engine: C ABI (include/sparx_pkt.h),
 // device workspace, pinned-staging upload, kernel sequencing and the
 // device-resident peel loop (a CUDA graph with a conditional WHILE node whose
-// body is one wave + the planner).
+// body is four wave kernels; the last block of each wave plans the next).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -70,6 +70,9 @@ struct Counters {  // device scalars
   uint32_t heavy_count;  //                      heavy vertices listed
   uint32_t hub_count;    // hub maps assigned
   uint32_t big_count;    // rows compacted by a block each
+  double cc_possible;    // clustering: sum of d(d - 1)/2 over vertices
+  double cc_local;       //             sum of local coefficients
+  unsigned long long cc_slots;  //      sum of slot supports
 };
 
 
@@ -396,6 +399,9 @@ struct UnionJob {
   void* out = nullptr;          // device truss output (u8 or u32 per slot)
   bool support_only = false;
   uint32_t* support_out = nullptr;  // device u32 per slot (support_only)
+  bool clustering = false;          // support_only, then local coefficients (f64 per vertex) into out
+  double cc_possible = 0, cc_local = 0;
+  unsigned long long cc_slots = 0;
   // results
   std::vector<MemberState> states;
   std::vector<unsigned long long> mem_tri;
@@ -592,7 +598,13 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   }
   CU(cudaEventRecord(E.tev[3], s));
 
-  if (J.support_only) {
+  if (J.support_only && J.clustering) {
+    k_clustering<<<vgrid, 256, 0, s>>>(J.off, row0, es, N, O.support_mode == SPARX_SUPPORT_U8, (double*)J.out,
+                                       &cnt->cc_possible, &cnt->cc_local, &cnt->cc_slots);
+    J.launches += 1;
+    CU(cudaEventRecord(E.tev[4], s));
+    CU(cudaEventRecord(E.tev[5], s));
+  } else if (J.support_only) {
     k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(row0, es, W, J.support_out,
                                                                        O.support_mode == SPARX_SUPPORT_U8);
     J.launches += 1;
@@ -724,6 +736,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   CU(cudaStreamSynchronize(s));
   J.tri = hc.tri;
   J.kmax = hc.kmax;
+  J.cc_possible = hc.cc_possible;
+  J.cc_local = hc.cc_local;
+  J.cc_slots = hc.cc_slots;
   if (!J.support_only && J.ctl.trace) {
     const char* trace_path = std::getenv("SPARX_TRACE_FILE");
     const size_t nrec = (size_t)std::min<unsigned long long>(J.ctl.waves_run, J.ctl.trace_cap);
@@ -792,9 +807,18 @@ int check_dims(uint64_t n_plus_1, uint64_t width) {
   return SPARX_OK;
 }
 
-// Single graph from host memory (ids u64 or u32).
+// Sums behind the clustering coefficients (out_host then holds one f64 local
+// coefficient per vertex).
+struct ClusterSums {
+  double possible = 0, local = 0;
+  unsigned long long slots = 0;
+};
+
+// Single graph from host memory (ids u64 or u32): truss per slot, support per
+// slot (support_only) or local clustering coefficients (cc != nullptr).
 int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int bits, uint64_t width,
-             void* out_host, bool support_only, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
+             void* out_host, bool support_only, const sparx_pkt_opts* opts, sparx_pkt_stats* stats,
+             ClusterSums* cc = nullptr) {
   g_last_error.clear();
   if (!offsets || (!nbrs && width) || (!out_host && width)) { set_error("null pointer"); return SPARX_E_ARG; }
   int rc = check_dims(n_plus_1, width);
@@ -813,15 +837,17 @@ int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int b
   J.N = n;
   J.W = width;
   J.members.push_back(Member{0, (uint32_t)n, 0, (uint32_t)width, 0, 0});
-  J.support_only = support_only;
-  const size_t out_bytes = support_only ? 4 * width : (O.out_bits / 8) * width;
+  J.support_only = support_only || cc;
+  J.clustering = cc != nullptr;
+  support_only = J.support_only;
+  const size_t out_bytes = J.clustering ? 8 * n : support_only ? 4 * width : (O.out_bits / 8) * width;
   J.L = make_layout(n, width, 1, true, out_bytes);
   rc = ensure_ws(E, J.L.total);
   if (rc) return rc;
   cudaStream_t s = E.stream;
   J.off = at<uint32_t>(E, J.L.off);
   J.nbr = at<uint32_t>(E, J.L.nbr);
-  if (support_only) J.support_out = at<uint32_t>(E, J.L.out);
+  if (support_only && !J.clustering) J.support_out = at<uint32_t>(E, J.L.out);
   else J.out = at<void>(E, J.L.out);
   char* stage[2] = {E.ws + J.L.stage0, E.ws + J.L.stage1};
   Counters* cnt = at<Counters>(E, J.L.cnt);
@@ -859,7 +885,12 @@ int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int b
     return rc;
   }
   CU(cudaEventRecord(E.tev[7], s));
-  rc = download(E, out_host, support_only ? (void*)J.support_out : J.out, out_bytes, s);
+  if (cc) {
+    cc->possible = J.cc_possible;
+    cc->local = J.cc_local;
+    cc->slots = J.cc_slots;
+  }
+  rc = download(E, out_host, (support_only && !J.clustering) ? (void*)J.support_out : J.out, out_bytes, s);
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
   auto t1 = std::chrono::steady_clock::now();
@@ -1409,6 +1440,23 @@ int sparx_pkt_run_u32(const uint64_t* offsets, uint64_t n_plus_1, const uint32_t
 int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
                         uint32_t* support_out, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
   return run_host(offsets, n_plus_1, neighbours, 64, width, support_out, true, opts, stats);
+}
+
+int sparx_clustering_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
+                         double* local_out, double* transitivity, double* average, const sparx_pkt_opts* opts,
+                         sparx_pkt_stats* stats) {
+  if (n_plus_1 > 1 && !local_out) {
+    g_last_error = "null pointer";
+    return SPARX_E_ARG;
+  }
+  ClusterSums cc;
+  const int rc = run_host(offsets, n_plus_1, neighbours, 64, width, local_out, true, opts, stats, &cc);
+  if (rc) return rc;
+  // clustering_coefficient.rs:178-181: (total slot support / 3) / 2 / total
+  // possible pairs, and the mean local coefficient (IEEE semantics for 0/0)
+  if (transitivity) *transitivity = (double)(cc.slots / 3) / 2.0 / cc.possible;
+  if (average) *average = cc.local / (double)(n_plus_1 - 1);
+  return SPARX_OK;
 }
 
 int sparx_pkt_run_device(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_neighbours, uint64_t width,

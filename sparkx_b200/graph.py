@@ -94,6 +94,19 @@ class GraphMemoryMap:
         r = self.index_node(u)
         return self._neighbours[r.start:r.stop]
 
+    # algorithm facade (graph/impl_algos.rs:29-40): k_truss is Burkhardt et al.'s by default
+    def k_truss(self):
+        from .pkt import AlgoBurkhardtEtAl
+        return AlgoBurkhardtEtAl.new(self)
+
+    def k_truss_bea(self):
+        from .pkt import AlgoBurkhardtEtAl
+        return AlgoBurkhardtEtAl.new(self)
+
+    def k_truss_pkt(self):
+        from .pkt import AlgoPKT
+        return AlgoPKT.new(self)
+
     def graph_id(self) -> str:
         """Stable id: the cache key the result file is named after."""
         if self._id is None:

@@ -87,7 +87,8 @@ class _GraphView(ctypes.Structure):
 
 EXPORTS = [
     "sparx_pkt_default_opts", "sparx_strerror", "sparx_last_error", "sparx_pkt_run",
-    "sparx_pkt_run_u32", "sparx_pkt_run_device", "sparx_triangles_run", "sparx_pkt_run_batch",
+    "sparx_pkt_run_u32", "sparx_pkt_run_device", "sparx_triangles_run", "sparx_clustering_run",
+    "sparx_pkt_run_batch",
     "sparx_pkt_run_device_noalloc",
     "sparx_server_create", "sparx_server_submit", "sparx_server_poll", "sparx_server_wait",
     "sparx_server_cancel", "sparx_server_destroy",
@@ -110,6 +111,9 @@ def lib():
         f = getattr(L, name)
         f.restype = i32
         f.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats)]
+    L.sparx_clustering_run.restype = i32
+    L.sparx_clustering_run.argtypes = [vp, u64, vp, u64, vp, P(ctypes.c_double), P(ctypes.c_double),
+                                       P(_Opts), P(_Stats)]
     L.sparx_pkt_run_device.restype = i32
     L.sparx_pkt_run_device.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats), vp]
     if hasattr(L, "sparx_pkt_run_device_noalloc"):
@@ -231,6 +235,22 @@ def run_triangles(offsets: np.ndarray, neighbours: np.ndarray, opts: PktOptions 
     return out, PktStats.from_c(st)
 
 
+def run_clustering(offsets: np.ndarray, neighbours: np.ndarray, opts: PktOptions | None = None):
+    """Local clustering coefficient per vertex (f64), transitivity, average and stats, as
+    ``ClusteringCoefficient::new`` computes them (clustering_coefficient.rs:41-52,93-190)."""
+    opts = opts or PktOptions()
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    nbr = np.ascontiguousarray(neighbours, dtype=np.uint64)
+    local = np.empty(max(off.shape[0] - 1, 0), dtype=np.float64)
+    trans, avg = ctypes.c_double(), ctypes.c_double()
+    st = _Stats()
+    o = opts.c()
+    _check(lib().sparx_clustering_run(off.ctypes.data, off.shape[0], nbr.ctypes.data, nbr.shape[0],
+                                      local.ctypes.data, ctypes.byref(trans), ctypes.byref(avg),
+                                      ctypes.byref(o), ctypes.byref(st)))
+    return local, trans.value, avg.value, PktStats.from_c(st)
+
+
 def _cache_file(g: GraphMemoryMap, kind: str) -> str:
     os.makedirs(CACHE_DIR, exist_ok=True)
     return os.path.join(CACHE_DIR, f"{kind}_{g.graph_id()}.mmap")
@@ -263,9 +283,11 @@ class AlgoPKT:
             mm.flush()
         return cls(g, truss, max(1, int(threads)), stats)
 
+    _cache_kind = "ktrusspkt"
+
     @classmethod
     def get_or_compute(cls, g: GraphMemoryMap, opts: PktOptions | None = None) -> "AlgoPKT":
-        path = _cache_file(g, "ktrusspkt")
+        path = _cache_file(g, cls._cache_kind)
         if os.path.exists(path):
             mm = np.memmap(path, dtype=np.uint8, mode="r")
             if mm.shape[0] >= g.width():
@@ -280,12 +302,69 @@ class AlgoPKT:
         return self._k_trusses
 
     def drop_cache(self) -> None:
-        path = _cache_file(self.g, "ktrusspkt")
+        path = _cache_file(self.g, self._cache_kind)
         os.remove(path)
 
     def get_throughput_factor(self) -> int:
         """pkt.rs:176-178: the bench divides by the CSR width."""
         return self.g.width()
+
+
+class AlgoBurkhardtEtAl(AlgoPKT):
+    """k-truss decomposition with the API of ``AlgoBurkhardtEtAl`` (burkhardt_et_al.rs:28-98), the
+    reference's default ``GraphMemoryMap::k_truss`` (graph/impl_algos.rs:29-36).
+
+    The truss decomposition is unique, so the result is the one the PKT engine computes; with
+    wide (default) support it equals the reference Burkhardt peel's.  In ``SUPPORT_U8`` mode the
+    engine follows the reference PKT's wrapped-count semantics, which differ from its Burkhardt
+    peel's (a count that wraps to zero removes the edge there)."""
+
+    _cache_kind = "ktrussbea"
+
+    @classmethod
+    def new_with_conf(cls, g: GraphMemoryMap, threads: int,
+                      opts: PktOptions | None = None) -> "AlgoBurkhardtEtAl":
+        opts = opts or PktOptions()
+        off, nbr = _arrays(g)
+        truss, stats = run_pkt(off, nbr, opts)
+        if opts.out_bits == 8:
+            path = _cache_file(g, cls._cache_kind)
+            mm = np.memmap(path, dtype=np.uint8, mode="w+", shape=(max(1, truss.shape[0]),))
+            mm[: truss.shape[0]] = truss
+            mm.flush()
+        return cls(g, truss, max(1, int(threads)), stats)
+
+
+class ClusteringCoefficient:
+    """Local clustering coefficients, transitivity and their average for a ``GraphMemoryMap``
+    (clustering_coefficient.rs:17-79), computed on the GPU from the triangle supports."""
+
+    def __init__(self, g: GraphMemoryMap, local: np.ndarray, transitivity: float, average: float,
+                 stats: PktStats):
+        self.g = g
+        self._local = local
+        self._transitivity = transitivity
+        self._average = average
+        self.stats = stats
+
+    @classmethod
+    def new(cls, g: GraphMemoryMap, opts: PktOptions | None = None) -> "ClusteringCoefficient":
+        off, nbr = _arrays(g)
+        local, trans, avg, stats = run_clustering(off, nbr, opts)
+        return cls(g, local, trans, avg, stats)
+
+    def get_average_clustering_coefficient(self) -> float:
+        return self._average
+
+    def get_node_clusteringcoefficient(self, node_id: int) -> float:
+        assert node_id < self.g.size(), "id < |V| --- not met"
+        return float(self._local[node_id])
+
+    def get_graph_transitivity(self) -> float:
+        return self._transitivity
+
+    def local_coefficients(self) -> np.ndarray:
+        return self._local
 
 
 class Triangles:

@@ -155,3 +155,50 @@ def test_generators_reproduce_fixture_graphs():
         h.update(np.ascontiguousarray(g.offsets, dtype="<u8").tobytes())
         h.update(np.ascontiguousarray(g.neighbours, dtype="<u4").tobytes())
         assert h.hexdigest() == fx[name]["csr_sha256"], name
+
+
+def _clustering_definition(g):
+    """Local coefficients from the definition: edges among u's neighbours over C(d, 2), d the
+    number of distinct neighbours (a self-loop counts as one, as the reference's row HashSet
+    does), and the reference's transitivity: triangles / sum of C(d, 2)."""
+    off = g.offsets.astype(np.int64)
+    nbrs = [set(int(x) for x in g.neighbours[off[u]:off[u + 1]]) for u in range(g.n)]
+    local, possible, tri_total = [], 0.0, 0
+    for u in range(g.n):
+        d = len(nbrs[u])
+        others = nbrs[u] - {u}
+        links = sum(1 for a in others for b in others if a < b and b in nbrs[a])
+        p = d * (d - 1) / 2.0 if d > 1 else 0.0
+        possible += p
+        tri_total += links
+        local.append(links / p if p > 0 else 0.0)
+    return np.array(local), (tri_total / 3) / possible if possible else float("nan")
+
+
+def test_clustering_known_answers():
+    # K3 and K4: every neighbour pair linked; the reference's transitivity is T / sum C(d, 2)
+    for n in (3, 4):
+        local, trans, avg = O.clustering(kn(n).offsets, kn(n).neighbours)
+        assert np.array_equal(local, np.ones(n)) and avg == 1.0
+        assert trans == pytest.approx(1.0 / 3.0, rel=1e-15)
+    path = gen.from_edges(3, [(0, 1), (1, 2)])
+    local, trans, avg = O.clustering(path.offsets, path.neighbours)
+    assert np.array_equal(local, np.zeros(3)) and trans == 0.0 and avg == 0.0
+    # a self-loop widens u's neighbourhood (d counts u) without adding triangles
+    g = gen.from_edges(3, [(0, 1), (1, 2), (0, 2), (0, 0)])
+    local, _, _ = O.clustering(g.offsets, g.neighbours)
+    assert local[0] == pytest.approx(1.0 / 3.0, rel=1e-15) and local[1] == 1.0
+
+
+def test_clustering_matches_definition():
+    rng = np.random.default_rng(11)
+    for _ in range(60):
+        g = random_graph(rng)
+        local, trans, avg = O.clustering(g.offsets, g.neighbours)
+        want_local, want_trans = _clustering_definition(g)
+        assert np.allclose(local, want_local, rtol=1e-15, atol=0)
+        if np.isnan(want_trans):
+            assert np.isnan(trans)
+        else:
+            assert trans == pytest.approx(want_trans, rel=1e-14)
+        assert avg == pytest.approx(want_local.sum() / g.n, rel=1e-14)
