@@ -124,6 +124,21 @@ int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64
                         sparx_pkt_stats* stats);
 
 /*
+ * k-core decomposition: the core number of every vertex.  Replaces
+ * AlgoLiuEtAl::new / compute_with_proc_mem (k_core/liu_et_al.rs:45-62,190-420)
+ * with its semantics: a vertex's degree is its row length (self-loop slots
+ * included), isolated vertices get core 0, and peeling at level k (k >= 1)
+ * removes every live vertex of degree <= k.  In SPARX_SUPPORT_U8 mode the
+ * degrees are reduced mod 256 like the reference's AtomicU8 counters.
+ * core_out is u8[n] (opts->out_bits == 8, the reference layout;
+ * SPARX_E_OVERFLOW_U8 if a core exceeds 255) or u32[n].  stats: levels,
+ * waves (sub-levels) and k_max (largest core) are filled.
+ */
+int sparx_kcore_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours,
+                    uint64_t width, void* core_out, const sparx_pkt_opts* opts,
+                    sparx_pkt_stats* stats);
+
+/*
  * Local clustering coefficient of every vertex, graph transitivity and the
  * average local coefficient, from the triangle supports.  Replaces
  * ClusteringCoefficient::new / compute (clustering_coefficient.rs:41-52,93-190)

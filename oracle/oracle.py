@@ -96,6 +96,45 @@ def triangles(off, nbr, mode=MODE_WIDE, threads=1, hash_map=False, eo_er=None):
     return sup
 
 
+def kcore(off, nbr, mode=MODE_WIDE):
+    """Core numbers as k_core/liu_et_al.rs:190-420 computes them, peeled sequentially (the
+    result does not depend on the order).  degree = row length, reduced mod 256 in MODE_U8
+    (AtomicU8, :258); degree-0 vertices are dead with core 0 (:259-265); from k = 1 (:295),
+    every live vertex with degree <= k is peeled with core k (:303-312); peeling u decrements a
+    neighbour's degree only while it exceeds k, and a neighbour whose degree was k + 1 is
+    peeled at the same level (:339-372); an empty level raises k (:316-327).  In MODE_U8 a
+    level past 255 is the reference's overflow error (never reached: degrees stay below 256)."""
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    nbr = np.ascontiguousarray(nbr, dtype=np.int64)
+    n = len(off) - 1
+    d = np.diff(off)
+    deg = (d & 0xFF) if mode == MODE_U8 else d.copy()
+    alive = d != 0
+    core = np.zeros(n, dtype=np.int64)
+    remaining = int(alive.sum())
+    k = 1
+    while remaining > 0:
+        front = np.nonzero(alive & (deg <= k))[0]
+        if front.size == 0:
+            if mode == MODE_U8 and k == 255:
+                raise OracleError("overflow when adding to k")
+            k += 1
+            continue
+        alive[front] = False
+        stack = [int(u) for u in front]
+        while stack:
+            u = stack.pop()
+            core[u] = k
+            remaining -= 1
+            for v in nbr[off[u]:off[u + 1]]:
+                if deg[v] > k:
+                    deg[v] -= 1
+                    if deg[v] == k and alive[v]:
+                        alive[v] = False
+                        stack.append(int(v))
+    return core
+
+
 def clustering(off, nbr, mode=MODE_WIDE, threads=1):
     """Local clustering coefficients, transitivity and their average as
     k_truss/clustering_coefficient.rs:93-190 computes them, with one worker (the reference

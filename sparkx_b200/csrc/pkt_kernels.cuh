@@ -2036,6 +2036,111 @@ __global__ void k_finalize(const unsigned long long* __restrict__ row0, const in
 }
 
 // support per slot (Triangles::new layout): sup of the slot's edge, 0 for self-loops
+// ---------------------------------------------------------------------------
+// k-core decomposition (the peel of liu_et_al.rs:190-420, level-synchronous):
+// degree = row length (mod 256 in u8 mode, the reference's AtomicU8); vertices
+// with degree 0 get core 0; at level k every live vertex with degree <= k is
+// peeled with core k, and peeling it decrements each neighbour's degree only
+// while that degree exceeds k; a neighbour whose degree drops from k + 1 to k
+// joins the next sub-level.  The result does not depend on the order.
+__global__ void __launch_bounds__(256) k_kcore_init(const uint32_t* __restrict__ off, uint32_t n, int u8mode,
+                                                    uint32_t* __restrict__ deg, uint32_t* __restrict__ alive,
+                                                    uint32_t* __restrict__ core,
+                                                    unsigned long long* __restrict__ remaining) {
+  uint32_t live = 0;
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    const uint32_t d = __ldg(off + u + 1) - __ldg(off + u);
+    deg[u] = u8mode ? (d & 0xFFu) : d;
+    alive[u] = d != 0;
+    core[u] = 0;
+    live += d != 0;
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) live += __shfl_xor_sync(kFull, live, d);
+  if (lane_id() == 0 && live) atomicAdd(remaining, (unsigned long long)live);
+}
+
+// Level k: live vertices with degree <= k form the first sub-level; the
+// smallest degree left is recorded so that empty levels are skipped.
+__global__ void __launch_bounds__(256) k_kcore_scan(const uint32_t* __restrict__ deg, uint32_t* __restrict__ alive,
+                                                    uint32_t n, uint32_t k, uint32_t* __restrict__ frontier,
+                                                    uint32_t* __restrict__ count, uint32_t* __restrict__ min_left) {
+  const uint32_t lane = lane_id();
+  uint32_t mn = 0xFFFFFFFFu;
+  for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; b < n; b += gridDim.x * blockDim.x) {
+    const uint32_t u = b + lane;
+    bool take = false;
+    if (u < n && alive[u]) {
+      const uint32_t d = deg[u];
+      if (d <= k) {
+        take = true;
+        alive[u] = 0;
+      } else {
+        mn = min(mn, d);
+      }
+    }
+    const unsigned bal = __ballot_sync(kFull, take);
+    if (bal) {
+      uint32_t at = 0;
+      if (lane == 0) at = atomicAdd(count, (uint32_t)__popc(bal));
+      at = __shfl_sync(kFull, at, 0);
+      if (take) frontier[at + __popc(bal & ((1u << lane) - 1))] = u;
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
+  if (lane == 0 && mn != 0xFFFFFFFFu) atomicMin(min_left, mn);
+}
+
+// One sub-level: a warp per frontier vertex.  The decrement-while-above-k is a
+// compare-and-swap loop; each failed swap means the degree dropped, so the
+// loop ends after at most (degree - k) tries.
+__global__ void __launch_bounds__(256) k_kcore_peel(const uint32_t* __restrict__ off,
+                                                    const uint32_t* __restrict__ nbr,
+                                                    const uint32_t* __restrict__ frontier, uint32_t count,
+                                                    uint32_t k, uint32_t* __restrict__ deg,
+                                                    uint32_t* __restrict__ alive, uint32_t* __restrict__ core,
+                                                    uint32_t* __restrict__ next, uint32_t* __restrict__ next_count) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = warp; i < count; i += nwarps) {
+    const uint32_t u = frontier[i];
+    if (lane == 0) core[u] = k;
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    for (uint32_t s0 = b; s0 < e; s0 += 32) {
+      const uint32_t s = s0 + lane;
+      bool push = false;
+      uint32_t v = 0;
+      if (s < e) {
+        v = __ldg(nbr + s);
+        uint32_t x = *(volatile uint32_t*)(deg + v);
+        while (x > k) {
+          const uint32_t old = atomicCAS(deg + v, x, x - 1);
+          if (old == x) {
+            push = x == k + 1 && atomicExch(alive + v, 0u) == 1u;
+            break;
+          }
+          x = old;
+        }
+      }
+      const unsigned bal = __ballot_sync(kFull, push);
+      if (bal) {
+        uint32_t at = 0;
+        if (lane == 0) at = atomicAdd(next_count, (uint32_t)__popc(bal));
+        at = __shfl_sync(kFull, at, 0);
+        if (push) next[at + __popc(bal & ((1u << lane) - 1))] = v;
+      }
+    }
+  }
+}
+
+template <typename OutT>
+__global__ void k_kcore_out(const uint32_t* __restrict__ core, uint32_t n, OutT* __restrict__ out) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+    out[u] = (OutT)core[u];
+}
+
 // Local clustering coefficient per vertex, and the sums behind the average and
 // the transitivity, from the edge supports (clustering_coefficient.rs:93-190
 // restated): with d = |N(u)| (distinct neighbours; a self-loop counts),

@@ -400,6 +400,8 @@ struct UnionJob {
   bool support_only = false;
   uint32_t* support_out = nullptr;  // device u32 per slot (support_only)
   bool clustering = false;          // support_only, then local coefficients (f64 per vertex) into out
+  bool kcore = false;               // k-core decomposition: core per vertex into out
+  uint32_t kc_levels = 0, kc_waves = 0, kc_max = 0;
   double cc_possible = 0, cc_local = 0;
   unsigned long long cc_slots = 0;
   // results
@@ -779,6 +781,13 @@ void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
     st->k_max = M.w ? J.states[g].max_level + 2 : 0;
   }
   if (J.members.size() == 1 && J.support_only) st->triangles = J.tri;
+  if (J.kcore) {
+    st->m = 0;
+    st->self_loops = 0;
+    st->levels = J.kc_levels;
+    st->waves = J.kc_waves;
+    st->k_max = J.kc_max;
+  }
   st->launches = J.launches;
   st->support_elements = J.support_elements;
   if (J.members.size() == 1) {
@@ -807,6 +816,122 @@ int check_dims(uint64_t n_plus_1, uint64_t width) {
   return SPARX_OK;
 }
 
+// k-core workspace: the uploaded CSR, degree, live flag, core and two
+// frontier queues per vertex (Layout fields reused by name).
+Layout make_kcore_layout(uint64_t N, uint64_t W, size_t out_bytes) {
+  Layout L{};
+  size_t p = 0;
+  auto take = [&](size_t bytes) {
+    size_t r = p;
+    p = align_up(p + std::max<size_t>(bytes, 1));
+    return r;
+  };
+  L.off = take(4 * (N + 1));
+  L.nbr = take(4 * W);
+  L.dplus = take(4 * N);  // degree
+  L.act0 = take(4 * N);   // live flag
+  L.opos = take(4 * N);   // core
+  L.q0 = take(4 * N);     // frontier
+  L.q1 = take(4 * N);     // next frontier
+  L.out = take(out_bytes);
+  L.stage0 = take(kStageBytes);
+  L.stage1 = take(kStageBytes);
+  L.cnt = take(sizeof(Counters));
+  L.tiles = take(64);     // scan counters: count, next count, smallest degree left, remaining
+  L.total = p;
+  return L;
+}
+
+// Level loop of the k-core peel (liu_et_al.rs:295-420): the host reads the
+// frontier size after each scan and sub-level.
+int run_kcore(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
+  const Layout& L = J.L;
+  const uint32_t N = (uint32_t)J.N;
+  Counters* cnt = at<Counters>(E, L.cnt);
+  {
+    uint32_t* herr = (uint32_t*)E.pinned_small;
+    CU(cudaMemcpyAsync(herr, &cnt->err, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (*herr) { J.err = *herr; return status_from_flags(*herr); }
+  }
+  uint32_t* deg = at<uint32_t>(E, L.dplus);
+  uint32_t* alive = at<uint32_t>(E, L.act0);
+  uint32_t* core = at<uint32_t>(E, L.opos);
+  uint32_t* qa = at<uint32_t>(E, L.q0);
+  uint32_t* qb = at<uint32_t>(E, L.q1);
+  uint32_t* sc = at<uint32_t>(E, L.tiles);  // [0] count, [1] next count, [2] smallest degree left
+  unsigned long long* remaining_d = (unsigned long long*)(sc + 4);
+  const int u8 = O.support_mode == SPARX_SUPPORT_U8;
+  const int vgrid = grid_for(N, 256, E.sm_count * 16);
+  CU(cudaMemsetAsync(remaining_d, 0, 8, s));
+  CU(cudaEventRecord(E.tev[1], s));
+  k_kcore_init<<<vgrid, 256, 0, s>>>(J.off, N, u8, deg, alive, core, remaining_d);
+  J.launches += 1;
+  uint32_t* h = (uint32_t*)E.pinned_small;
+  unsigned long long remaining = 0;
+  CU(cudaMemcpyAsync(h, remaining_d, 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  std::memcpy(&remaining, h, 8);
+  CU(cudaEventRecord(E.tev[4], s));
+  uint64_t k = 1;
+  const auto t_start = std::chrono::steady_clock::now();
+  while (remaining > 0) {
+    if (O.timeout_ms && std::chrono::steady_clock::now() - t_start > std::chrono::milliseconds(O.timeout_ms)) {
+      set_error("k-core peel exceeded the time budget");
+      return SPARX_E_TIMEOUT;
+    }
+    CU(cudaMemsetAsync(sc, 0, 8, s));
+    CU(cudaMemsetAsync(sc + 2, 0xFF, 4, s));
+    k_kcore_scan<<<vgrid, 256, 0, s>>>(deg, alive, N, (uint32_t)k, qa, sc, sc + 2);
+    J.launches += 1;
+    CU(cudaMemcpyAsync(h, sc, 12, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    uint32_t count = h[0];
+    const uint32_t min_left = h[2];
+    if (count == 0) {
+      // no live vertex at this level: go to the smallest degree left
+      if (min_left == 0xFFFFFFFFu) { set_error("k-core: live vertices but none found"); return SPARX_E_CUDA; }
+      k = std::max<uint64_t>(k + 1, min_left);
+      continue;
+    }
+    J.kc_levels += 1;
+    J.kc_max = (uint32_t)k;
+    while (count > 0) {
+      remaining -= std::min<unsigned long long>(remaining, count);
+      CU(cudaMemsetAsync(sc + 1, 0, 4, s));
+      const int pgrid = grid_for(32ull * count, 256, E.sm_count * 16);
+      k_kcore_peel<<<pgrid, 256, 0, s>>>(J.off, J.nbr, qa, count, (uint32_t)k, deg, alive, core, qb, sc + 1);
+      J.launches += 1;
+      J.kc_waves += 1;
+      CU(cudaMemcpyAsync(h + 1, sc + 1, 4, cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+      count = h[1];
+      std::swap(qa, qb);
+    }
+    k += 1;
+  }
+  CU(cudaEventRecord(E.tev[5], s));
+  if (O.out_bits == 8 && J.kc_max > 255) {
+    // the reference's u8 level counter overflows (liu_et_al.rs:335-343)
+    set_error("a core number exceeds 255 with 8-bit output");
+    J.err = kErrOverflowU8;
+    return SPARX_E_OVERFLOW_U8;
+  }
+  if (N) {
+    if (O.out_bits == 8) k_kcore_out<uint8_t><<<vgrid, 256, 0, s>>>(core, N, (uint8_t*)J.out);
+    else k_kcore_out<uint32_t><<<vgrid, 256, 0, s>>>(core, N, (uint32_t*)J.out);
+    J.launches += 1;
+  }
+  CU(cudaEventRecord(E.tev[6], s));
+  CU(cudaEventRecord(E.tev[2], s));
+  CU(cudaEventRecord(E.tev[3], s));
+  CU(cudaStreamSynchronize(s));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, E.tev[4], E.tev[5]));
+  J.ms_peel = ms;
+  return SPARX_OK;
+}
+
 // Sums behind the clustering coefficients (out_host then holds one f64 local
 // coefficient per vertex).
 struct ClusterSums {
@@ -818,7 +943,7 @@ struct ClusterSums {
 // slot (support_only) or local clustering coefficients (cc != nullptr).
 int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int bits, uint64_t width,
              void* out_host, bool support_only, const sparx_pkt_opts* opts, sparx_pkt_stats* stats,
-             ClusterSums* cc = nullptr) {
+             ClusterSums* cc = nullptr, bool kcore = false) {
   g_last_error.clear();
   if (!offsets || (!nbrs && width) || (!out_host && width)) { set_error("null pointer"); return SPARX_E_ARG; }
   int rc = check_dims(n_plus_1, width);
@@ -839,9 +964,11 @@ int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int b
   J.members.push_back(Member{0, (uint32_t)n, 0, (uint32_t)width, 0, 0});
   J.support_only = support_only || cc;
   J.clustering = cc != nullptr;
+  J.kcore = kcore;
   support_only = J.support_only;
-  const size_t out_bytes = J.clustering ? 8 * n : support_only ? 4 * width : (O.out_bits / 8) * width;
-  J.L = make_layout(n, width, 1, true, out_bytes);
+  const size_t out_bytes = kcore ? (O.out_bits / 8) * n
+                           : J.clustering ? 8 * n : support_only ? 4 * width : (O.out_bits / 8) * width;
+  J.L = kcore ? make_kcore_layout(n, width, out_bytes) : make_layout(n, width, 1, true, out_bytes);
   rc = ensure_ws(E, J.L.total);
   if (rc) return rc;
   cudaStream_t s = E.stream;
@@ -879,7 +1006,7 @@ int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int b
                 (uint32_t)((width + kStageBytes / (bits / 8) - 1) / (kStageBytes / (bits / 8)));
   auto t_up_host = std::chrono::steady_clock::now();
   (void)t_up_host;
-  rc = run_union(E, J, O, s);
+  rc = kcore ? run_kcore(E, J, O, s) : run_union(E, J, O, s);
   if (rc) {
     fill_stats(J, 0, stats);
     return rc;
@@ -1440,6 +1567,15 @@ int sparx_pkt_run_u32(const uint64_t* offsets, uint64_t n_plus_1, const uint32_t
 int sparx_triangles_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
                         uint32_t* support_out, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
   return run_host(offsets, n_plus_1, neighbours, 64, width, support_out, true, opts, stats);
+}
+
+int sparx_kcore_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
+                    void* core_out, const sparx_pkt_opts* opts, sparx_pkt_stats* stats) {
+  if (n_plus_1 > 1 && !core_out) {
+    g_last_error = "null pointer";
+    return SPARX_E_ARG;
+  }
+  return run_host(offsets, n_plus_1, neighbours, 64, width, core_out, false, opts, stats, nullptr, true);
 }
 
 int sparx_clustering_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,

@@ -94,7 +94,7 @@ class GraphMemoryMap:
         r = self.index_node(u)
         return self._neighbours[r.start:r.stop]
 
-    # algorithm facade (graph/impl_algos.rs:29-40): k_truss is Burkhardt et al.'s by default
+    # algorithm facade (graph/impl_algos.rs:25-40): k_truss is Burkhardt et al.'s by default
     def k_truss(self):
         from .pkt import AlgoBurkhardtEtAl
         return AlgoBurkhardtEtAl.new(self)
@@ -102,6 +102,10 @@ class GraphMemoryMap:
     def k_truss_bea(self):
         from .pkt import AlgoBurkhardtEtAl
         return AlgoBurkhardtEtAl.new(self)
+
+    def k_core_lea(self):
+        from .pkt import AlgoLiuEtAl
+        return AlgoLiuEtAl.new(self)
 
     def k_truss_pkt(self):
         from .pkt import AlgoPKT

@@ -88,6 +88,7 @@ class _GraphView(ctypes.Structure):
 EXPORTS = [
     "sparx_pkt_default_opts", "sparx_strerror", "sparx_last_error", "sparx_pkt_run",
     "sparx_pkt_run_u32", "sparx_pkt_run_device", "sparx_triangles_run", "sparx_clustering_run",
+    "sparx_kcore_run",
     "sparx_pkt_run_batch",
     "sparx_pkt_run_device_noalloc",
     "sparx_server_create", "sparx_server_submit", "sparx_server_poll", "sparx_server_wait",
@@ -111,6 +112,8 @@ def lib():
         f = getattr(L, name)
         f.restype = i32
         f.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats)]
+    L.sparx_kcore_run.restype = i32
+    L.sparx_kcore_run.argtypes = [vp, u64, vp, u64, vp, P(_Opts), P(_Stats)]
     L.sparx_clustering_run.restype = i32
     L.sparx_clustering_run.argtypes = [vp, u64, vp, u64, vp, P(ctypes.c_double), P(ctypes.c_double),
                                        P(_Opts), P(_Stats)]
@@ -251,6 +254,20 @@ def run_clustering(offsets: np.ndarray, neighbours: np.ndarray, opts: PktOptions
     return local, trans.value, avg.value, PktStats.from_c(st)
 
 
+def run_kcore(offsets: np.ndarray, neighbours: np.ndarray, opts: PktOptions | None = None):
+    """Core number per vertex (u8 or u32 per ``opts.out_bits``) and stats, as
+    ``AlgoLiuEtAl::new`` computes them (k_core/liu_et_al.rs:45-62,190-420)."""
+    opts = opts or PktOptions()
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    nbr = np.ascontiguousarray(neighbours, dtype=np.uint64)
+    out = np.empty(max(off.shape[0] - 1, 0), dtype=np.uint8 if opts.out_bits == 8 else np.uint32)
+    st = _Stats()
+    o = opts.c()
+    _check(lib().sparx_kcore_run(off.ctypes.data, off.shape[0], nbr.ctypes.data, nbr.shape[0],
+                                 out.ctypes.data, ctypes.byref(o), ctypes.byref(st)))
+    return out, PktStats.from_c(st)
+
+
 def _cache_file(g: GraphMemoryMap, kind: str) -> str:
     os.makedirs(CACHE_DIR, exist_ok=True)
     return os.path.join(CACHE_DIR, f"{kind}_{g.graph_id()}.mmap")
@@ -333,6 +350,60 @@ class AlgoBurkhardtEtAl(AlgoPKT):
             mm[: truss.shape[0]] = truss
             mm.flush()
         return cls(g, truss, max(1, int(threads)), stats)
+
+
+class AlgoLiuEtAl:
+    """k-core decomposition of a ``GraphMemoryMap`` with the API of ``AlgoLiuEtAl``
+    (k_core/liu_et_al.rs:24-188): one core number per vertex, u8 in the reference's layout."""
+
+    _cache_kind = "kcorelea"
+
+    def __init__(self, g: GraphMemoryMap, k_cores: np.ndarray, threads: int,
+                 stats: PktStats | None = None):
+        self.g = g
+        self._k_cores = k_cores
+        self.threads = threads
+        self.stats = stats
+
+    @classmethod
+    def new(cls, g: GraphMemoryMap, opts: PktOptions | None = None) -> "AlgoLiuEtAl":
+        return cls.new_with_conf(g, g.thread_num(), opts)
+
+    @classmethod
+    def new_with_conf(cls, g: GraphMemoryMap, threads: int,
+                      opts: PktOptions | None = None) -> "AlgoLiuEtAl":
+        opts = opts or PktOptions()
+        off, nbr = _arrays(g)
+        cores, stats = run_kcore(off, nbr, opts)
+        if opts.out_bits == 8:
+            path = _cache_file(g, cls._cache_kind)
+            mm = np.memmap(path, dtype=np.uint8, mode="w+", shape=(max(1, cores.shape[0]),))
+            mm[: cores.shape[0]] = cores
+            mm.flush()
+        return cls(g, cores, max(1, int(threads)), stats)
+
+    @classmethod
+    def get_or_compute(cls, g: GraphMemoryMap, opts: PktOptions | None = None) -> "AlgoLiuEtAl":
+        path = _cache_file(g, cls._cache_kind)
+        if os.path.exists(path):
+            mm = np.memmap(path, dtype=np.uint8, mode="r")
+            if mm.shape[0] >= g.size():
+                return cls(g, np.asarray(mm[: g.size()]), g.thread_num())
+        return cls.new(g, opts)
+
+    def coreness(self, node: int) -> int:
+        assert node < self.g.size()
+        return int(self._k_cores[node])
+
+    def k_cores(self) -> np.ndarray:
+        return self._k_cores
+
+    def drop_cache(self) -> None:
+        os.remove(_cache_file(self.g, self._cache_kind))
+
+    def get_throughput_factor(self) -> int:
+        """liu_et_al.rs:186-188: the bench divides by the CSR width."""
+        return self.g.width()
 
 
 class ClusteringCoefficient:

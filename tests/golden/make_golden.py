@@ -7,8 +7,8 @@ graphs also store the full truss arrays.  The oracle used per workload is
 recorded: the restatement of the reference's PKT (oracle.pkt) wherever it
 finishes in minutes, cross-checked against the restated Burkhardt peel and
 the independent exact peel (oracle.fast_truss); the independent peel alone for
-R-MAT-22, where the restatement's hash-map-per-frontier-edge processing would
-take hours.
+R-MAT-22 and R-MAT-24, where the restatement's hash-map-per-frontier-edge
+processing would take hours.
 
     python tests/golden/make_golden.py [--only NAME ...]
 """
@@ -35,6 +35,8 @@ WORKLOADS = {
     "cfg1_er_100k_1m": dict(fn="er", n=100_000, m=1_000_000, seed=1, oracles=("pkt", "burkhardt", "fast"),
                             modes=(0, 1)),
     "cfg2_rmat22": dict(fn="rmat", scale=22, ef=16, seed=2, oracles=("fast",), modes=(0,)),
+    # config 5's 1% tail: the first R-MAT-24 request of the served stream
+    "cfg5_rmat24_tail": dict(fn="rmat", scale=24, ef=16, seed=100, oracles=("fast",), modes=(0,)),
     "cfg3_debruijn": dict(fn="dbg", seq_len=20_000_000, k=21, copies=1000, seg_len=10_000, mut_rate=0.05,
                           seed=3, oracles=("pkt", "fast"), modes=(0, 1)),
     "rmat16": dict(fn="rmat", scale=16, ef=16, seed=2, oracles=("pkt", "burkhardt", "fast"), modes=(0, 1)),

@@ -202,3 +202,37 @@ def test_clustering_matches_definition():
         else:
             assert trans == pytest.approx(want_trans, rel=1e-14)
         assert avg == pytest.approx(want_local.sum() / g.n, rel=1e-14)
+
+
+def _core_definition(g):
+    """Textbook core numbers: repeatedly remove a vertex of minimum remaining degree; its core
+    is the largest minimum seen so far (graphs without self-loops)."""
+    off = g.offsets.astype(np.int64)
+    adj = [set(int(x) for x in g.neighbours[off[u]:off[u + 1]]) for u in range(g.n)]
+    deg = {u: len(adj[u]) for u in range(g.n)}
+    core, level = {}, 0
+    while deg:
+        u = min(deg, key=lambda x: (deg[x], x))
+        level = max(level, deg[u])
+        core[u] = level
+        for v in adj[u]:
+            if v in deg:
+                deg[v] -= 1
+        del deg[u]
+    return np.array([core[u] for u in range(g.n)])
+
+
+def test_kcore_known_answers():
+    assert list(O.kcore(*(lambda g: (g.offsets, g.neighbours))(gen.from_edges(3, [(0, 1), (1, 2)])))) == [1, 1, 1]
+    assert list(O.kcore(kn(5).offsets, kn(5).neighbours)) == [4] * 5
+    g = gen.from_edges(5, [(0, 1), (0, 2), (0, 3), (1, 2)])  # triangle, a pendant, an isolated vertex
+    assert list(O.kcore(g.offsets, g.neighbours)) == [2, 2, 2, 1, 0]
+    # u8 degrees: K300's degree 299 wraps to 43, so every vertex is peeled at level 43
+    assert set(O.kcore(kn(300).offsets, kn(300).neighbours, mode=O.MODE_U8)) == {43}
+
+
+def test_kcore_matches_definition():
+    rng = np.random.default_rng(17)
+    for _ in range(60):
+        g = random_graph(rng, self_loop_p=0.0)
+        assert np.array_equal(O.kcore(g.offsets, g.neighbours), _core_definition(g))
