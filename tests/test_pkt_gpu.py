@@ -172,7 +172,8 @@ def test_self_loops_and_isolated():
     assert t0.size == 0
 
 
-@pytest.mark.parametrize("name", ["dbg_small", "rmat16", "rmat18", "cfg1_er_100k_1m", "cfg3_debruijn", "cfg2_rmat22"])
+@pytest.mark.parametrize("name", ["dbg_small", "rmat16", "rmat18", "cfg1_er_100k_1m", "cfg3_debruijn", "cfg2_rmat22",
+                                  "cfg5_rmat24_tail"])
 def test_golden_workloads(name):
     fx = fixtures()[name]
     p = fx["params"]
