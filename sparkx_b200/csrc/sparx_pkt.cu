@@ -775,7 +775,7 @@ void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
   st->self_loops = M.w - 2ull * M.m;
   if (g < J.mem_tri.size()) st->triangles = J.mem_tri[g] / 3;
   if (g < J.mem_maxsup.size()) st->max_support = J.mem_maxsup[g];
-  if (g < J.states.size()) {
+  if (g < J.states.size() && !J.support_only) {  // support-only runs have no peel state
     st->levels = J.states[g].levels;
     st->waves = J.states[g].waves;
     st->k_max = M.w ? J.states[g].max_level + 2 : 0;
