@@ -8,8 +8,8 @@ truss per CSR slot) of the workload graph.  Prints ONE JSON line on rank 0.
          launching stream; edges/s = CSR width (directed slots, the
          reference's throughput factor g.width()) / time, summed over ranks.
   e2e    the same through the reference-layout C ABI call (sparx_pkt_run) with
-         host u64 arrays: host->device upload and the u8 truss download are
-         inside the timed region.
+         host u64 arrays: host->device upload and the download of the 32-bit
+         truss numbers (one u32 per slot) are inside the timed region.
   --impl reference   the reference's CPU PKT (the oracle's restatement of
          pkt.rs, hash maps, all host threads) on a bounded sample of the same
          workload family.

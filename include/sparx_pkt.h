@@ -148,6 +148,9 @@ int sparx_kcore_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* 
  * (sum of d(d-1)/2); *average = sum of local / n.  In SPARX_SUPPORT_U8 mode the
  * slot supports are reduced mod 256 like the reference's AtomicU8 counts.  The
  * reference divides by 3 per worker thread; this is its one-thread value.
+ * These are the INTENDED coefficients: the reference's compute() zeroes the
+ * support counters before reading them (clustering_coefficient.rs:130-135),
+ * so it returns 0 for every coefficient; this call does not reproduce that.
  * local_out is f64[n]; transitivity and average may be NULL.
  */
 int sparx_clustering_run(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours,
@@ -159,21 +162,26 @@ int sparx_clustering_run(const uint64_t* offsets, uint64_t n_plus_1, const uint6
  * counterpart in the reference.
  *
  * For callers that must not allocate device memory when they ask for a
- * decomposition: code running while a stream is captured into a CUDA graph in
- * global or thread-local mode (cudaMalloc is not permitted there), services
- * whose device memory is reserved up front by their own pool, and
- * latency-critical paths that cannot wait for or fail on cudaMalloc.  All
- * scratch lives in one fixed file-scope device array of
+ * decomposition: services whose device memory is reserved up front by their
+ * own pool (an allocation outside it is a fault for them), and
+ * latency-critical request paths that cannot wait for or fail on cudaMalloc.
+ * All scratch lives in one fixed file-scope device array of
  * SPARX_NOALLOC_SCRATCH_BYTES per device (present on every GPU that loads the
  * library, until exit); graphs needing more get SPARX_E_TOO_LARGE (roughly
  * 1.4 M CSR slots).  The call allocates no device or pinned memory, streams or
- * events.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture begins.  All
+ * events.
+ *
+ * Each call looks up the array's device address on the current device
+ * (cudaGetSymbolAddress); the first call on a device also loads the library's
+ * device code there, so make that first call before any stream capture begins.
+ * The call is host-synchronous: it reads small results back and waits for
+ * `cuda_stream` several times and returns once the stream has finished the
+ * result, so `cuda_stream` must not be a stream that is being captured.  All
  * calls on a device share the array and it keeps the previous call's
- * contents: calls that overlap on the GPU (other streams, other host
- * threads) race and corrupt each other; serialize them.  The peel runs as
- * host-launched waves on `cuda_stream` and the call returns when the stream
- * has finished.
+ * contents (each call clears what must start at zero): calls that overlap on
+ * the GPU (other streams, other host threads) race and corrupt each other;
+ * serialize them.  A call that fails after its first launch waits for the
+ * stream before it returns, so the array is idle again.
  *   d_offsets u64[n_plus_1], d_neighbours u32[width], d_truss_out u32[width]
  *   device: CUDA ordinal (-1 = current)
  */

@@ -135,22 +135,35 @@ def kcore(off, nbr, mode=MODE_WIDE):
     return core
 
 
-def clustering(off, nbr, mode=MODE_WIDE, threads=1):
-    """Local clustering coefficients, transitivity and their average as
-    k_truss/clustering_coefficient.rs:93-190 computes them, with one worker (the reference
-    divides the triangle total by 3 per worker thread, clustering_coefficient.rs:157, so its
-    transitivity depends on the thread count; one worker is the exact value).
+def clustering(off, nbr, mode=MODE_WIDE, threads=1, faithful=False):
+    """Local clustering coefficients, transitivity and their average, with the
+    definitions of k_truss/clustering_coefficient.rs:93-190 but the INTENDED
+    triangle counts (default), or the reference's actual output (faithful=True).
 
-    For u with d distinct neighbours (the row's HashSet, clustering_coefficient.rs:140-155):
+    Reference defect D4: compute() builds the supports with Triangles::new
+    (clustering_coefficient.rs:105) and then, before reading them, overwrites
+    every slot's counter with AtomicU8::new(0) (:130-135).  The reference
+    therefore reads zero supports: every local coefficient is 0, the average is
+    0 and the transitivity is 0 / 2 / (sum of possible pairs), i.e. 0 (NaN when
+    no vertex has two neighbours).  It also sums a thread's slot supports into
+    `total_triangles_t`, whose type is inferred from the u8 load (:129,144), so
+    with real supports that running sum would wrap modulo 256.  faithful=True
+    returns exactly that zero output; the default computes what the code means:
+
+    For u with d distinct neighbours (the row's HashSet, :140-155):
     possible = d(d-1)/2 if d > 1 else 0; t = ceil(row support sum / 2); local = t / possible
     when possible is a normal float, else 0 (:160-172).  transitivity = (sum of all slot
-    supports // 3) / 2 / sum(possible) (:157,178-181); average = sum(local) / n (:177).
-    Slot supports come from ``triangles`` (AtomicU8 counts in MODE_U8)."""
+    supports // 3) / 2 / sum(possible) (:157,178-181), summed without the u8 wrap and with one
+    worker (the reference divides by 3 per worker thread, :157, so its value would depend on
+    the thread count); average = sum(local) / n (:177).  Slot supports come from
+    ``triangles`` (AtomicU8 counts in MODE_U8)."""
     off = np.ascontiguousarray(off, dtype=np.int64)
     nbr = np.ascontiguousarray(nbr, dtype=np.int64)
     n = len(off) - 1
     sup = triangles(off.astype(np.uint64), nbr.astype(np.uint64), mode=mode, threads=threads)
     sup = sup.astype(np.uint64)
+    if faithful:
+        sup[:] = 0  # clustering_coefficient.rs:130-135 zeroes the counters before reading them
     if mode == MODE_U8:
         sup &= np.uint64(0xFF)
     rows = np.repeat(np.arange(n), np.diff(off))

@@ -39,6 +39,10 @@
 //   D3 shared_slice.rs:665-682 push_slice refuses a push that exactly fills
 //      the queue (write_idx + len < max), so a frontier holding every slot
 //      (e.g. a lone triangle) is dropped; here the queues hold width + 1.
+// A fourth defect, in the clustering coefficient built on the supports (D4:
+// clustering_coefficient.rs:130-135 zeroes the supports before reading them),
+// is restated in oracle.py's `clustering`, which computes the intended
+// coefficients by default and the reference's zero output on request.
 //
 // Input: simple symmetric CSR (offsets u64[n+1], neighbour ids u32, rows
 // sorted ascending, no duplicate entries).  Self-loop slots are allowed and
@@ -436,10 +440,33 @@ int burkhardt(const Csr& g, const uint64_t* er, const uint32_t* sup0, int u8mode
   return ORC_OK;
 }
 
-// Sorted-list intersection of the rows of u and v, excluding u and v.
+// Sorted-list intersection of the rows of u and v, excluding u and v: f(i, j)
+// for every common neighbour, i its slot in u's row, j in v's.  Rows of
+// similar length are merged; otherwise each entry of the shorter row is
+// binary-searched in the longer one (a hub row of 10^5 entries is not walked
+// once per incident edge).
 template <class F>
 void for_common(const Csr& g, uint64_t u, uint64_t v, F&& f) {
   uint64_t i = g.off[u], ie = g.off[u + 1], j = g.off[v], je = g.off[v + 1];
+  const uint64_t du = ie - i, dv = je - j;
+  if (du * 16 < dv || dv * 16 < du) {
+    const bool u_short = du <= dv;
+    const uint64_t sb = u_short ? i : j, se = u_short ? ie : je;
+    const uint64_t lb = u_short ? j : i, le = u_short ? je : ie;
+    for (uint64_t x = sb; x < se; ++x) {
+      const uint32_t w = g.nbr[x];
+      if (w == u || w == v) continue;
+      uint64_t lo = lb, hi = le;
+      while (lo < hi) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (g.nbr[mid] < w) lo = mid + 1; else hi = mid;
+      }
+      if (lo < le && g.nbr[lo] == w) {
+        if (u_short) f(x, lo); else f(lo, x);
+      }
+    }
+    return;
+  }
   while (i < ie && j < je) {
     uint32_t a = g.nbr[i], b = g.nbr[j];
     if (a < b) ++i;
@@ -458,34 +485,38 @@ void for_common(const Csr& g, uint64_t u, uint64_t v, F&& f) {
 // two, so every graph with an edge fails (a 2-truss edge has 0 < 2).  Here:
 // symmetric truss on both slots; support among edges with truss >= k is at
 // least k - 2 (membership); support among edges with truss >= k + 1 is below
-// k - 1 (local maximality).  Returns the first failing slot + 1, or 0.
+// k - 1 (local maximality).  Returns the smallest failing slot + 1, or 0.
+// Vertices are handed out dynamically (hub rows would otherwise leave one
+// thread with most of the work).
 uint64_t verify(const Csr& g, const uint64_t* er, const uint32_t* truss, int T) {
   const uint64_t n = g.n;
-  std::atomic<uint64_t> bad{0};
-  const uint64_t load = (n + T - 1) / T;
-  run_threads(T, [&](int tid) {
-    uint64_t begin = std::min<uint64_t>(tid * load, n), end = std::min<uint64_t>(begin + load, n);
-    for (uint64_t u = begin; u < end && !bad.load(); ++u) {
-      for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s) {
-        uint64_t v = g.nbr[s];
-        if (v == u) {
-          if (truss[s] != 2) { bad = s + 1; return; }
-          continue;
-        }
-        if (v < u) continue;
-        uint32_t k = truss[s];
-        if (truss[er[s]] != k || k < 2) { bad = s + 1; return; }
-        uint64_t in_k = 0, in_k1 = 0;
-        for_common(g, u, v, [&](uint64_t i, uint64_t j) {
-          uint32_t a = truss[i], b = truss[j];
-          if (a >= k && b >= k) ++in_k;
-          if (a >= k + 1 && b >= k + 1) ++in_k1;
-        });
-        if (in_k + 2 < k || in_k1 + 1 >= k) { bad = s + 1; return; }
+  std::atomic<uint64_t> bad{UINT64_MAX};
+  auto fail = [&](uint64_t s) {
+    uint64_t cur = bad.load();
+    while (s < cur && !bad.compare_exchange_weak(cur, s)) {}
+  };
+#pragma omp parallel for schedule(dynamic, 64) num_threads(T)
+  for (uint64_t u = 0; u < n; ++u) {
+    for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s) {
+      uint64_t v = g.nbr[s];
+      if (v == u) {
+        if (truss[s] != 2) fail(s);
+        continue;
       }
+      if (v < u) continue;
+      uint32_t k = truss[s];
+      if (truss[er[s]] != k || k < 2) { fail(s); continue; }
+      uint64_t in_k = 0, in_k1 = 0;
+      for_common(g, u, v, [&](uint64_t i, uint64_t j) {
+        uint32_t a = truss[i], b = truss[j];
+        if (a >= k && b >= k) ++in_k;
+        if (a >= k + 1 && b >= k + 1) ++in_k1;
+      });
+      if (in_k + 2 < k || in_k1 + 1 >= k) fail(s);
     }
-  });
-  return bad.load();
+  }
+  const uint64_t b = bad.load();
+  return b == UINT64_MAX ? 0 : b + 1;
 }
 
 // Independent exact truss decomposition (no reference counterpart), used for

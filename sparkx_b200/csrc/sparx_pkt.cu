@@ -1651,15 +1651,16 @@ int sparx_pkt_run_device(const uint64_t* d_offsets, uint64_t n_plus_1, const uin
 // Allocation-free entry point (no counterpart in the reference).
 //
 // Some callers cannot allocate device memory at the moment they need a
-// decomposition: code that runs while a CUDA stream is being captured into a
-// graph in global or thread-local capture mode (cudaMalloc is not permitted
-// then), services that reserve all device memory up front through their own
-// pool and treat any allocation outside it as a fault, and latency-critical
-// request paths that must neither wait for nor fail on cudaMalloc.  For them
-// this variant of the single-graph pipeline keeps every scratch array in one
-// fixed, file-scope device array instead of the engine's workspace.  It
-// allocates nothing (device or pinned host memory, streams or events): the
-// caller passes device inputs and the device output, and a stream.
+// decomposition: services that reserve all device memory up front through
+// their own pool and treat any allocation outside it as a fault, and
+// latency-critical request paths that must neither wait for nor fail on
+// cudaMalloc.  For them this variant of the single-graph pipeline keeps every
+// scratch array in one fixed, file-scope device array instead of the engine's
+// workspace.  It allocates nothing (device or pinned host memory, streams or
+// events): the caller passes device inputs and the device output, and a
+// stream.  The call is host-synchronous: it reads scalars back and waits for
+// the stream several times, so `cuda_stream` must not be a stream that is
+// being captured.
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // per device; bounds the graph size below
@@ -1667,31 +1668,42 @@ constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // per device; bounds the 
 // Lives in every GPU that loads this library, until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mu;
 constexpr int kMaxDevices = 64;
-void* g_noalloc_addr[kMaxDevices] = {};
 
-// Device address of the scratch array for `device` (which must be current).
-// Host code cannot use the symbol itself as a device pointer, so the address is
-// looked up once per device and cached.
+// Device address of the scratch array on `device` (which must be current).
+// In host code the symbol is only a host-side stand-in, so the address is
+// looked up with cudaGetSymbolAddress.  The first call on a device also loads
+// the module there; later calls are cheap, and looking the address up on every
+// call (rather than caching it) keeps it right after a context is torn down
+// and recreated.
 int noalloc_scratch(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices) {
     set_error("device ordinal out of range");
     return SPARX_E_ARG;
   }
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      set_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-      return SPARX_E_CUDA;
-    }
-    g_noalloc_addr[device] = p;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    return SPARX_E_CUDA;
   }
-  *out = (unsigned char*)g_noalloc_addr[device];
+  *out = (unsigned char*)p;
   return SPARX_OK;
 }
+
+// Waits for the stream when a call leaves early after its first launch, so the
+// shared array is idle when the call returns (kernels already queued would
+// otherwise keep writing to it while the caller's next call starts).
+struct DrainOnExit {
+  cudaStream_t s;
+  bool armed = false;
+  ~DrainOnExit() {
+    if (armed) {
+      cudaStreamSynchronize(s);
+      cudaGetLastError();
+    }
+  }
+};
 
 // The same arrays as the engine's workspace, minus staging and output.
 Layout make_noalloc_layout(uint64_t N, uint64_t W) {
@@ -1765,6 +1777,8 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   const int wave_blocks = std::max(1, per_sm) * sm;
   const uint32_t N = (uint32_t)n;
 
+  DrainOnExit drain{s};
+  drain.armed = true;
   // the array keeps the previous call's contents: reset what must start at zero
   CU(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
   k_narrow_offsets<<<grid_for(n_plus_1, 256, sm * 16), 256, 0, s>>>((const unsigned long long*)d_offsets, off,
@@ -1773,7 +1787,10 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   Counters hc;
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
-  if (hc.err) return status_from_flags(hc.err);
+  if (hc.err) {
+    set_error("invalid CSR input (offsets or neighbour ids)");
+    return status_from_flags(hc.err);
+  }
 
   const int vgrid = grid_for(N, 256, sm * 32);  // row kernels: 32 vertices per warp
   uint32_t* big = (uint32_t*)P(L.big);  // big_count was cleared with the counters above
@@ -1785,10 +1802,19 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
-  if (hc.err) return status_from_flags(hc.err);
+  if (hc.err) {
+    set_error("invalid CSR input (row order, duplicates or ids)");
+    return status_from_flags(hc.err);
+  }
   const uint64_t m = m32;
-  if (2 * m + hc.self_loops != width) return SPARX_E_INVALID_CSR;
-  if (m > kEidMask) return SPARX_E_TOO_LARGE;
+  if (2 * m + hc.self_loops != width) {
+    set_error("CSR is not symmetric");
+    return SPARX_E_INVALID_CSR;
+  }
+  if (m > kEidMask) {
+    set_error("a graph has >= 2^28 edges");
+    return SPARX_E_TOO_LARGE;
+  }
   k_orient_fill<<<vgrid, 256, 0, s>>>(off, d_nbr, N, opos, ocol, osrc, row0, (uint32_t*)P(L.q0), big,
                                       &cnt->big_count);
   k_orient_reverse<<<grid_for(width, 256, sm * 16), 256, 0, s>>>(d_nbr, (uint32_t*)P(L.q0), width, opos, ocol,
@@ -1863,7 +1889,9 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
     k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(row0, es, width, d_out, 0, 0, &cnt->kmax, err);
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
+  drain.armed = false;
   CU(cudaGetLastError());
+  if (hc.err) set_error("device peel reported an error");
   return status_from_flags(hc.err);
 }
 

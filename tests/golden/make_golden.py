@@ -10,7 +10,14 @@ the independent exact peel (oracle.fast_truss); the independent peel alone for
 R-MAT-22 and R-MAT-24, where the restatement's hash-map-per-frontier-edge
 processing would take hours.
 
-    python tests/golden/make_golden.py [--only NAME ...]
+Every mode-0 fixture is also certified by the corrected verifier
+(oracle.verify: symmetric truss, support >= k - 2 inside the k-truss, local
+maximality), an independent check of the truss definition that does not
+depend on any peel; ``"verified": true`` records a pass.  ``--verify`` runs
+that certification alone on fixtures already in the file (regenerating each
+graph and its truss, which must hash to the stored values).
+
+    python tests/golden/make_golden.py [--only NAME ...] [--verify]
 """
 from __future__ import annotations
 
@@ -41,6 +48,8 @@ WORKLOADS = {
                           seed=3, oracles=("pkt", "fast"), modes=(0, 1)),
     "rmat16": dict(fn="rmat", scale=16, ef=16, seed=2, oracles=("pkt", "burkhardt", "fast"), modes=(0, 1)),
     "rmat18": dict(fn="rmat", scale=18, ef=16, seed=2, oracles=("pkt", "fast"), modes=(0, 1)),
+    # the PKT restatement against the independent peel one size above R-MAT-18
+    "rmat20": dict(fn="rmat", scale=20, ef=16, seed=2, oracles=("pkt", "fast"), modes=(0,)),
     "dbg_small": dict(fn="dbg", seq_len=200_000, k=21, copies=50, seg_len=2_000, mut_rate=0.05, seed=3,
                       oracles=("pkt", "burkhardt", "fast"), modes=(0, 1)),
     # small graphs whose full truss arrays are committed
@@ -121,6 +130,8 @@ def fixture(name, spec):
         out["modes"][str(mode)] = {"truss_sha256": truss_sha(base), "k_max": int(base.max()) if base.size else 0,
                                    "hist": {str(i): int(c) for i, c in enumerate(hist) if c},
                                    "oracles": list(results)}
+        if mode == 0:
+            out["modes"]["0"].update(certify(g, base))
         if spec.get("arrays"):
             arr = os.path.join(HERE, f"{name}.npz")
             prev = dict(np.load(arr)) if mode and os.path.exists(arr) else {}
@@ -131,6 +142,32 @@ def fixture(name, spec):
     out["seconds"] = round(time.time() - t0, 1)
     print(name, out["seconds"], "s", flush=True)
     return out
+
+
+def certify(g, truss):
+    """The corrected verifier's verdict on a truss assignment (mode 0 only: the
+    u8 mode's wrapped counts are not a truss decomposition)."""
+    t0 = time.time()
+    bad = O.verify(g.offsets, g.neighbours, truss, threads=os.cpu_count() or 1)
+    if bad >= 0:
+        raise SystemExit(f"verifier rejects slot {bad}")
+    return {"verified": True, "verify_seconds": round(time.time() - t0, 1)}
+
+
+def verify_existing(name, entry):
+    """Regenerate a stored fixture's graph and truss, check both hashes, certify."""
+    spec = WORKLOADS.get(name)
+    if spec is None and name.startswith("cfg4_mix_"):
+        spec = dict(fn="mix", index=int(name.rsplit("_", 1)[1]))
+    g = graph_for(spec)
+    if csr_sha(g) != entry["csr_sha256"]:
+        raise SystemExit(f"{name}: generator output changed")
+    truss = O.fast_truss(g.offsets, g.neighbours)[0]
+    if truss_sha(truss) != entry["modes"]["0"]["truss_sha256"]:
+        raise SystemExit(f"{name}: truss differs from the stored fixture")
+    res = certify(g, truss)
+    print(name, "verified in", res["verify_seconds"], "s", flush=True)
+    return res
 
 
 def mix_fixtures():
@@ -151,6 +188,7 @@ def mix_fixtures():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
+    ap.add_argument("--verify", action="store_true", help="certify stored fixtures only")
     args = ap.parse_args()
     O.build()
     path = os.path.join(HERE, "fixtures.json")
@@ -158,6 +196,15 @@ def main():
     if os.path.exists(path):
         with open(path) as f:
             data = json.load(f)
+    if args.verify:
+        for name in args.only or sorted(data):
+            res = verify_existing(name, data[name])
+            with open(path) as f:
+                current = json.load(f)
+            current[name]["modes"]["0"].update(res)
+            with open(path, "w") as f:
+                json.dump(current, f, indent=1, sort_keys=True)
+        return
     names = args.only or list(WORKLOADS) + ["cfg4_mix"]
     for name in names:
         if name == "cfg4_mix":

@@ -204,6 +204,21 @@ def test_clustering_matches_definition():
         assert avg == pytest.approx(want_local.sum() / g.n, rel=1e-14)
 
 
+def test_clustering_faithful_mode_reproduces_the_reference_zeroing():
+    """Defect D4: clustering_coefficient.rs:130-135 zeroes the supports before reading them,
+    so the reference's coefficients are all 0 (transitivity NaN without any possible pair).
+    The faithful mode pins that output; the default mode (what the GPU engine returns) keeps
+    the intended values."""
+    g = kn(5)
+    local, trans, avg = O.clustering(g.offsets, g.neighbours, faithful=True)
+    assert np.array_equal(local, np.zeros(5)) and trans == 0.0 and avg == 0.0
+    local, trans, avg = O.clustering(g.offsets, g.neighbours)
+    assert np.array_equal(local, np.ones(5)) and avg == 1.0
+    path = gen.from_edges(2, [(0, 1)])
+    _, trans, _ = O.clustering(path.offsets, path.neighbours, faithful=True)
+    assert np.isnan(trans)
+
+
 def _core_definition(g):
     """Textbook core numbers: repeatedly remove a vertex of minimum remaining degree; its core
     is the largest minimum seen so far (graphs without self-loops)."""
