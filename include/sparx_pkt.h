@@ -10,11 +10,16 @@
  * exactly those arrays and fill that result; every call returns a status
  * code (0 = SPARX_OK), never aborts, and never falls back to the CPU.
  *
- * Input contract (as produced by the reference's cache builders, minus
- * multi-edges): rows sorted strictly ascending, both directions of every
- * edge present, ids < n.  Self-loop slots are accepted and get truss 2
- * (triangles.rs:194-195, impl_csc.rs:148-153).  Parallel edges return
- * SPARX_E_MULTIGRAPH.
+ * Input contract (as produced by the reference's cache builders): rows
+ * sorted ascending, both directions of every edge present, ids < n.
+ * Self-loop slots are accepted and get truss 2 (triangles.rs:194-195,
+ * impl_csc.rs:148-153).  Parallel edges (equal ids side by side in a row, the
+ * reference's OneOrMany paths: impl_csc.rs:154-215, triangles.rs:172-224,
+ * pkt.rs:373-395) are accepted: a triangle is one choice of a copy of each of
+ * its three pairs, every copy of a pair gets the pair's truss number, and a
+ * pair must appear the same number of times in both of its rows
+ * (SPARX_E_INVALID_CSR otherwise).  Only the allocation-free entry point
+ * rejects parallel edges (SPARX_E_MULTIGRAPH).
  */
 #ifndef SPARX_PKT_H
 #define SPARX_PKT_H
@@ -29,12 +34,13 @@ extern "C" {
 /* ---- status codes ---------------------------------------------------- */
 #define SPARX_OK              0
 #define SPARX_E_INVALID_CSR   1  /* unsorted row, asymmetric, id >= n, bad offsets */
-#define SPARX_E_MULTIGRAPH    2  /* duplicate slot in a row */
+#define SPARX_E_MULTIGRAPH    2  /* parallel edges given to the allocation-free entry point */
 #define SPARX_E_OVERFLOW_U8   3  /* truss > 255 with 8-bit output (pkt.rs:508-516) */
 #define SPARX_E_OOM           4  /* device memory or HBM budget exhausted */
 #define SPARX_E_TIMEOUT       5  /* device-side peel exceeded its time budget */
 #define SPARX_E_CUDA          6  /* CUDA runtime error (see sparx_last_error) */
-#define SPARX_E_TOO_LARGE     7  /* width >= 2^32 or m >= 2^28 per graph */
+#define SPARX_E_TOO_LARGE     7  /* width >= 2^32, m >= 2^28 per graph, > 65535 copies of a pair,
+                                    or a multigraph support >= 2^31 */
 #define SPARX_E_ARG           8  /* bad argument */
 #define SPARX_E_NOT_FOUND     9  /* unknown ticket */
 #define SPARX_E_CANCELLED    10  /* request cancelled before completion */
@@ -57,8 +63,10 @@ typedef struct sparx_pkt_opts {
 } sparx_pkt_opts;
 
 typedef struct sparx_pkt_stats {
-  uint64_t n, width, m, self_loops;
-  uint64_t triangles;      /* sum of support / 3 (wide counters) */
+  uint64_t n, width, m, self_loops;  /* m: distinct pairs; self_loops: self-loop slots (not split
+                                        per member for a batched multigraph: 0 there) */
+  uint64_t triangles;      /* sum of support / 3 (wide counters); a multigraph counts each
+                              choice of copies of the three pairs */
   uint64_t max_support;    /* before the peel, after the u8 wrap in u8 mode */
   uint32_t k_max;          /* largest truss number */
   uint32_t levels;         /* non-empty peel levels */
@@ -169,7 +177,8 @@ int sparx_clustering_run(const uint64_t* offsets, uint64_t n_plus_1, const uint6
  * SPARX_NOALLOC_SCRATCH_BYTES per device (present on every GPU that loads the
  * library, until exit); graphs needing more get SPARX_E_TOO_LARGE (roughly
  * 1.4 M CSR slots).  The call allocates no device or pinned memory, streams or
- * events.
+ * events.  Parallel edges return SPARX_E_MULTIGRAPH (their deduplicated rows
+ * would need more scratch; sparx_pkt_run_device takes them).
  *
  * Each call looks up the array's device address on the current device
  * (cudaGetSymbolAddress); the first call on a device also loads the library's

@@ -236,35 +236,38 @@ def fast_truss(off, nbr, mode=MODE_WIDE, threads=None):
 def brute_force_truss(off, nbr):
     """Truss per slot straight from the definition: the k-truss is the largest
     subgraph in which every edge lies in >= k-2 triangles; an edge's truss is
-    the largest such k.  Pure Python: small graphs only."""
+    the largest such k.  In a multigraph a triangle is one choice of a copy of
+    each of its three pairs, so a copy of (u, v) lies in sum over common
+    neighbours w of mu(u, w) * mu(v, w) of them, and all copies of a pair share
+    its truss.  Pure Python: small graphs only."""
     off = np.asarray(off, dtype=np.int64)
     nbr = np.asarray(nbr, dtype=np.int64)
     n = len(off) - 1
-    adj = [set() for _ in range(n)]
-    edges = set()
+    mu = {}
     for u in range(n):
         for s in range(off[u], off[u + 1]):
             v = int(nbr[s])
-            if v != u:
-                adj[u].add(v)
-                edges.add((min(u, v), max(u, v)))
-    truss = {e: 2 for e in edges}
-    live = set(edges)
+            if v > u:
+                mu[(u, v)] = mu.get((u, v), 0) + 1
+    truss = {e: 2 for e in mu}
+    live = set(mu)
     k = 3
     while live:
         # peel to the k-truss of the current live graph
         ladj = {}
         for (u, v) in live:
-            ladj.setdefault(u, set()).add(v)
-            ladj.setdefault(v, set()).add(u)
+            ladj.setdefault(u, {})[v] = mu[(u, v)]
+            ladj.setdefault(v, {})[u] = mu[(u, v)]
         changed = True
         while changed:
             changed = False
             for (u, v) in list(live):
-                if len(ladj[u] & ladj[v]) < k - 2:
+                au, av = ladj[u], ladj[v]
+                sup = sum(c * av[w] for w, c in au.items() if w in av and w != u and w != v)
+                if sup < k - 2:
                     live.discard((u, v))
-                    ladj[u].discard(v)
-                    ladj[v].discard(u)
+                    del au[v]
+                    del av[u]
                     changed = True
         for e in live:
             truss[e] = k
@@ -274,4 +277,25 @@ def brute_force_truss(off, nbr):
         for s in range(off[u], off[u + 1]):
             v = int(nbr[s])
             out[s] = 2 if v == u else truss[(min(u, v), max(u, v))]
+    return out
+
+
+def support_definition(off, nbr):
+    """Triangles per slot from the definition (multigraph-aware): a copy of (u, v)
+    lies in sum over w != u, v of mu(u, w) * mu(v, w) triangles.  Small graphs."""
+    off = np.asarray(off, dtype=np.int64)
+    nbr = np.asarray(nbr, dtype=np.int64)
+    n = len(off) - 1
+    cnt = [dict() for _ in range(n)]
+    for u in range(n):
+        for s in range(off[u], off[u + 1]):
+            v = int(nbr[s])
+            if v != u:
+                cnt[u][v] = cnt[u].get(v, 0) + 1
+    out = np.zeros(len(nbr), dtype=np.uint64)
+    for u in range(n):
+        for s in range(off[u], off[u + 1]):
+            v = int(nbr[s])
+            if v != u:
+                out[s] = sum(c * cnt[v][w] for w, c in cnt[u].items() if w in cnt[v] and w != v)
     return out

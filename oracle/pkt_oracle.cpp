@@ -39,15 +39,20 @@
 //   D3 shared_slice.rs:665-682 push_slice refuses a push that exactly fills
 //      the queue (write_idx + len < max), so a frontier holding every slot
 //      (e.g. a lone triangle) is dropped; here the queues hold width + 1.
+// D5, in the multi-edge reciprocal index, is described at edge_index.
 // A fourth defect, in the clustering coefficient built on the supports (D4:
 // clustering_coefficient.rs:130-135 zeroes the supports before reading them),
 // is restated in oracle.py's `clustering`, which computes the intended
 // coefficients by default and the reference's zero output on request.
 //
-// Input: simple symmetric CSR (offsets u64[n+1], neighbour ids u32, rows
-// sorted ascending, no duplicate entries).  Self-loop slots are allowed and
-// get truss 2, as in the reference (triangles.rs:194, impl_csc.rs:148-153).
-// Parallel edges (the reference's OneOrMany paths) are rejected.
+// Input: symmetric CSR (offsets u64[n+1], neighbour ids u32, rows sorted
+// non-decreasing).  Self-loop slots are allowed and get truss 2, as in the
+// reference (triangles.rs:194, impl_csc.rs:148-153).  Parallel edges (equal
+// neighbour ids side by side in a row, as GGCAT's orientation labels give
+// them) follow the reference's OneOrMany paths: every copy is its own slot
+// with its own reciprocal (impl_csc.rs:154-215), a vertex maps to all of its
+// copies (triangles.rs:172-191, pkt.rs:373-395, burkhardt_et_al.rs:288-312),
+// and a triangle is one choice of a copy of each of its three pairs.
 #include <algorithm>
 #include <atomic>
 #include <barrier>
@@ -78,18 +83,22 @@ struct Csr {
   uint64_t width() const { return off[n]; }
 };
 
-int validate(const Csr& g) {
+// Rows sorted non-decreasing, ids < n; *multi tells whether any row repeats
+// a neighbour (a multigraph).
+int validate(const Csr& g, bool* multi = nullptr) {
   if (g.off[0] != 0) return ORC_E_INVALID;
+  bool dup = false;
   for (uint64_t u = 0; u < g.n; ++u) {
     if (g.off[u + 1] < g.off[u]) return ORC_E_INVALID;
     for (uint64_t i = g.off[u]; i < g.off[u + 1]; ++i) {
       if (g.nbr[i] >= g.n) return ORC_E_INVALID;
       if (i > g.off[u]) {
-        if (g.nbr[i] == g.nbr[i - 1]) return ORC_E_MULTIGRAPH;
+        if (g.nbr[i] == g.nbr[i - 1]) dup = true;
         if (g.nbr[i] < g.nbr[i - 1]) return ORC_E_INVALID;
       }
     }
   }
+  if (multi) *multi = dup;
   return ORC_OK;
 }
 
@@ -100,47 +109,66 @@ void run_threads(int T, const std::function<void(int)>& fn) {
   for (auto& x : th) x.join();
 }
 
-// Vertex -> slot lookup used where the reference keeps a HashMap<usize, _>
-// per vertex (triangles.rs:171, pkt.rs:323, burkhardt_et_al.rs:288).
+// Vertex -> slots lookup used where the reference keeps a
+// HashMap<usize, OneOrMany<usize>> per vertex (triangles.rs:171-191,
+// pkt.rs:373-395, burkhardt_et_al.rs:288-312): put() is called for a row's
+// slots in order, so the copies of one neighbour are consecutive slots and the
+// OneOrMany list is the range [first, first + count).
 //   HashSlots   std::unordered_map, for the timed CPU baseline.
 //   DenseSlots  a vertex-indexed array reset after each use; same answers.
 struct HashSlots {
-  std::unordered_map<uint64_t, uint64_t> m;
+  std::unordered_map<uint64_t, std::pair<uint64_t, uint64_t>> m;
   explicit HashSlots(uint64_t) {}
-  void put(uint64_t w, uint64_t slot) { m.emplace(w, slot); }
-  bool get(uint64_t w, uint64_t* slot) const {
+  void put(uint64_t w, uint64_t slot) {
+    auto it = m.try_emplace(w, slot, 0).first;
+    ++it->second.second;
+  }
+  bool get(uint64_t w, uint64_t* first, uint64_t* count) const {
     auto it = m.find(w);
     if (it == m.end()) return false;
-    *slot = it->second;
+    *first = it->second.first;
+    *count = it->second.second;
     return true;
   }
   void clear() { m.clear(); }
 };
 
 struct DenseSlots {
-  std::vector<uint64_t> slot;  // slot + 1, 0 = absent
+  std::vector<uint64_t> slot;  // first slot + 1, 0 = absent
+  std::vector<uint32_t> count;
   std::vector<uint64_t> used;
-  explicit DenseSlots(uint64_t n) : slot(n, 0) {}
+  explicit DenseSlots(uint64_t n) : slot(n, 0), count(n, 0) {}
   void put(uint64_t w, uint64_t s) {
-    if (!slot[w]) used.push_back(w);
-    slot[w] = s + 1;
+    if (!slot[w]) { used.push_back(w); slot[w] = s + 1; }
+    ++count[w];
   }
-  bool get(uint64_t w, uint64_t* s) const {
+  bool get(uint64_t w, uint64_t* first, uint64_t* cnt) const {
     if (!slot[w]) return false;
-    *s = slot[w] - 1;
+    *first = slot[w] - 1;
+    *cnt = count[w];
     return true;
   }
   void clear() {
-    for (uint64_t w : used) slot[w] = 0;
+    for (uint64_t w : used) { slot[w] = 0; count[w] = 0; }
     used.clear();
   }
 };
 
 // graph/impl_csc.rs:87-263.  Pass 1 (:124-139): eo[u] = first slot of u whose
 // neighbour id is > u, else off[u+1].  Pass 2 (:143-241): for each slot u->v
-// with v <= u: a self-loop is its own reciprocal (:148-153); otherwise binary
-// search u in v's upper part [eo[v], off[v+1]) and link both directions
-// (:217-235).  The multi-edge adjacency search (:154-215) has no input here.
+// with v <= u: a self-loop is its own reciprocal (:148-153); the first copy of
+// u->v binary-searches u in v's upper part (:217-235; the search may land on
+// any copy of u there); a second copy takes the slot just after, else just
+// before, the previous copy's reciprocal (:154-180); a later copy walks
+// forwards, then backwards, from the first copy's reciprocal to the first
+// copy of u not yet taken (:181-215).  Both directions are linked.
+//
+// Defect D5, not reproduced: the reference bounds neither those walks and
+// probes (only by the array's ends) nor its binary search (inclusive upper
+// bound off[v+1]) to v's row, so when v's copies of u end its row and row
+// v + 1 starts with u, a copy is paired with a slot of vertex v + 1 and a slot
+// of v stays unpaired (er is then not a pairing and the reference's supports
+// go to the wrong slots).  Here every probe stays inside [eo[v], off[v+1]).
 int edge_index(const Csr& g, uint64_t* eo, uint64_t* er, int T) {
   const uint64_t n = g.n;
   const uint64_t load = (n + T - 1) / T;
@@ -155,18 +183,68 @@ int edge_index(const Csr& g, uint64_t* eo, uint64_t* er, int T) {
       eo[u] = at;
     }
     sync.arrive_and_wait();
+    // prev: the previous slot's (v, reciprocal) pairs, One = a single entry
+    std::vector<std::pair<uint64_t, uint64_t>> prev;
     for (uint64_t u = begin; u < end; ++u) {
+      prev.assign(1, {n, 0});
       for (uint64_t s = g.off[u]; s < eo[u]; ++s) {
-        uint64_t v = g.nbr[s];
-        if (v == u) { er[s] = s; continue; }
-        uint64_t lo = eo[v], hi = g.off[v + 1];
-        while (lo < hi) {
-          uint64_t mid = lo + (hi - lo) / 2;
-          if (g.nbr[mid] < u) lo = mid + 1; else hi = mid;
+        const uint64_t v = g.nbr[s];
+        if (v == u) {
+          er[s] = s;
+          prev.assign(1, {v, s});
+          continue;
         }
-        if (lo == g.off[v + 1] || g.nbr[lo] != u) { status = ORC_E_INVALID; return; }
-        er[s] = lo;
-        er[lo] = s;
+        const uint64_t vb = eo[v], ve = g.off[v + 1];  // v's upper part (D5: probes stay inside)
+        if (prev[0].first == v) {
+          uint64_t rec = UINT64_MAX;
+          if (prev.size() == 1) {
+            const uint64_t po = prev[0].second;
+            if (po + 1 < ve && g.nbr[po + 1] == u) rec = po + 1;
+            else if (po > vb && g.nbr[po - 1] == u) rec = po - 1;
+          } else {
+            auto taken = [&](uint64_t r) {
+              for (auto& pr : prev) if (pr.second == r) return true;
+              return false;
+            };
+            uint64_t r = prev[0].second;
+            while (r + 1 < ve && g.nbr[r + 1] == u) {
+              ++r;
+              if (!taken(r)) { rec = r; break; }
+            }
+            if (rec == UINT64_MAX) {
+              r = prev[0].second;
+              while (r > vb && g.nbr[r - 1] == u) {
+                --r;
+                if (!taken(r)) { rec = r; break; }
+              }
+            }
+          }
+          if (rec == UINT64_MAX) { status = ORC_E_INVALID; return; }
+          prev.push_back({v, rec});
+          er[s] = rec;
+          er[rec] = s;
+          continue;
+        }
+        // the reference's probe order (floor + (ceil - floor) / 2 with ceil
+        // starting at off[v+1], which picks the copy of u it lands on); a probe
+        // at off[v+1] itself, outside the row, ends the search (D5)
+        uint64_t lo = vb, hi = ve, rec = UINT64_MAX;
+        while (lo <= hi) {
+          const uint64_t mid = lo + (hi - lo) / 2;
+          if (mid >= ve) break;
+          const uint64_t d = g.nbr[mid];
+          if (d == u) { rec = mid; break; }
+          if (d > u) {
+            if (mid == vb) break;
+            hi = mid - 1;
+          } else {
+            lo = mid + 1;
+          }
+        }
+        if (rec == UINT64_MAX) { status = ORC_E_INVALID; return; }
+        er[s] = rec;
+        er[rec] = s;
+        prev.assign(1, {v, rec});
       }
     }
   });
@@ -180,15 +258,22 @@ int edge_index(const Csr& g, uint64_t* eo, uint64_t* er, int T) {
       if (g.nbr[s] < u) ++lower; else ++upper;
     }
   }
-  return lower == upper ? ORC_OK : ORC_E_INVALID;
+  if (lower != upper) return ORC_E_INVALID;
+  // a copy paired twice leaves another unpaired: each upper slot must be the
+  // reciprocal of the lower slot that names it
+  for (uint64_t u = 0; u < n; ++u)
+    for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s)
+      if (er[er[s]] != s) return ORC_E_INVALID;
+  return ORC_OK;
 }
 
 // k_truss/triangles.rs:144-243.  Threads own vertex ranges (:159-168).  For
-// each u: map the upper neighbours w > u to their slots (:172-191); for each
-// lower slot u->v (v < u, v != u; :192-195) walk v's upper part backwards
-// while w > u (:197-200); each hit is the triangle v < u < w, credited on all
-// six directed slots (:206-211).  Counters are u32; u8 mode keeps the low
-// byte, which is what the reference's wrapping AtomicU8 adds leave.
+// each u: map the upper neighbours w > u to their slots (:172-191, all copies);
+// for each lower slot u->v (v < u, v != u; :192-195) walk v's upper part
+// backwards while w > u (:197-200); each copy u->w of a hit is the triangle
+// v < u < w, credited on all six directed slots (:201-222).  Counters are u32;
+// u8 mode keeps the low byte, which is what the reference's wrapping AtomicU8
+// adds leave.
 template <class Slots>
 void triangles(const Csr& g, const uint64_t* eo, const uint64_t* er, int T, int u8mode,
                uint32_t* sup) {
@@ -207,10 +292,12 @@ void triangles(const Csr& g, const uint64_t* eo, const uint64_t* er, int T, int 
         for (uint64_t vw = g.off[v + 1]; vw-- > eo[v];) {
           uint64_t w = g.nbr[vw];
           if (w <= u) break;
-          uint64_t uw;
-          if (!map.get(w, &uw)) continue;
-          const uint64_t slots[6] = {uv, vw, uw, er[uv], er[vw], er[uw]};
-          for (uint64_t x : slots) s[x].fetch_add(1, std::memory_order_relaxed);
+          uint64_t first, copies;
+          if (!map.get(w, &first, &copies)) continue;
+          for (uint64_t uw = first; uw < first + copies; ++uw) {
+            const uint64_t slots[6] = {uv, vw, uw, er[uv], er[vw], er[uw]};
+            for (uint64_t x : slots) s[x].fetch_add(1, std::memory_order_relaxed);
+          }
         }
       }
       map.clear();
@@ -325,19 +412,21 @@ int pkt(const Csr& g, const uint64_t* er, const uint32_t* sup0, int T, int u8mod
             if (prev <= l) s[x].store((uint32_t)l, std::memory_order_relaxed);
           };
           for (uint64_t vw = g.off[v]; vw < g.off[v + 1]; ++vw) {
-            uint64_t w = g.nbr[vw], uw;
-            if (!map.get(w, &uw)) continue;
-            uint64_t wu = er[uw];
-            if (processed[vw] || processed[wu]) continue;
-            uint32_t s_vw = s[vw].load(std::memory_order_relaxed);
-            uint32_t s_wu = s[wu].load(std::memory_order_relaxed);
-            if (s_vw > l && s_wu > l) {
-              dec(vw);
-              dec(wu);
-            } else if (s_vw > l && (uv < wu || !in_curr[wu])) {
-              dec(vw);
-            } else if (s_wu > l && (uv < vw || !in_curr[vw])) {
-              dec(wu);
+            uint64_t w = g.nbr[vw], first, copies;
+            if (!map.get(w, &first, &copies)) continue;
+            for (uint64_t uw = first; uw < first + copies; ++uw) {  // pkt.rs:404-409
+              uint64_t wu = er[uw];
+              if (processed[vw] || processed[wu]) continue;
+              uint32_t s_vw = s[vw].load(std::memory_order_relaxed);
+              uint32_t s_wu = s[wu].load(std::memory_order_relaxed);
+              if (s_vw > l && s_wu > l) {
+                dec(vw);
+                dec(wu);
+              } else if (s_vw > l && (uv < wu || !in_curr[wu])) {
+                dec(vw);
+              } else if (s_wu > l && (uv < vw || !in_curr[vw])) {
+                dec(wu);
+              }
             }
           }
           map.clear();
@@ -422,16 +511,18 @@ int burkhardt(const Csr& g, const uint64_t* er, const uint32_t* sup0, int u8mode
         if (w != u && w != v) map.put(w, uw);
       }
       for (uint64_t vw = g.off[v]; vw < g.off[v + 1]; ++vw) {
-        uint64_t w = g.nbr[vw], uw;
-        if (!map.get(w, &uw)) continue;
-        uint64_t wu = er[uw];
-        if (tris[vw] != 0 && tris[wu] != 0) {
-          uint32_t p = tris[wu]--;
-          if (u8mode) tris[wu] &= 0xFF;
-          if (p == k + 1) stack.push_back({w, wu});
-          p = tris[vw]--;
-          if (u8mode) tris[vw] &= 0xFF;
-          if (p == k + 1) stack.push_back({v, vw});
+        uint64_t w = g.nbr[vw], first, copies;
+        if (!map.get(w, &first, &copies)) continue;
+        for (uint64_t uw = first; uw < first + copies; ++uw) {  // :321-356, every copy
+          uint64_t wu = er[uw];
+          if (tris[vw] != 0 && tris[wu] != 0) {
+            uint32_t p = tris[wu]--;
+            if (u8mode) tris[wu] &= 0xFF;
+            if (p == k + 1) stack.push_back({w, wu});
+            p = tris[vw]--;
+            if (u8mode) tris[vw] &= 0xFF;
+            if (p == k + 1) stack.push_back({v, vw});
+          }
         }
       }
       map.clear();
@@ -440,30 +531,40 @@ int burkhardt(const Csr& g, const uint64_t* er, const uint32_t* sup0, int u8mode
   return ORC_OK;
 }
 
-// Sorted-list intersection of the rows of u and v, excluding u and v: f(i, j)
-// for every common neighbour, i its slot in u's row, j in v's.  Rows of
-// similar length are merged; otherwise each entry of the shorter row is
+// Sorted-list intersection of the rows of u and v, excluding u and v:
+// f(i, ci, j, cj) for every common neighbour w, with [i, i + ci) its copies in
+// u's row and [j, j + cj) in v's (ci = cj = 1 in a simple graph).  Rows of
+// similar length are merged; otherwise each neighbour of the shorter row is
 // binary-searched in the longer one (a hub row of 10^5 entries is not walked
 // once per incident edge).
 template <class F>
 void for_common(const Csr& g, uint64_t u, uint64_t v, F&& f) {
   uint64_t i = g.off[u], ie = g.off[u + 1], j = g.off[v], je = g.off[v + 1];
+  auto run = [&](uint64_t x, uint64_t end) {
+    uint64_t y = x + 1;
+    while (y < end && g.nbr[y] == g.nbr[x]) ++y;
+    return y - x;
+  };
   const uint64_t du = ie - i, dv = je - j;
   if (du * 16 < dv || dv * 16 < du) {
     const bool u_short = du <= dv;
     const uint64_t sb = u_short ? i : j, se = u_short ? ie : je;
     const uint64_t lb = u_short ? j : i, le = u_short ? je : ie;
-    for (uint64_t x = sb; x < se; ++x) {
+    for (uint64_t x = sb; x < se;) {
       const uint32_t w = g.nbr[x];
-      if (w == u || w == v) continue;
-      uint64_t lo = lb, hi = le;
-      while (lo < hi) {
-        const uint64_t mid = lo + (hi - lo) / 2;
-        if (g.nbr[mid] < w) lo = mid + 1; else hi = mid;
+      const uint64_t cx = run(x, se);
+      if (w != u && w != v) {
+        uint64_t lo = lb, hi = le;
+        while (lo < hi) {
+          const uint64_t mid = lo + (hi - lo) / 2;
+          if (g.nbr[mid] < w) lo = mid + 1; else hi = mid;
+        }
+        if (lo < le && g.nbr[lo] == w) {
+          const uint64_t cl = run(lo, le);
+          if (u_short) f(x, cx, lo, cl); else f(lo, cl, x, cx);
+        }
       }
-      if (lo < le && g.nbr[lo] == w) {
-        if (u_short) f(x, lo); else f(lo, x);
-      }
+      x += cx;
     }
     return;
   }
@@ -472,9 +573,10 @@ void for_common(const Csr& g, uint64_t u, uint64_t v, F&& f) {
     if (a < b) ++i;
     else if (b < a) ++j;
     else {
-      if (a != u && a != v) f(i, j);
-      ++i;
-      ++j;
+      const uint64_t ci = run(i, ie), cj = run(j, je);
+      if (a != u && a != v) f(i, ci, j, cj);
+      i += ci;
+      j += cj;
     }
   }
 }
@@ -483,9 +585,12 @@ void for_common(const Csr& g, uint64_t u, uint64_t v, F&& f) {
 // stored truss k, support_{>=k} >= k (:176-184) and support_{>=k+1} < k+1
 // (:188-197); with k = support level + 2 (pkt.rs:525) those bounds are off by
 // two, so every graph with an edge fails (a 2-truss edge has 0 < 2).  Here:
-// symmetric truss on both slots; support among edges with truss >= k is at
-// least k - 2 (membership); support among edges with truss >= k + 1 is below
-// k - 1 (local maximality).  Returns the smallest failing slot + 1, or 0.
+// symmetric truss on both slots, the same truss on every copy of a parallel
+// edge; support among edges with truss >= k is at least k - 2 (membership);
+// support among edges with truss >= k + 1 is below k - 1 (local maximality).
+// A common neighbour w counts once per choice of copies of u-w and v-w (the
+// reference's triangle count in a multigraph).  Returns the smallest failing
+// slot + 1, or 0.
 // Vertices are handed out dynamically (hub rows would otherwise leave one
 // thread with most of the work).
 uint64_t verify(const Csr& g, const uint64_t* er, const uint32_t* truss, int T) {
@@ -506,12 +611,20 @@ uint64_t verify(const Csr& g, const uint64_t* er, const uint32_t* truss, int T) 
       if (v < u) continue;
       uint32_t k = truss[s];
       if (truss[er[s]] != k || k < 2) { fail(s); continue; }
+      if (s > g.off[u] && g.nbr[s - 1] == v) {  // a later copy: same truss as the first
+        if (truss[s - 1] != k) fail(s);
+        continue;
+      }
       uint64_t in_k = 0, in_k1 = 0;
-      for_common(g, u, v, [&](uint64_t i, uint64_t j) {
+      bool mixed = false;
+      for_common(g, u, v, [&](uint64_t i, uint64_t ci, uint64_t j, uint64_t cj) {
         uint32_t a = truss[i], b = truss[j];
-        if (a >= k && b >= k) ++in_k;
-        if (a >= k + 1 && b >= k + 1) ++in_k1;
+        for (uint64_t x = 1; x < ci; ++x) mixed |= truss[i + x] != a;
+        for (uint64_t x = 1; x < cj; ++x) mixed |= truss[j + x] != b;
+        if (a >= k && b >= k) in_k += ci * cj;
+        if (a >= k + 1 && b >= k + 1) in_k1 += ci * cj;
       });
+      if (mixed) { fail(s); continue; }
       if (in_k + 2 < k || in_k1 + 1 >= k) fail(s);
     }
   }
@@ -526,8 +639,15 @@ uint64_t verify(const Csr& g, const uint64_t* er, const uint32_t* truss, int T) 
 // charges its surviving edges once, when its first edge is peeled, and ties
 // inside one frontier go to the smallest id.  Rows are rebuilt without
 // peeled edges whenever the live edge count halves.
-int fast_truss(const Csr& g, int T, int u8mode, uint32_t* truss_out, uint64_t* tri_out,
-               uint64_t* levels_out) {
+//
+// Multigraphs: the rows are first reduced to distinct neighbours with a
+// multiplicity mu per pair (all copies of a pair are interchangeable, so they
+// share one truss number); a triangle of pairs (e, f, h) then stands for
+// mu_e * mu_f * mu_h triangles of copies: a copy of e lies in mu_f * mu_h of
+// them, and peeling e removes mu_e * mu_h from each copy of f.  This weighted
+// peel shares no code with the copy-by-copy restatements above.
+int fast_truss_core(const Csr& g, const uint32_t* mult, int T, int u8mode, uint32_t* truss_out,
+                    uint64_t* tri_out, uint64_t* levels_out) {
   const uint64_t n = g.n, W = g.width();
   omp_set_num_threads(T);
   auto deg = [&](uint64_t x) { return g.off[x + 1] - g.off[x]; };
@@ -547,12 +667,17 @@ int fast_truss(const Csr& g, int T, int u8mode, uint32_t* truss_out, uint64_t* t
   const uint64_t m = upc[n];
   std::vector<uint64_t> eid(W, UINT64_MAX);
   std::vector<uint32_t> src(m), dst(m);
+  std::vector<int64_t> mu(m, 1);
   std::atomic<int> bad{0};
 #pragma omp parallel for schedule(static)
   for (uint64_t u = 0; u < n; ++u) {
     uint64_t p = upc[u];
     for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s)
-      if (g.nbr[s] > u) { eid[s] = p; src[p] = (uint32_t)u; dst[p] = g.nbr[s]; ++p; }
+      if (g.nbr[s] > u) {
+        eid[s] = p; src[p] = (uint32_t)u; dst[p] = g.nbr[s];
+        if (mult) mu[p] = mult[s];
+        ++p;
+      }
   }
 #pragma omp parallel for schedule(dynamic, 1024)
   for (uint64_t u = 0; u < n; ++u)
@@ -593,18 +718,20 @@ int fast_truss(const Csr& g, int T, int u8mode, uint32_t* truss_out, uint64_t* t
       uint64_t b = ocol[p];
       uint64_t i = opos[a], ie = opos[a + 1], j = opos[b], je = opos[b + 1];
       int64_t cnt = 0;
+      const int64_t mp = mu[oeid[p]];
       while (i < ie && j < je) {
         if (ocol[i] < ocol[j]) ++i;
         else if (ocol[j] < ocol[i]) ++j;
         else {
-          ++cnt;
-          as[oeid[i]].fetch_add(1, std::memory_order_relaxed);
-          as[oeid[j]].fetch_add(1, std::memory_order_relaxed);
+          const int64_t mi = mu[oeid[i]], mj = mu[oeid[j]];
+          cnt += mi * mj;
+          as[oeid[i]].fetch_add(mp * mj, std::memory_order_relaxed);
+          as[oeid[j]].fetch_add(mp * mi, std::memory_order_relaxed);
           ++i; ++j;
         }
       }
       if (cnt) as[oeid[p]].fetch_add(cnt, std::memory_order_relaxed);
-      tri += cnt;
+      tri += (uint64_t)(cnt * mp);
     }
   }
   if (tri_out) *tri_out = tri;
@@ -686,12 +813,12 @@ int fast_truss(const Csr& g, int T, int u8mode, uint32_t* truss_out, uint64_t* t
             bool fin = state[f] == 1, hin = state[h] == 1;
             if (fin && f < e) continue;
             if (hin && h < e) continue;
-            auto dec = [&](uint64_t x) {
-              int64_t prev = as[x].fetch_sub(1, std::memory_order_relaxed);
-              if (prev == l + 1) mine.push_back(x);
+            auto dec = [&](uint64_t x, int64_t d) {
+              int64_t prev = as[x].fetch_sub(d, std::memory_order_relaxed);
+              if (prev > l && prev - d <= l) mine.push_back(x);
             };
-            if (!fin && as[f].load(std::memory_order_relaxed) > l) dec(f);
-            if (!hin && as[h].load(std::memory_order_relaxed) > l) dec(h);
+            if (!fin && as[f].load(std::memory_order_relaxed) > l) dec(f, mu[e] * mu[h]);
+            if (!hin && as[h].load(std::memory_order_relaxed) > l) dec(h, mu[e] * mu[f]);
           }
         }
       }
@@ -713,6 +840,38 @@ int fast_truss(const Csr& g, int T, int u8mode, uint32_t* truss_out, uint64_t* t
     uint64_t v = (e == UINT64_MAX) ? 2 : (uint64_t)s[e] + 2;
     truss_out[x] = u8mode ? (uint32_t)(v & 0xFF) : (uint32_t)v;
   }
+  return ORC_OK;
+}
+
+// Multigraph front end of fast_truss_core: distinct neighbours per row with
+// their multiplicities, then every copy takes its pair's truss number.
+int fast_truss(const Csr& g, bool multi, int T, int u8mode, uint32_t* truss_out, uint64_t* tri_out,
+               uint64_t* levels_out) {
+  if (!multi) return fast_truss_core(g, nullptr, T, u8mode, truss_out, tri_out, levels_out);
+  const uint64_t n = g.n, W = g.width();
+  std::vector<uint64_t> off2(n + 1, 0);
+  for (uint64_t u = 0; u < n; ++u) {
+    uint64_t c = 0;
+    for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s) c += s == g.off[u] || g.nbr[s] != g.nbr[s - 1];
+    off2[u + 1] = off2[u] + c;
+  }
+  std::vector<uint32_t> nbr2(off2[n]), mult(off2[n], 0);
+  std::vector<uint64_t> to2(W);
+  for (uint64_t u = 0; u < n; ++u) {
+    uint64_t p = off2[u];
+    for (uint64_t s = g.off[u]; s < g.off[u + 1]; ++s) {
+      if (s > g.off[u] && g.nbr[s] == g.nbr[s - 1]) --p;
+      nbr2[p] = g.nbr[s];
+      ++mult[p];
+      to2[s] = p;
+      ++p;
+    }
+  }
+  std::vector<uint32_t> t2(off2[n]);
+  const int rc = fast_truss_core(Csr{n, off2.data(), nbr2.data()}, mult.data(), T, u8mode, t2.data(), tri_out,
+                                 levels_out);
+  if (rc) return rc;
+  for (uint64_t s = 0; s < W; ++s) truss_out[s] = t2[to2[s]];
   return ORC_OK;
 }
 
@@ -769,9 +928,10 @@ uint64_t orc_verify(uint64_t n, const uint64_t* off, const uint32_t* nbr, const 
 int orc_fast_truss(uint64_t n, const uint64_t* off, const uint32_t* nbr, int threads, int u8mode,
                    uint32_t* truss, uint64_t* triangles, uint64_t* levels) {
   Csr g{n, off, nbr};
-  int rc = validate(g);
+  bool multi = false;
+  int rc = validate(g, &multi);
   if (rc) return rc;
-  return fast_truss(g, threads < 1 ? 1 : threads, u8mode, truss, triangles, levels);
+  return fast_truss(g, multi, threads < 1 ? 1 : threads, u8mode, truss, triangles, levels);
 }
 
 }  // extern "C"

@@ -92,6 +92,7 @@ struct PeelArrays {
   uint4* qd1;
   const uint32_t* hub_slot;
   const uint32_t* hub_map;
+  const uint32_t* mu;  // multigraphs: multiplicity per edge id (nullptr: simple graph)
   uint32_t n;
 };
 
@@ -111,15 +112,16 @@ struct UnionRegs {
   uint4* qd1;
   const uint32_t* __restrict__ hub_slot;
   const uint32_t* __restrict__ hub_map;
+  const uint32_t* __restrict__ mu;
   uint32_t n;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
       : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]),
-        qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), n(p->n) {}
+        qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), mu(nullptr), n(p->n) {}
   __device__ __forceinline__ UnionRegs(const Union* p, const PeelArrays& a)
       : off(p->off), row(p->row), ocol(a.ocol), osrc(a.osrc), es(a.es),
         act0(a.act0), act1(a.act1), q0(a.q0), q1(a.q1),
-        qd0(a.qd0), qd1(a.qd1), hub_slot(a.hub_slot), hub_map(a.hub_map), n(a.n) {}
+        qd0(a.qd0), qd1(a.qd1), hub_slot(a.hub_slot), hub_map(a.hub_map), mu(a.mu), n(a.n) {}
 };
 
 // A queue-entry descriptor whose longer row belongs to a hub carries
@@ -741,11 +743,18 @@ __device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i,
                                                 unsigned long long j, bool valid);
 
 // 8 resident blocks per SM (32 registers): the pass is latency-bound and
-// loses more to fewer warps than to the few spilled values
+// loses more to fewer warps than to the few spilled values.
+//
+// kMulti (multigraphs, `mu` = multiplicity per edge id): a triangle of pairs
+// (e, f, h) stands for mu_e * mu_f * mu_h triangles of copies, so a copy of e
+// is credited mu_f * mu_h (each hit lane adds its own product; the one-atomic
+// run credit of the simple form is for unit weights only).
+template <bool kMulti>
 __global__ void __launch_bounds__(256, 8) k_support_balanced(
     const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
     const uint32_t* __restrict__ osrc, const unsigned long long* __restrict__ spref, uint32_t m,
-    int2* __restrict__ es, unsigned long long* __restrict__ tri_total, uint32_t* __restrict__ err) {
+    int2* __restrict__ es, unsigned long long* __restrict__ tri_total, uint32_t* __restrict__ err,
+    const uint32_t* __restrict__ mu) {
   const uint32_t lane = lane_id();
   const unsigned long long total = spref[m];
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -779,17 +788,27 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
         if (q < le && __ldg(ocol + q) == c) p = q;
       }
       const bool hit = valid && p != kInvalid;
-      if (hit) {
-        atomicAdd(&es[sb + o].x, 1);
-        atomicAdd(&es[p].x, 1);
-        found_total++;
-      }
-      // credit e once per run of lanes sharing it
-      const unsigned hits = __ballot_sync(kFull, hit);
-      const unsigned grp = __match_any_sync(kFull, valid ? e : kInvalid);
-      if (valid && lane == (uint32_t)(__ffs(grp) - 1)) {
-        const int cnt = __popc(grp & hits);
-        if (cnt) atomicAdd(&es[e].x, cnt);
+      if (kMulti) {
+        if (hit) {
+          const uint32_t me = __ldg(mu + e), mf = __ldg(mu + sb + o), mh = __ldg(mu + p);
+          atomicAdd(&es[sb + o].x, (int)(me * mh));
+          atomicAdd(&es[p].x, (int)(me * mf));
+          atomicAdd(&es[e].x, (int)(mf * mh));
+          found_total += (unsigned long long)me * mf * mh;
+        }
+      } else {
+        if (hit) {
+          atomicAdd(&es[sb + o].x, 1);
+          atomicAdd(&es[p].x, 1);
+          found_total++;
+        }
+        // credit e once per run of lanes sharing it
+        const unsigned hits = __ballot_sync(kFull, hit);
+        const unsigned grp = __match_any_sync(kFull, valid ? e : kInvalid);
+        if (valid && lane == (uint32_t)(__ffs(grp) - 1)) {
+          const int cnt = __popc(grp & hits);
+          if (cnt) atomicAdd(&es[e].x, cnt);
+        }
       }
       i = e_last;
       // fast path: while the next 32 elements all lie inside edge i, the
@@ -830,13 +849,23 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
           }
           const uint32_t q = lower_bound_u32(ocol, lo, hi, c);
           const bool fh = q < hi && __ldg(ocol + q) == c;
-          if (fh) {
-            atomicAdd(&es[fsb + fo].x, 1);
-            atomicAdd(&es[q].x, 1);
-            found_total++;
+          if (kMulti) {
+            if (fh) {
+              const uint32_t me = __ldg(mu + i), mf = __ldg(mu + fsb + fo), mh = __ldg(mu + q);
+              atomicAdd(&es[fsb + fo].x, (int)(me * mh));
+              atomicAdd(&es[q].x, (int)(me * mf));
+              atomicAdd(&es[i].x, (int)(mf * mh));
+              found_total += (unsigned long long)me * mf * mh;
+            }
+          } else {
+            if (fh) {
+              atomicAdd(&es[fsb + fo].x, 1);
+              atomicAdd(&es[q].x, 1);
+              found_total++;
+            }
+            const int cnt = __popc(__ballot_sync(kFull, fh));
+            if (lane == 0 && cnt) atomicAdd(&es[i].x, cnt);
           }
-          const int cnt = __popc(__ballot_sync(kFull, fh));
-          if (lane == 0 && cnt) atomicAdd(&es[i].x, cnt);
         } while (kb + 64 <= stop);
       }
     }
@@ -1092,9 +1121,12 @@ __device__ __forceinline__ void flush_member_stats(uint32_t g, unsigned long lon
   if (mx) atomicMax(mem_maxsup + g, mx);
 }
 
+// Multigraphs (mu != nullptr): a pair's support is per copy, so its triangle
+// credits are support * mu; a support that wrapped past 2^31 is a capacity error.
 __global__ void __launch_bounds__(256) k_peel_setup(const Union* __restrict__ Up, const Member* __restrict__ mem,
                                                     int u8mode, unsigned long long* __restrict__ mem_tri,
-                                                    uint32_t* __restrict__ mem_maxsup) {
+                                                    uint32_t* __restrict__ mem_maxsup,
+                                                    const uint32_t* __restrict__ mu, uint32_t* __restrict__ err) {
   const Union U = *Up;
   const uint32_t G = U.G;
   uint32_t cur = kInvalid;
@@ -1115,7 +1147,12 @@ __global__ void __launch_bounds__(256) k_peel_setup(const Union* __restrict__ Up
       cur = g; sum = 0; mx = 0;
     }
     int32_t s = U.es[e].x;
-    sum += (unsigned long long)s;
+    if (mu) {
+      if (s < 0) atomicOr(err, kErrCapacity);
+      sum += (unsigned long long)(uint32_t)s * __ldg(mu + e);
+    } else {
+      sum += (unsigned long long)s;
+    }
     if (u8mode) s &= 0xFF;
     U.es[e] = make_int2(s, (int)kTagActive);
     mx = max(mx, (uint32_t)s);
@@ -1202,8 +1239,14 @@ __device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x) {
 //   only f above l                      -> charge f unless h is in this frontier
 //                                          with a smaller id than e
 //   only h above l                      -> symmetric
-// A charge that lands on l + 1 queues the edge for the next sub-level; a
-// charge that goes below l is restored to l.
+// A charge that takes the support from above l to l or below queues the edge
+// for the next sub-level; a charge that goes below l is restored to l.
+//
+// A charge is 1 in a simple graph.  In a multigraph (kMulti) a triangle of
+// pairs stands for mu_e * mu_f * mu_h triangles of copies, and peeling e
+// removes mu_e * mu_h of them from each copy of f (mu_e * mu_f from h): the
+// charge is that product, applied at once.
+template <bool kMulti>
 __device__ __forceinline__ void pkt_rule(const UnionRegs& U, uint32_t e, uint32_t f, int2 es_f, uint32_t h,
                                          uint32_t l, uint32_t W, bool& pf, bool& ph) {
   pf = ph = false;
@@ -1216,15 +1259,21 @@ __device__ __forceinline__ void pkt_rule(const UnionRegs& U, uint32_t e, uint32_
   if (sf > L && sh > L) { df = true; dh = true; }
   else if (sf > L) df = (e < h) || (th != W);
   else if (sh > L) dh = (e < f) || (tf != W);
+  int32_t cf = 1, ch = 1;
+  if (kMulti && (df || dh)) {
+    const int32_t me = (int32_t)__ldg(U.mu + e), mf = (int32_t)__ldg(U.mu + f), mh = (int32_t)__ldg(U.mu + h);
+    cf = me * mh;
+    ch = me * mf;
+  }
   if (df) {
-    int32_t prev = atomicSub(&U.es[f].x, 1);
-    if (prev == L + 1) pf = true;
-    else if (prev <= L) atomicMax(&U.es[f].x, L);
+    int32_t prev = atomicSub(&U.es[f].x, cf);
+    if (prev > L && prev - cf <= L) pf = true;
+    if (prev - cf < L) atomicMax(&U.es[f].x, L);
   }
   if (dh) {
-    int32_t prev = atomicSub(&U.es[h].x, 1);
-    if (prev == L + 1) ph = true;
-    else if (prev <= L) atomicMax(&U.es[h].x, L);
+    int32_t prev = atomicSub(&U.es[h].x, ch);
+    if (prev > L && prev - ch <= L) ph = true;
+    if (prev - ch < L) atomicMax(&U.es[h].x, L);
   }
 }
 
@@ -1280,6 +1329,9 @@ constexpr int kKeepBuf = 256;
 #define SPARX_MERGE_CHUNKS 2  // long-row chunks of 32 entries loaded per merge round
 #endif
 constexpr int kMergeChunks = SPARX_MERGE_CHUNKS;
+#ifndef SPARX_STATE_AFTER_SEARCH
+#define SPARX_STATE_AFTER_SEARCH 1  // read the other edges' states after the search, on hits only
+#endif
 
 struct PushStage {
   uint32_t* eid;  // this warp's kPushBuf staged edges
@@ -1493,6 +1545,7 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
 //                       <= level -> queued for this level; else kept
 //   frontier element j  element o of the shorter working row of frontier
 //                       edge e, searched in the longer row; a hit is a triangle
+template <bool kMulti>
 __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs a) {
   __shared__ uint32_t s_push_eid[kWaveWarps][kPushBuf];
   __shared__ uint32_t s_keep[kWaveWarps][kKeepBuf];
@@ -1586,12 +1639,14 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           uint32_t f = (uint32_t)(pr >> 32), h = kInvalid, p = kInvalid;
           // f == kInvalid: a self-loop entry; f == e: the frontier edge itself
           bool look = el && f != kInvalid && f != e;
-          // the other edge of the short row: already processed -> nothing to resolve
           int2 es_f = make_int2(0, 0);
+#if !SPARX_STATE_AFTER_SEARCH
+          // the other edge of the short row: already processed -> nothing to resolve
           if (look) {
             es_f = U.es[f];
             look = (uint32_t)es_f.y >= W;
           }
+#endif
           // lane 0 is always valid: its rows decide, so the branch and the
           // merge below are warp-uniform
           const uint32_t e0 = __shfl_sync(kFull, e, 0);
@@ -1674,7 +1729,13 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           const bool hit = look && p != kInvalid && h != kInvalid;
           const uint32_t nhit = __popc(__ballot_sync(kFull, hit));
           if (lane == 0) s_cnt[0][wib] += nhit;
-          if (hit) pkt_rule(U, e, f, es_f, h, level, W, pf, ph);
+#if SPARX_STATE_AFTER_SEARCH
+          // both other edges' states are read only for a found triangle (a
+          // quarter of the elements on R-MAT); the search may run for an f
+          // that is already processed, which pkt_rule then skips
+          if (hit) es_f = U.es[f];
+#endif
+          if (hit) pkt_rule<kMulti>(U, e, f, es_f, h, level, W, pf, ph);
           push_edge(ps, U, M, st, a.err, q_sel, pf, f, W);
           push_edge(ps, U, M, st, a.err, q_sel, ph, h, W);
           i = x_last;
@@ -2009,16 +2070,19 @@ __global__ void k_compact_commit(Union* U, const uint32_t* off2, const unsigned 
 
 
 // Kernel E: truss per slot = level + 2 (pkt.rs:524-526); self-loop slots 2.
+// Multigraphs: `smap` takes each slot of the caller's CSR to its pair's slot
+// in the deduplicated rows (nullptr: the rows are the caller's).
 template <typename OutT>
 __global__ void k_finalize(const unsigned long long* __restrict__ row0, const int2* __restrict__ es,
                            unsigned long long width, OutT* __restrict__ out, int u8mode, int out8,
-                           uint32_t* __restrict__ kmax, uint32_t* __restrict__ err) {
+                           uint32_t* __restrict__ kmax, uint32_t* __restrict__ err,
+                           const uint32_t* __restrict__ smap) {
   unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   uint32_t mx = 0;
   bool ovf = false;
   for (; i < width; i += stride) {
-    const uint32_t e = (uint32_t)(__ldg(row0 + i) >> 32);
+    const uint32_t e = (uint32_t)(__ldg(row0 + (smap ? __ldg(smap + i) : i)) >> 32);
     uint32_t t = 2;
     if (e != kInvalid) {
       const uint32_t s = (uint32_t)__ldg(&es[e].x);
@@ -2155,12 +2219,16 @@ __device__ __forceinline__ uint32_t slot_support(unsigned long long pr, const in
   return u8mode ? (s & 0xFFu) : s;
 }
 
+// Multigraphs: the rows are the deduplicated ones (so d counts distinct
+// neighbours, the reference's HashSet) and `mult` gives each slot's copies,
+// every copy carrying the pair's support.
 __global__ void __launch_bounds__(256) k_clustering(const uint32_t* __restrict__ off,
                                                     const unsigned long long* __restrict__ row0,
                                                     const int2* __restrict__ es, uint32_t n, int u8mode,
                                                     double* __restrict__ local, double* __restrict__ sum_possible,
                                                     double* __restrict__ sum_local,
-                                                    unsigned long long* __restrict__ sum_slots) {
+                                                    unsigned long long* __restrict__ sum_slots,
+                                                    const uint32_t* __restrict__ mult) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -2172,14 +2240,16 @@ __global__ void __launch_bounds__(256) k_clustering(const uint32_t* __restrict__
     if (u < n) { b = __ldg(off + u); e = __ldg(off + u + 1); }
     unsigned long long ts = 0;
     if (u < n && e - b <= kLaneRow)
-      for (uint32_t s = b; s < e; ++s) ts += slot_support(__ldg(row0 + s), es, u8mode);
+      for (uint32_t s = b; s < e; ++s)
+        ts += (unsigned long long)slot_support(__ldg(row0 + s), es, u8mode) * (mult ? __ldg(mult + s) : 1u);
     unsigned big = __ballot_sync(kFull, u < n && e - b > kLaneRow);
     while (big) {
       const int j = __ffs(big) - 1;
       big &= big - 1;
       const uint32_t bb = __shfl_sync(kFull, b, j), be = __shfl_sync(kFull, e, j);
       unsigned long long c = 0;
-      for (uint32_t s = bb + lane; s < be; s += 32) c += slot_support(__ldg(row0 + s), es, u8mode);
+      for (uint32_t s = bb + lane; s < be; s += 32)
+        c += (unsigned long long)slot_support(__ldg(row0 + s), es, u8mode) * (mult ? __ldg(mult + s) : 1u);
 #pragma unroll
       for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(kFull, c, d);
       if (lane == (uint32_t)j) ts = c;
@@ -2209,14 +2279,98 @@ __global__ void __launch_bounds__(256) k_clustering(const uint32_t* __restrict__
 }
 
 __global__ void k_support_slots(const unsigned long long* __restrict__ row0, const int2* __restrict__ es,
-                                unsigned long long width, uint32_t* __restrict__ out, int u8mode) {
+                                unsigned long long width, uint32_t* __restrict__ out, int u8mode,
+                                const uint32_t* __restrict__ smap) {
   unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (; i < width; i += stride) {
-    const uint32_t e = (uint32_t)(__ldg(row0 + i) >> 32);
+    const uint32_t e = (uint32_t)(__ldg(row0 + (smap ? __ldg(smap + i) : i)) >> 32);
     uint32_t s = e == kInvalid ? 0u : (uint32_t)__ldg(&es[e].x);
     out[i] = u8mode ? (s & 0xFFu) : s;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Multigraphs (the reference's OneOrMany paths, impl_csc.rs:154-215,
+// triangles.rs:172-224, pkt.rs:373-395): parallel edges are equal neighbour
+// ids side by side in a row.  All copies of a pair are interchangeable, so
+// they share one truss number; the engine reduces each row to its distinct
+// neighbours with a multiplicity per slot, runs the weighted support and peel
+// on those rows, and maps every caller slot back to its pair.  A warp per row
+// (cold path: only multigraphs take it).
+//   k_dedupe_count  distinct neighbours per row
+//   k_dedupe_fill   deduplicated rows, copies per slot, caller slot -> slot
+//   k_mult_out      multiplicity per edge id, from each pair's out-slot
+//   k_mult_check    an in-slot must agree (else the CSR is not symmetric)
+__global__ void __launch_bounds__(256) k_dedupe_count(const uint32_t* __restrict__ off,
+                                                      const uint32_t* __restrict__ nbr, uint32_t n,
+                                                      uint32_t* __restrict__ dcount) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    uint32_t c = 0;
+    for (uint32_t s0 = b; s0 < e; s0 += 32) {
+      const uint32_t s = s0 + lane;
+      const bool head = s < e && (s == b || __ldg(nbr + s) != __ldg(nbr + s - 1));
+      c += __popc(__ballot_sync(kFull, head));
+    }
+    if (lane == 0) dcount[u] = c;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dedupe_fill(const uint32_t* __restrict__ off,
+                                                     const uint32_t* __restrict__ nbr, uint32_t n,
+                                                     const uint32_t* __restrict__ off2,
+                                                     uint32_t* __restrict__ nbr2, uint32_t* __restrict__ mult2,
+                                                     uint32_t* __restrict__ smap, uint32_t* __restrict__ err) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+    uint32_t p0 = __ldg(off2 + u);  // slot of the run before this chunk's first head, + 1
+    for (uint32_t s0 = b; s0 < e; s0 += 32) {
+      const uint32_t s = s0 + lane;
+      const uint32_t v = s < e ? __ldg(nbr + s) : 0u;
+      const bool head = s < e && (s == b || v != __ldg(nbr + s - 1));
+      const unsigned hb = __ballot_sync(kFull, head);
+      // the run holding slot s: heads up to and including this lane
+      const uint32_t pos = p0 + __popc(hb & (0xFFFFFFFFu >> (31 - lane))) - 1;
+      if (s < e) {
+        if (head) nbr2[pos] = v;
+        smap[s] = pos;
+        const uint32_t c = atomicAdd(mult2 + pos, 1u);
+        if (c == 0xFFFFu) atomicOr(err, kErrCapacity);  // more than 65535 copies of one pair
+      }
+      p0 += __popc(hb);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_mult_out(const unsigned long long* __restrict__ row0,
+                                                  const uint32_t* __restrict__ owner,
+                                                  const uint32_t* __restrict__ mult2, unsigned long long width,
+                                                  uint32_t* __restrict__ mu) {
+  for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < width;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t e = (uint32_t)(__ldg(row0 + s) >> 32);
+    if (e != kInvalid && __ldg(owner + s) == kInvalid) mu[e] = __ldg(mult2 + s);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_mult_check(const unsigned long long* __restrict__ row0,
+                                                    const uint32_t* __restrict__ owner,
+                                                    const uint32_t* __restrict__ mult2, unsigned long long width,
+                                                    const uint32_t* __restrict__ mu, uint32_t* __restrict__ err) {
+  bool bad = false;
+  for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < width;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t e = (uint32_t)(__ldg(row0 + s) >> 32);
+    if (e != kInvalid && __ldg(owner + s) != kInvalid) bad |= __ldg(mu + e) != __ldg(mult2 + s);
+  }
+  if (bad) atomicOr(err, kErrAsym);
 }
 
 }  // namespace sparx

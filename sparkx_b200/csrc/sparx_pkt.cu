@@ -172,7 +172,10 @@ struct Engine {
   cudaEvent_t tev[8] = {};
   void* pinned_small = nullptr;  // 4 KB for scalar read-backs
   PeelGraph peel;
-  int wave_blocks = 0;
+  int wave_blocks = 0;        // k_wave<false> grid (resident blocks per SM x SMs)
+  int wave_blocks_multi = 0;  // k_wave<true> grid (multigraphs)
+  char* ws2 = nullptr;        // multigraph rows, multiplicities and slot map (allocated on first use)
+  size_t ws2_cap = 0;
   ulonglong4* trace = nullptr;  // wave trace records (SPARX_TRACE_FILE set)
   std::mutex mu;
 };
@@ -196,8 +199,10 @@ int engine_init(Engine& E, int device) {
   for (auto& e : E.tev) CU(cudaEventCreate(&e));
   CU(cudaHostAlloc(&E.pinned_small, 4096, cudaHostAllocDefault));
   int per_sm = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave, 256, 0));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave<false>, 256, 0));
   E.wave_blocks = std::max(1, per_sm) * E.sm_count;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave<true>, 256, 0));
+  E.wave_blocks_multi = std::max(1, per_sm) * E.sm_count;
   return SPARX_OK;
 }
 
@@ -242,6 +247,20 @@ int ensure_ws(Engine& E, size_t bytes) {
     }
   }
   E.ws_cap = cap;
+  return SPARX_OK;
+}
+
+int ensure_ws2(Engine& E, size_t bytes) {
+  if (E.ws2_cap >= bytes) return SPARX_OK;
+  if (E.ws2) { CU(cudaStreamSynchronize(E.stream)); CU(cudaFree(E.ws2)); E.ws2 = nullptr; E.ws2_cap = 0; }
+  cudaError_t e = cudaMalloc(&E.ws2, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("multigraph workspace of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+    E.ws2 = nullptr;
+    return SPARX_E_OOM;
+  }
+  E.ws2_cap = bytes;
   return SPARX_OK;
 }
 
@@ -328,14 +347,15 @@ constexpr size_t kHeavySmemLimit = 160u << 10;
 int launch_support(int sm_count, uint32_t support_kernel, uint32_t n, uint64_t m, uint32_t max_dplus,
                    const uint32_t* opos, const uint32_t* ocol, const uint32_t* osrc, int2* es,
                    unsigned long long* spref, unsigned long long* tiles, Counters* cnt, uint32_t* heavy_list,
-                   cudaStream_t s, uint32_t* launches, unsigned long long* support_elements) {
+                   cudaStream_t s, uint32_t* launches, unsigned long long* support_elements,
+                   const uint32_t* mu = nullptr) {
   if (m == 0) return SPARX_OK;
   uint32_t slots = 8;
   while (slots < 2 * max_dplus) slots <<= 1;
   const size_t hsmem = heavy_smem_bytes(slots, max_dplus);
   // auto picks the balanced form: on R-MAT-22 it runs in 131 ms against 221 ms
   // for the vertex form (B200, measured)
-  const bool vertex_form = support_kernel == 2;
+  const bool vertex_form = support_kernel == 2 && !mu;  // multigraph weights: the balanced form only
   if (vertex_form && hsmem <= kHeavySmemLimit) {
     k_support_light<<<sm_count * 8, 256, 0, s>>>(opos, ocol, n, es, &cnt->tri, heavy_list, &cnt->heavy_count,
                                                  &cnt->vcursor);
@@ -347,7 +367,12 @@ int launch_support(int sm_count, uint32_t support_kernel, uint32_t n, uint64_t m
     return SPARX_OK;
   }
   exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, tiles, &cnt->grand, s);
-  k_support_balanced<<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri, &cnt->err);
+  if (mu)
+    k_support_balanced<true><<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri,
+                                                          &cnt->err, mu);
+  else
+    k_support_balanced<false><<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri,
+                                                           &cnt->err, nullptr);
   *launches += 4;
   CU(cudaMemcpyAsync(support_elements, spref + m, 8, cudaMemcpyDeviceToHost, s));
   return SPARX_OK;
@@ -401,6 +426,8 @@ struct UnionJob {
   uint32_t* support_out = nullptr;  // device u32 per slot (support_only)
   bool clustering = false;          // support_only, then local coefficients (f64 per vertex) into out
   bool kcore = false;               // k-core decomposition: core per vertex into out
+  bool multi = false;               // parallel edges found: rows were deduplicated
+  uint64_t slot_self_loops = 0;     // self-loop slots of the caller's CSR
   uint32_t kc_levels = 0, kc_waves = 0, kc_max = 0;
   double cc_possible = 0, cc_local = 0;
   unsigned long long cc_slots = 0;
@@ -434,6 +461,7 @@ PeelArrays peel_arrays(const Union& U) {
   a.qd1 = U.qd[1];
   a.hub_slot = U.hub_slot;
   a.hub_map = U.hub_map;
+  a.mu = nullptr;
   a.n = U.n;
   return a;
 }
@@ -446,7 +474,7 @@ constexpr int kWavesPerIteration = SPARX_WAVES_PER_ITERATION;
 int build_peel_graph(Engine& E, const UnionJob& J, const PeelArrays& arr) {
   const Layout& L = J.L;
   std::vector<size_t> key = {(size_t)E.ws, L.uni, L.mem, L.st, L.ctl, L.wpref, L.cnt, (size_t)J.members.size(),
-                             (size_t)E.wave_blocks};
+                             (size_t)E.wave_blocks, (size_t)E.wave_blocks_multi};
   // the arrays are baked into the captured kernels' parameters
   static_assert(sizeof(PeelArrays) % sizeof(size_t) == 0, "PeelArrays is keyed word by word");
   const size_t* words = reinterpret_cast<const size_t*>(&arr);
@@ -482,7 +510,10 @@ int build_peel_graph(Engine& E, const UnionJob& J, const PeelArrays& arr) {
   CU(cudaStreamBeginCaptureToGraph(E.capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
   // several waves per loop iteration: a wave that finds the loop stopped does
   // nothing, and the condition is read once per iteration
-  for (int i = 0; i < kWavesPerIteration; ++i) k_wave<<<E.wave_blocks, 256, 0, E.capture>>>(wa);
+  for (int i = 0; i < kWavesPerIteration; ++i) {
+    if (arr.mu) k_wave<true><<<E.wave_blocks_multi, 256, 0, E.capture>>>(wa);
+    else k_wave<false><<<E.wave_blocks, 256, 0, E.capture>>>(wa);
+  }
   cudaGraph_t captured;
   CU(cudaStreamEndCapture(E.capture, &captured));
   cudaGraphExec_t ex;
@@ -522,41 +553,89 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   // -- orientation (Kernel B) --
   const bool hubs_possible = L.hub_cap > 0 && !J.support_only;
   uint32_t* hub_hist = hubs_possible ? at<uint32_t>(E, L.hub_hist) : nullptr;
-  if (hubs_possible) {
-    CU(cudaMemsetAsync(hub_hist, 0, 4 * 34, s));
-    k_hub_hist<<<grid_for(N, 256, E.sm_count * 4), 256, 0, s>>>(J.off, N, hub_hist);
-    J.launches += 1;
-  }
-  // rows orientation and compaction give a block each (listed by original degree)
   uint32_t* big = at<uint32_t>(E, L.big);
-  CU(cudaMemsetAsync(&cnt->big_count, 0, 4, s));
-  k_big_rows<<<grid_for(N, 256, E.sm_count * 8), 256, 0, s>>>(J.off, N, big, &cnt->big_count);
-  k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus, big,
-                                       &cnt->big_count);
-  J.launches += 1;
-  exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
-  J.launches += 4;
-  CU(cudaMemcpyAsync(dmem, J.members.data(), sizeof(Member) * G, cudaMemcpyHostToDevice, s));
-  k_member_edges<<<grid_for(G, 256, 1024), 256, 0, s>>>(dmem, G, opos);
-  J.launches += 1;
-  CU(cudaMemcpyAsync(J.members.data(), dmem, sizeof(Member) * G, cudaMemcpyDeviceToHost, s));
+  // multigraphs: deduplicated rows, copies per slot, caller slot -> slot and
+  // multiplicity per edge id (in the second workspace), filled by pass 0
+  uint64_t Ws = W;                      // slots of the rows the pipeline runs on
+  uint32_t* mult2 = nullptr;
+  uint32_t* smap = nullptr;
+  uint32_t* mu = nullptr;
   Counters hc;
-  CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   uint32_t m32 = 0;
-  CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
   uint32_t hist[34] = {};
-  if (hubs_possible) CU(cudaMemcpyAsync(hist, hub_hist, 4 * 33, cudaMemcpyDeviceToHost, s));
-  CU(cudaStreamSynchronize(s));
+  for (int pass = 0;; ++pass) {
+    if (hubs_possible) {
+      CU(cudaMemsetAsync(hub_hist, 0, 4 * 34, s));
+      k_hub_hist<<<grid_for(N, 256, E.sm_count * 4), 256, 0, s>>>(J.off, N, hub_hist);
+      J.launches += 1;
+    }
+    // rows orientation and compaction give a block each (listed by original degree)
+    CU(cudaMemsetAsync(&cnt->big_count, 0, 4, s));
+    k_big_rows<<<grid_for(N, 256, E.sm_count * 8), 256, 0, s>>>(J.off, N, big, &cnt->big_count);
+    k_orient_count<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus, &cnt->self_loops, err, &cnt->max_dplus, big,
+                                         &cnt->big_count);
+    J.launches += 1;
+    exclusive_scan<uint32_t>(LoadU32{dplus}, N, opos, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
+    J.launches += 4;
+    CU(cudaMemcpyAsync(dmem, J.members.data(), sizeof(Member) * G, cudaMemcpyHostToDevice, s));
+    k_member_edges<<<grid_for(G, 256, 1024), 256, 0, s>>>(dmem, G, opos);
+    J.launches += 1;
+    CU(cudaMemcpyAsync(J.members.data(), dmem, sizeof(Member) * G, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
+    if (hubs_possible) CU(cudaMemcpyAsync(hist, hub_hist, 4 * 33, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (pass == 0) J.slot_self_loops = hc.self_loops;
+    if (pass > 0 || hc.err != kErrMulti) break;
+    // parallel edges and no other defect: reduce every row to its distinct
+    // neighbours (copies per slot, caller slot -> slot), then orient again
+    J.multi = true;
+    const uint64_t Mx = std::max<uint64_t>(W / 2, 1);
+    const size_t o_off = 0, o_nbr = align_up(4 * (N + 1)), o_mult = o_nbr + align_up(4 * W),
+                 o_smap = o_mult + align_up(4 * W), o_mu = o_smap + align_up(4 * W), total = o_mu + align_up(4 * Mx);
+    int rc = ensure_ws2(E, total);
+    if (rc) return rc;
+    uint32_t* off2 = (uint32_t*)(E.ws2 + o_off);
+    uint32_t* nbr2 = (uint32_t*)(E.ws2 + o_nbr);
+    mult2 = (uint32_t*)(E.ws2 + o_mult);
+    smap = (uint32_t*)(E.ws2 + o_smap);
+    mu = (uint32_t*)(E.ws2 + o_mu);
+    const int wgrid = grid_for(32ull * N, 256, E.sm_count * 16);  // a warp per row
+    k_dedupe_count<<<wgrid, 256, 0, s>>>(J.off, J.nbr, N, dplus);
+    exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
+    CU(cudaMemsetAsync(mult2, 0, 4 * std::max<uint64_t>(W, 1), s));
+    CU(cudaMemsetAsync(err, 0, 4, s));
+    CU(cudaMemsetAsync(&cnt->self_loops, 0, 8, s));
+    CU(cudaMemsetAsync(&cnt->max_dplus, 0, 4, s));
+    k_dedupe_fill<<<wgrid, 256, 0, s>>>(J.off, J.nbr, N, off2, nbr2, mult2, smap, err);
+    J.launches += 6;
+    uint32_t ws32 = 0;
+    CU(cudaMemcpyAsync(&ws32, off2 + N, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    Ws = ws32;
+    J.off = off2;
+    J.nbr = nbr2;
+  }
   J.self_loops = hc.self_loops;
   if (hc.err) { J.err = hc.err; return status_from_flags(hc.err); }
   const uint64_t m = m32;
-  if (2 * m + hc.self_loops != W) { J.err = kErrAsym; return SPARX_E_INVALID_CSR; }
+  if (2 * m + hc.self_loops != Ws) { J.err = kErrAsym; return SPARX_E_INVALID_CSR; }
   for (const Member& M : J.members)
     if (M.m > kEidMask) { set_error("a graph has >= 2^28 edges"); return SPARX_E_TOO_LARGE; }
   {
     uint32_t* owner = at<uint32_t>(E, L.q0);  // in-slot owners; the q buffers are idle until the peel
     k_orient_fill<<<vgrid, 256, 0, s>>>(J.off, J.nbr, N, opos, ocol, osrc, row0, owner, big, &cnt->big_count);
-    k_orient_reverse<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(J.nbr, owner, W, opos, ocol, row0, err);
+    k_orient_reverse<<<grid_for(Ws, 256, E.sm_count * 16), 256, 0, s>>>(J.nbr, owner, Ws, opos, ocol, row0, err);
+    if (J.multi) {
+      // multiplicity per edge id from its out-slot; the in-slot must agree
+      k_mult_out<<<grid_for(Ws, 256, E.sm_count * 16), 256, 0, s>>>(row0, owner, mult2, Ws, mu);
+      k_mult_check<<<grid_for(Ws, 256, E.sm_count * 16), 256, 0, s>>>(row0, owner, mult2, Ws, mu, err);
+      J.launches += 2;
+      uint32_t* herr = (uint32_t*)E.pinned_small;
+      CU(cudaMemcpyAsync(herr, err, 4, cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+      if (*herr) { J.err = *herr; return status_from_flags(*herr); }
+    }
   }
   J.launches += 2;
   // hub maps: the smallest power-of-two degree bound (>= kHubMinDegree) whose
@@ -595,20 +674,20 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   {
     int rc = launch_support(E.sm_count, O.support_kernel, N, m, hc.max_dplus, opos, ocol, osrc, es,
                             at<unsigned long long>(E, L.q0), at<unsigned long long>(E, L.tiles), cnt,
-                            at<uint32_t>(E, L.act0), s, &J.launches, &J.support_elements);
+                            at<uint32_t>(E, L.act0), s, &J.launches, &J.support_elements, mu);
     if (rc) return rc;
   }
   CU(cudaEventRecord(E.tev[3], s));
 
   if (J.support_only && J.clustering) {
     k_clustering<<<vgrid, 256, 0, s>>>(J.off, row0, es, N, O.support_mode == SPARX_SUPPORT_U8, (double*)J.out,
-                                       &cnt->cc_possible, &cnt->cc_local, &cnt->cc_slots);
+                                       &cnt->cc_possible, &cnt->cc_local, &cnt->cc_slots, mult2);
     J.launches += 1;
     CU(cudaEventRecord(E.tev[4], s));
     CU(cudaEventRecord(E.tev[5], s));
   } else if (J.support_only) {
     k_support_slots<<<grid_for(W, 256, E.sm_count * 16), 256, 0, s>>>(row0, es, W, J.support_out,
-                                                                       O.support_mode == SPARX_SUPPORT_U8);
+                                                                       O.support_mode == SPARX_SUPPORT_U8, smap);
     J.launches += 1;
     CU(cudaEventRecord(E.tev[4], s));
     CU(cudaEventRecord(E.tev[5], s));
@@ -640,7 +719,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     c0.G = G;
     c0.max_waves = 3ull * m + 64;  // each frontier wave processes >= 1 edge; <= 2 scans per level
     c0.timeout_ns = O.timeout_ms * 1000000ull;
-    c0.csr_slots = W;
+    c0.csr_slots = Ws;
     c0.compact_min = kCompactMinSlots;
     // wave trace: when SPARX_TRACE_FILE names a file, the planner records
     // each wave's start time and work there (first 2^20 waves)
@@ -655,7 +734,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       k_peel_setup<<<grid_for(m, 256, E.sm_count * 8), 256, 0, s>>>(at<Union>(E, L.uni), dmem,
                                                                      O.support_mode == SPARX_SUPPORT_U8,
                                                                      at<unsigned long long>(E, L.mem_tri),
-                                                                     at<uint32_t>(E, L.mem_maxsup));
+                                                                     at<uint32_t>(E, L.mem_maxsup), mu, err);
     k_peel_init<<<1, 1024, 0, s>>>(dmem, at<MemberState>(E, L.st), at<Control>(E, L.ctl),
                                    at<unsigned long long>(E, L.wpref), G);
     J.launches += m > 0 ? 2 : 1;
@@ -663,6 +742,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     WaveArgs wa;
     wa.Up = at<Union>(E, L.uni);
     wa.arr = peel_arrays(U);
+    wa.arr.mu = mu;
     wa.mem = dmem;
     wa.st = at<MemberState>(E, L.st);
     wa.ctl = at<Control>(E, L.ctl);
@@ -683,7 +763,10 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
         CU(cudaStreamSynchronize(s));
       } else {
         for (;;) {
-          for (int i = 0; i < 16; ++i) k_wave<<<E.wave_blocks, 256, 0, s>>>(wa);
+          for (int i = 0; i < 16; ++i) {
+            if (mu) k_wave<true><<<E.wave_blocks_multi, 256, 0, s>>>(wa);
+            else k_wave<false><<<E.wave_blocks, 256, 0, s>>>(wa);
+          }
           J.launches += 16;
           CU(cudaMemcpyAsync(hctl, wa.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
           CU(cudaStreamSynchronize(s));
@@ -717,9 +800,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     const int u8 = O.support_mode == SPARX_SUPPORT_U8;
     if (W > 0) {
       if (O.out_bits == 8)
-        k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(row0, es, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err);
+        k_finalize<uint8_t><<<fgrid, 256, 0, s>>>(row0, es, W, (uint8_t*)J.out, u8, 1, &cnt->kmax, err, smap);
       else
-        k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(row0, es, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err);
+        k_finalize<uint32_t><<<fgrid, 256, 0, s>>>(row0, es, W, (uint32_t*)J.out, u8, 0, &cnt->kmax, err, smap);
       J.launches += 1;
     }
   }
@@ -772,7 +855,10 @@ void fill_stats(const UnionJob& J, uint32_t g, sparx_pkt_stats* st) {
   st->n = M.n;
   st->width = M.w;
   st->m = M.m;
-  st->self_loops = M.w - 2ull * M.m;
+  // a multigraph's width also counts parallel copies: its self-loop slots were
+  // counted before the rows were deduplicated (for a lone graph; not split per
+  // member in a batch)
+  st->self_loops = !J.multi ? M.w - 2ull * M.m : J.members.size() == 1 ? J.slot_self_loops : 0;
   if (g < J.mem_tri.size()) st->triangles = J.mem_tri[g] / 3;
   if (g < J.mem_maxsup.size()) st->max_support = J.mem_maxsup[g];
   if (g < J.states.size() && !J.support_only) {  // support-only runs have no peel state
@@ -1282,6 +1368,7 @@ void engine_release(Engine* E) {
   if (E->stream) cudaStreamSynchronize(E->stream);
   if (E->peel.exec) { cudaGraphExecDestroy(E->peel.exec); cudaGraphDestroy(E->peel.graph); }
   if (E->ws) cudaFree(E->ws);
+  if (E->ws2) cudaFree(E->ws2);
   if (E->trace) cudaFree(E->trace);
   for (int i = 0; i < 2; ++i) {
     if (E->pinned[i]) cudaFreeHost(E->pinned[i]);
@@ -1773,7 +1860,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   uint32_t* err = &cnt->err;
   int sm = 148, per_sm = 1;
   CU(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device));
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave, 256, 0));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave<false>, 256, 0));
   const int wave_blocks = std::max(1, per_sm) * sm;
   const uint32_t N = (uint32_t)n;
 
@@ -1866,7 +1953,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   CU(cudaMemsetAsync(P(L.mem_maxsup), 0, 4, s));
   if (m > 0)
     k_peel_setup<<<grid_for(m, 256, sm * 8), 256, 0, s>>>(dU, dM, 0, (unsigned long long*)P(L.mem_tri),
-                                                           (uint32_t*)P(L.mem_maxsup));
+                                                           (uint32_t*)P(L.mem_maxsup), nullptr, err);
   k_peel_init<<<1, 1024, 0, s>>>(dM, dS, dC, wpref, 1);
   WaveArgs wa;
   wa.Up = dU;
@@ -1879,14 +1966,15 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   wa.handle = cudaGraphConditionalHandle{};
   wa.use_handle = 0;
   for (;;) {
-    for (int i = 0; i < 16; ++i) k_wave<<<wave_blocks, 256, 0, s>>>(wa);
+    for (int i = 0; i < 16; ++i) k_wave<false><<<wave_blocks, 256, 0, s>>>(wa);
     uint32_t done = 0;
     CU(cudaMemcpyAsync(&done, &dC->done, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     if (done) break;
   }
   if (width)
-    k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(row0, es, width, d_out, 0, 0, &cnt->kmax, err);
+    k_finalize<uint32_t><<<grid_for(width, 256, sm * 16), 256, 0, s>>>(row0, es, width, d_out, 0, 0, &cnt->kmax, err,
+                                                                       nullptr);
   CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   drain.armed = false;

@@ -189,3 +189,45 @@ def from_edges(n: int, edges, bits: int = 32) -> Csr:
 
 def log_uniform_mean(lo: float, hi: float) -> float:
     return (hi - lo) / math.log(hi / lo)
+
+
+def from_multi_edges(n: int, edges, bits: int = 32) -> Csr:
+    """Symmetric multigraph CSR from an undirected edge list in which repeats
+    are parallel edges: every (u, v), u != v, adds slot v to row u and slot u to
+    row v; a self-loop (u, u) adds one slot u to row u (its own reciprocal, as
+    in the reference's edge index).  Rows sorted ascending, copies side by side
+    (the layout the reference's GGCAT cache gives parallel edges)."""
+    rows = [[] for _ in range(n)]
+    for u, v in edges:
+        rows[u].append(v)
+        if u != v:
+            rows[v].append(u)
+    off = np.zeros(n + 1, dtype=np.uint64)
+    nbr = []
+    for u in range(n):
+        r = sorted(rows[u])
+        nbr.extend(r)
+        off[u + 1] = off[u] + len(r)
+    return Csr(off, np.asarray(nbr, dtype=np.uint32 if bits == 32 else np.uint64), "multi-edges")
+
+
+def with_parallel_edges(g: Csr, frac: float, max_extra: int = 2, seed: int = 0) -> Csr:
+    """A multigraph from a simple graph: each undirected edge (self-loops
+    excepted) gets, with probability ``frac``, between 1 and ``max_extra``
+    extra copies (seeded), added to both of its rows."""
+    rng = np.random.default_rng(seed)
+    off = g.offsets.astype(np.int64)
+    nbr = g.neighbours.astype(np.int64)
+    src = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(off))
+    up = src < nbr
+    a, b = src[up], nbr[up]
+    extra = np.where(rng.random(a.shape[0]) < frac, rng.integers(1, max_extra + 1, a.shape[0]), 0)
+    ea, eb = np.repeat(a, extra), np.repeat(b, extra)
+    rs = np.concatenate([src, ea, eb])
+    cs = np.concatenate([nbr, eb, ea])
+    order = np.lexsort((cs, rs))
+    rs, cs = rs[order], cs[order]
+    new_off = np.zeros(g.n + 1, dtype=np.uint64)
+    np.cumsum(np.bincount(rs, minlength=g.n), out=new_off[1:])
+    return Csr(new_off, cs.astype(np.uint32 if g.neighbours.dtype == np.uint32 else np.uint64),
+               f"{g.name}-parallel{frac}")

@@ -50,6 +50,23 @@ def random_graph(rng, n_max=40, self_loop_p=0.2):
     return gen.from_edges(n, edges)
 
 
+def random_multigraph(rng, n_max=30):
+    """A random graph whose edges repeat (parallel copies, up to four of a pair) and
+    which may carry repeated self-loops."""
+    from sparkx_b200 import gen
+    n = int(rng.integers(2, n_max))
+    p = rng.uniform(0.05, 0.8)
+    edges = []
+    for i in range(n):
+        for j in range(i + 1, n):
+            if rng.random() < p:
+                edges += [(i, j)] * int(rng.choice([1, 1, 1, 2, 3, 4]))
+    for _ in range(int(rng.integers(0, 3))):
+        v = int(rng.integers(0, n))
+        edges += [(v, v)] * int(rng.integers(1, 3))
+    return gen.from_multi_edges(n, edges)
+
+
 # Hand-derived known answers: (name, n, edges, expected truss per undirected edge)
 def kats():
     out = []

@@ -3,7 +3,7 @@ known answers, a brute-force definition and each other."""
 import numpy as np
 import pytest
 
-from conftest import book, expected_truss, kats, kn, random_graph
+from conftest import random_multigraph, book, expected_truss, kats, kn, random_graph
 from oracle import oracle as O
 from sparkx_b200 import gen
 
@@ -251,3 +251,74 @@ def test_kcore_matches_definition():
     for _ in range(60):
         g = random_graph(rng, self_loop_p=0.0)
         assert np.array_equal(O.kcore(g.offsets, g.neighbours), _core_definition(g))
+
+
+# ---- multigraphs (the reference's OneOrMany paths) -------------------------------------
+
+def test_multigraph_known_answers():
+    # a triangle whose edge (0, 1) is doubled: two triangles of copies; a copy of (0, 1) lies in
+    # one, (1, 2) and (0, 2) in two each -> every edge is in the 3-truss, none in the 4-truss
+    g = gen.from_multi_edges(3, [(0, 1), (0, 1), (1, 2), (0, 2)])
+    assert np.array_equal(O.triangles(g.offsets, g.neighbours), [1, 1, 2, 1, 1, 2, 2, 2])
+    for f in (O.pkt, O.burkhardt, lambda o, n: O.fast_truss(o, n)[0], O.brute_force_truss):
+        assert np.array_equal(f(g.offsets, g.neighbours), np.full(8, 3))
+    # every pair doubled: each copy lies in 2 * 2 = 4 triangles -> the 6-truss
+    g = gen.from_multi_edges(3, [(0, 1), (1, 2), (0, 2)] * 2)
+    for f in (O.pkt, O.burkhardt, lambda o, n: O.fast_truss(o, n)[0], O.brute_force_truss):
+        assert np.array_equal(f(g.offsets, g.neighbours), np.full(12, 6))
+    # parallel self-loops: truss 2 each, their own reciprocals
+    g = gen.from_multi_edges(3, [(0, 1), (1, 2), (0, 2), (1, 1), (1, 1)])
+    _, er = O.edge_index(g.offsets, g.neighbours)
+    loops = [s for s in range(g.width) if g.neighbours[s] == 1 and 2 <= s < 6]
+    assert all(er[s] == s for s in loops) and len(loops) == 2
+    t = O.pkt(g.offsets, g.neighbours)
+    assert all(t[s] == 2 for s in loops)
+    assert O.verify(g.offsets, g.neighbours, t) == -1
+
+
+def test_multigraph_edge_index_pairs_copies():
+    rng = np.random.default_rng(31)
+    for _ in range(40):
+        g = random_multigraph(rng)
+        eo, er = O.edge_index(g.offsets, g.neighbours, threads=3)
+        off = g.offsets.astype(np.int64)
+        row = np.repeat(np.arange(g.n), np.diff(off))
+        er = er.astype(np.int64)
+        assert np.array_equal(er[er], np.arange(g.width))            # an involution
+        assert np.array_equal(row[er], g.neighbours.astype(np.int64))  # joins a copy of the same pair
+        assert np.array_equal(g.neighbours[er].astype(np.int64), row)
+
+
+def test_multigraph_restatements_agree_with_definition():
+    rng = np.random.default_rng(32)
+    for i in range(60):
+        g = random_multigraph(rng)
+        want_sup = O.support_definition(g.offsets, g.neighbours)
+        assert np.array_equal(O.triangles(g.offsets, g.neighbours, hash_map=bool(i & 1)), want_sup)
+        want = O.brute_force_truss(g.offsets, g.neighbours)
+        assert np.array_equal(O.pkt(g.offsets, g.neighbours, threads=1 + i % 4, hash_map=bool(i & 1)), want)
+        assert np.array_equal(O.burkhardt(g.offsets, g.neighbours, hash_map=bool(i & 2)), want)
+        t, tri, _ = O.fast_truss(g.offsets, g.neighbours, threads=2)
+        assert np.array_equal(t, want)
+        assert tri * 6 == int(want_sup.sum())
+        assert O.verify(g.offsets, g.neighbours, want) == -1
+
+
+def test_multigraph_verifier_rejects_wrong_assignments():
+    g = gen.from_multi_edges(4, [(0, 1), (0, 1), (1, 2), (0, 2), (2, 3), (1, 3)])
+    t = O.brute_force_truss(g.offsets, g.neighbours)
+    assert O.verify(g.offsets, g.neighbours, t) == -1
+    for s in range(g.width):
+        if g.neighbours[s] == s:
+            continue
+        bad = t.copy()
+        bad[s] += 1
+        assert O.verify(g.offsets, g.neighbours, bad) >= 0
+
+
+def test_multigraph_larger_graphs_pkt_equals_fast_peel():
+    for seed, frac in ((1, 0.2), (2, 0.5)):
+        g = gen.with_parallel_edges(gen.rmat(11, 8, seed=seed), frac, max_extra=3, seed=seed)
+        want = O.fast_truss(g.offsets, g.neighbours)[0]
+        assert np.array_equal(O.pkt(g.offsets, g.neighbours, threads=4), want)
+        assert O.verify(g.offsets, g.neighbours, want, threads=4) == -1
