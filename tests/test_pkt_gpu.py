@@ -282,3 +282,15 @@ def test_support_kernel_forms_agree(kernel):
         assert np.array_equal(sup, ref)
         t, _ = run_pkt(g.offsets, g.neighbours, PktOptions(out_bits=32, support_kernel=kernel))
         assert np.array_equal(t, O.pkt(g.offsets, g.neighbours, threads=4))
+
+
+def test_sharded_batch_single_rank_uses_the_engine():
+    """shard.run_sharded_batch without a process group: one rank, the CUDA batch call, the
+    same results as the oracle (the gloo tests cover placement and the gather on CPU)."""
+    from sparkx_b200 import shard
+    gs = [gen.rmat(10, 8, seed=s) for s in range(3)] + [gen.erdos_renyi(5000, 30000, 9)]
+    out = shard.run_sharded_batch([shard.work_estimate(g.n, g.width) for g in gs],
+                                  lambda i: (gs[i].offsets, gs[i].neighbours), opts=O32)
+    assert out.parts == [[0, 1, 2, 3]]
+    for g, (t, st, status) in zip(gs, out.results):
+        assert status == 0 and np.array_equal(t, O.pkt(g.offsets, g.neighbours))
