@@ -15,7 +15,10 @@ truss per CSR slot) of the workload graph.  Prints ONE JSON line on rank 0.
          workload family.
 
 Multi-GPU: a single graph does not shard (PKT's sub-level barrier would need a
-cross-GPU exchange per sub-level), so N ranks run N replicas (weak scaling).
+cross-GPU exchange per sub-level), so for the R-MAT-22 workload N ranks run N
+replicas (weak scaling).  Independent graphs do shard: --workload mix places
+the batched mix's members on the ranks (LPT) and each rank decomposes its own
+through shard.run_sharded_batch.
 """
 from __future__ import annotations
 
@@ -134,56 +137,97 @@ def cpu_pkt_sample(threads: int):
     return g.width / dt, dt, sample
 
 
-def run_mix(args):
-    """Config 4: a sample of the batched mix, batched vs one decomposition per call."""
-    import torch  # noqa: F401  (initialises the device first)
-    from sparkx_b200 import gen
-    from sparkx_b200.pkt import PktOptions, run_batch, run_pkt
-    t0 = time.perf_counter()
+def run_mix(args, rank=0, world=1, local=0):
+    """Config 4: the batched mix, batched (one union per HBM budget, one launch per wave) vs one
+    decomposition per call, in chunks of --mix-chunk members (bounded host memory).  Both arms
+    decompose the same graphs and every member's truss numbers must agree.  With --autotune the
+    knobs are first tuned on a sample of the mix (both arms then use the cache).  Under torchrun
+    (N ranks) the members are placed with LPT and each rank generates and decomposes its own
+    (shard.run_sharded_batch); times are the slowest rank's."""
+    import torch
+    from sparkx_b200 import gen, shard
+    from sparkx_b200.pkt import PktOptions, autotune_batch, run_batch, run_pkt
+    torch.cuda.set_device(local)
+    opts = PktOptions(out_bits=32, device=local)
     members = [gen.mix_member(i) for i in range(args.mix_count)]
-    graphs = [gen.mix_graph(m) for m in members]
-    log(f"mix: {len(graphs)} graphs, {sum(g.width for g in graphs)} slots, generated in "
-        f"{time.perf_counter() - t0:.1f}s")
-    opts = PktOptions(out_bits=32)
-    pairs = [(g.offsets, g.neighbours) for g in graphs]
-    run_batch(pairs[: min(8, len(pairs))], opts)  # warm-up
-    run_pkt(*pairs[0], opts)
-    tb = []
-    for _ in range(args.steps):
-        t1 = time.perf_counter()
-        res = run_batch(pairs, opts)
-        tb.append(time.perf_counter() - t1)
-    assert all(r[2] == 0 for r in res)
-    tp = []
-    for _ in range(max(1, args.steps // 2)):
-        t1 = time.perf_counter()
-        solo = [run_pkt(o, n, opts)[0] for o, n in pairs]
-        tp.append(time.perf_counter() - t1)
-    same = all(np.array_equal(r[0], s) for r, s in zip(res, solo))
-    small = [i for i, g in enumerate(graphs) if g.n < 10_000]
-    tps = []
-    if small:
-        sp = [pairs[i] for i in small]
-        t1 = time.perf_counter()
-        run_batch(sp, opts)
-        tb_small = time.perf_counter() - t1
-        t1 = time.perf_counter()
-        for o, n in sp:
-            run_pkt(o, n, opts)
-        tps = [tb_small, time.perf_counter() - t1]
-    b = statistics.median(tb)
-    p = statistics.median(tp)
-    out = {"metric": "PKT batched mix graphs/s", "value": len(graphs) / b, "unit": "graphs/s",
-           "per_graph_value": len(graphs) / p, "batched_speedup": p / b, "n_graphs": len(graphs),
-           "slots": sum(g.width for g in graphs), "same_results_as_per_graph": same,
-           "edges_per_s_batched": sum(g.width for g in graphs) / b,
-           "small_graphs": {"count": len(small), "batched_graphs_per_s": len(small) / tps[0] if tps else None,
-                            "per_graph_graphs_per_s": len(small) / tps[1] if tps else None,
-                            "speedup": tps[1] / tps[0] if tps else None},
-           "config": {"workload": f"first {len(graphs)} members of the batched mix (config 4 distribution: "
-                                  "ER or R-MAT, n log-uniform in [1e3,1e6], avg degree uniform [4,64], "
-                                  "seeds 1000+i)"}}
-    print(json.dumps(out), flush=True)
+    works = [shard.work_estimate(m.n, 2 * m.pairs) for m in members]
+    mine = shard.assign_lpt(works, world)[rank]
+    tuned = None
+    if args.autotune:
+        sample = [gen.mix_graph(members[i]) for i in mine[: min(24, len(mine))]]
+        tuned = autotune_batch([(g.offsets, g.neighbours) for g in sample], opts, repeats=2)
+        log(f"rank {rank}: autotuned {tuned}")
+    warm = gen.mix_graph(members[mine[0]])
+    run_batch([(warm.offsets, warm.neighbours)], opts)
+    run_pkt(warm.offsets, warm.neighbours, opts)
+    t_gen = t_batch = t_plain = dev_plain = dev_batch_union = 0.0
+    slots = n_done = 0
+    same = True
+    small = {"batch": 0.0, "plain": 0.0, "count": 0}
+    step = args.mix_chunk * world
+    for c0 in range(0, len(members), step):
+        chunk = list(range(c0, min(c0 + step, len(members))))
+        loaded = {}
+
+        def load(j):  # j indexes the chunk; each rank builds only the graphs placed on it
+            t1 = time.perf_counter()
+            g = gen.mix_graph(members[chunk[j]])
+            loaded[j] = g
+            nonlocal_t[0] += time.perf_counter() - t1
+            return g.offsets, g.neighbours
+
+        nonlocal_t = [0.0]
+        out = shard.run_sharded_batch([works[i] for i in chunk], load, opts=opts, gather=False)
+        t_gen += nonlocal_t[0]
+        t_batch += out.seconds  # slowest rank's time for this chunk
+        res = out.local
+        assert all(r[2] == 0 for r in res.values()), [r[2] for r in res.values() if r[2]]
+        seen = set()
+        for r in res.values():  # members of a union share its phases: count each union once
+            key = (r[1].ms_orient, r[1].ms_support, r[1].ms_peel)
+            if key not in seen:
+                seen.add(key)
+                dev_batch_union += (r[1].ms_orient + r[1].ms_support + r[1].ms_peel + r[1].ms_finalize) / 1e3
+        t_plain_chunk = 0.0
+        for j, r in sorted(res.items()):
+            g = loaded[j]
+            t1 = time.perf_counter()
+            t, st = run_pkt(g.offsets, g.neighbours, opts)
+            dt = time.perf_counter() - t1
+            t_plain_chunk += dt
+            dev_plain += (st.ms_orient + st.ms_support + st.ms_peel + st.ms_finalize) / 1e3
+            same &= bool(np.array_equal(t, r[0]))
+            if g.n < 10_000:
+                small["plain"] += dt
+                small["count"] += 1
+        t_plain += shard.max_over_ranks(t_plain_chunk, torch.device("cuda", local))
+        sp = [(loaded[j].offsets, loaded[j].neighbours) for j in sorted(loaded) if loaded[j].n < 10_000]
+        if sp:
+            t1 = time.perf_counter()
+            run_batch(sp, opts)
+            small["batch"] += time.perf_counter() - t1
+        slots += sum(g.width for g in loaded.values())
+        n_done += len(loaded)
+        log(f"rank {rank}: {n_done} members, batch {t_batch:.1f}s plain {t_plain:.1f}s gen {t_gen:.1f}s")
+        del loaded, res, out
+    same = shard.max_over_ranks(0.0 if same else 1.0, torch.device("cuda", local)) == 0.0
+    if rank == 0:
+        out = {"metric": "PKT batched mix graphs/s", "value": args.mix_count / t_batch, "unit": "graphs/s",
+               "n_gpus": world, "per_graph_value": args.mix_count / t_plain, "batched_speedup": t_plain / t_batch,
+               "n_graphs": args.mix_count, "slots_rank0": slots, "same_results_as_per_graph": same,
+               "edges_per_s_batched_rank0": slots / t_batch,
+               "device_seconds_rank0": {"per_graph_sum": dev_plain, "batched_unions_sum": dev_batch_union},
+               "wall_seconds": {"batched": t_batch, "per_graph": t_plain, "generation_rank0": t_gen},
+               "small_graphs_rank0": {"count": small["count"],
+                                      "speedup": small["plain"] / small["batch"] if small["batch"] else None},
+               "autotuned": None if tuned is None else {"tuning": tuned[0].__dict__, "key": list(tuned[1])},
+               "config": {"workload": f"batched mix, members 0..{args.mix_count - 1} (config 4 distribution: "
+                                      "ER or R-MAT 50/50, n log-uniform in [1e3,1e6], avg degree uniform [4,64], "
+                                      "seeds 1000+i)", "chunk": args.mix_chunk,
+                          "parallelism": f"LPT shards x{world}", "timing": "host wall clock per call "
+                          "(the batch API is host-synchronous: uploads, decompositions and downloads), "
+                          "max over ranks"}}
+        print(json.dumps(out), flush=True)
     return 0
 
 
@@ -287,6 +331,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["mix", "serve"], default="rmat22")
     ap.add_argument("--mix-count", type=int, default=256)
+    ap.add_argument("--mix-chunk", type=int, default=256, help="mix: members generated and run per chunk")
+    ap.add_argument("--autotune", action="store_true", help="mix: tune the knobs on a sample first")
     ap.add_argument("--rates", type=float, nargs="*", default=[50.0, 200.0, 1000.0])
     ap.add_argument("--tail", action="store_true", help="serve: add the 1% R-MAT-24 tail")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -305,6 +351,17 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload == "mix":
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            try:
+                return run_mix(args, rank, world, local)
+            finally:
+                dist.barrier()
+                dist.destroy_process_group()
         return run_mix(args)
     if args.workload == "serve":
         return run_serve(args)

@@ -199,6 +199,52 @@ int sparx_pkt_run_device_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1,
                                  const uint32_t* d_neighbours, uint64_t width, uint32_t* d_truss_out,
                                  int device, void* cuda_stream);
 
+/* ---- tuning ------------------------------------------------------------ */
+/*
+ * Performance knobs of the engine (no counterpart in the reference, whose
+ * only knob is its thread count).  None changes a result.  Each launch
+ * picks them from a cache keyed on the degree signature of the rows it runs
+ * on: key = {floor(log2(slots)), floor(log2(max degree)) + 1, eighths of the
+ * slots that lie in rows of degree >= 256}; a key without an entry uses the
+ * defaults below.  sparx_autotune fills the cache by measuring candidates on a
+ * sample graph; the file named by the environment variable SPARX_TUNE_FILE is
+ * read on first use and rewritten by each autotune.  An explicit
+ * opts->support_kernel (1 or 2) overrides the tuned support form.
+ */
+typedef struct sparx_tuning {
+  uint32_t struct_size;     /* sizeof(sparx_tuning) */
+  uint32_t merge_ratio;     /* peel: merge the two rows when the longer is <= this x the shorter (8) */
+  uint32_t hub_min_degree;  /* dense neighbour -> edge maps for vertices of at least this degree,
+                               >= 256, or 0 for none (1024) */
+  uint32_t sample_min;      /* support: longer out-lists of at least this length are narrowed
+                               through 64 samples before the search (64) */
+  uint32_t support_kernel;  /* 1 balanced edge form, 2 vertex form (1) */
+  uint32_t compact_pct;     /* peel: rebuild the working rows once live entries fill at most
+                               this percentage of them (85) */
+} sparx_tuning;
+
+int sparx_tuning_default(sparx_tuning* t);
+/* The key of a host CSR (its offsets only). */
+int sparx_tuning_signature(const uint64_t* offsets, uint64_t n_plus_1, uint32_t key[3]);
+/* Cached knobs for a key (*found = 0: the defaults are returned). */
+int sparx_tuning_lookup(const uint32_t key[3], sparx_tuning* out, int* found);
+int sparx_tuning_store(const uint32_t key[3], const sparx_tuning* t);
+int sparx_tuning_clear(void);
+/* Knobs and key of the last launch on this thread. */
+int sparx_tuning_last(sparx_tuning* used, uint32_t key[3]);
+int sparx_tuning_save(const char* path);
+int sparx_tuning_load(const char* path);
+
+/*
+ * Autotune on one sample graph (host, the reference's layout): coordinate
+ * descent from the defaults over the support form and sampling threshold
+ * (timed by the support pass), then the hub floor, merge ratio and compaction
+ * fill (timed by orientation + peel); `repeats` decompositions per candidate
+ * (median).  Stores the winner under the sample's key and returns it.
+ */
+int sparx_autotune(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
+                   const sparx_pkt_opts* opts, uint32_t repeats, sparx_tuning* best, uint32_t key[3]);
+
 /* ---- batched decomposition -------------------------------------------- */
 /* One member of a batch: host arrays in the reference's layout (u64 ids) or
  * u32 ids (neighbour_bits 32).  truss_out follows opts->out_bits. */
@@ -221,6 +267,15 @@ typedef struct sparx_graph_view {
  */
 int sparx_pkt_run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
                         const sparx_pkt_opts* opts, int* status_out, sparx_pkt_stats* stats_out);
+
+/*
+ * Autotune a batch: the candidates run over the whole batch and are timed on
+ * its first union (whose key receives the winner); pass a representative
+ * sample that fits one union under the budget.  Results are written to the
+ * members' truss_out (every candidate gives the same numbers).
+ */
+int sparx_autotune_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
+                         const sparx_pkt_opts* opts, uint32_t repeats, sparx_tuning* best, uint32_t key[3]);
 
 /* ---- serving: continuous batching ------------------------------------ */
 typedef struct sparx_server sparx_server;

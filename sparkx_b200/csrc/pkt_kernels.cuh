@@ -69,7 +69,9 @@ struct Union {  // the prepared concatenated graph, as the peel sees it
   unsigned long long* q[2];
   uint4* qd[2];                    // per queue entry {short row start, length, long row begin, end}
   const uint32_t* hub_slot;        // vertex -> hub map index or kInvalid; nullptr = no hub maps
-  const uint32_t* hub_map;         // hub k's neighbours: hub_map[k * n + id] = edge id or kInvalid
+  const uint32_t* hub_map;         // map pool: hub k's neighbour id w -> hub_map[hub_base[k] + w]
+  const uint32_t* hub_base;        // per hub: its map's start in the pool minus its member's first
+                                   // vertex id (u32 arithmetic, so base + w wraps into the map)
   uint32_t n;
   uint32_t m;
   uint32_t width;
@@ -92,8 +94,10 @@ struct PeelArrays {
   uint4* qd1;
   const uint32_t* hub_slot;
   const uint32_t* hub_map;
-  const uint32_t* mu;  // multigraphs: multiplicity per edge id (nullptr: simple graph)
+  const uint32_t* hub_base;
+  const uint32_t* mu;    // multigraphs: multiplicity per edge id (nullptr: simple graph)
   uint32_t n;
+  uint32_t merge_ratio;  // merge the rows when the longer is at most this many times the shorter
 };
 
 // Field-by-field copy of a device-resident Union into registers (a struct
@@ -112,21 +116,24 @@ struct UnionRegs {
   uint4* qd1;
   const uint32_t* __restrict__ hub_slot;
   const uint32_t* __restrict__ hub_map;
+  const uint32_t* __restrict__ hub_base;
   const uint32_t* __restrict__ mu;
   uint32_t n;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
       : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]),
-        qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), mu(nullptr), n(p->n) {}
+        qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), hub_base(p->hub_base),
+        mu(nullptr), n(p->n) {}
   __device__ __forceinline__ UnionRegs(const Union* p, const PeelArrays& a)
       : off(p->off), row(p->row), ocol(a.ocol), osrc(a.osrc), es(a.es),
         act0(a.act0), act1(a.act1), q0(a.q0), q1(a.q1),
-        qd0(a.qd0), qd1(a.qd1), hub_slot(a.hub_slot), hub_map(a.hub_map), mu(a.mu), n(a.n) {}
+        qd0(a.qd0), qd1(a.qd1), hub_slot(a.hub_slot), hub_map(a.hub_map), hub_base(a.hub_base), mu(a.mu),
+        n(a.n) {}
 };
 
-// A queue-entry descriptor whose longer row belongs to a hub carries
-// kHubDesc | hub index in place of the longer row's begin (row positions stay
-// below 2^31 whenever hub maps are built).
+// A queue-entry descriptor whose longer row belongs to a hub carries kHubDesc
+// in place of the longer row's begin and the hub's map base in place of its
+// end (row positions stay below 2^31 whenever hub maps are built).
 constexpr uint32_t kHubDesc = 0x80000000u;
 
 struct Member {  // static per-member ranges
@@ -166,6 +173,8 @@ struct Control {
   uint32_t exit_reason;           // why the loop stopped: kExit*
   uint32_t blocks_done;           // wave blocks finished (the last one plans the next wave)
   uint32_t compactions;
+  uint32_t compact_pct;           // compact when live entries fill at most this % of the working rows
+  uint32_t pad0;
   unsigned long long merge_iters; // warp iterations resolved by the row merge
   unsigned long long lane_iters;  // warp iterations resolved by per-lane searches
   unsigned long long merge_chunks;// 32-entry chunks of longer rows read by merges
@@ -754,7 +763,7 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
     const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
     const uint32_t* __restrict__ osrc, const unsigned long long* __restrict__ spref, uint32_t m,
     int2* __restrict__ es, unsigned long long* __restrict__ tri_total, uint32_t* __restrict__ err,
-    const uint32_t* __restrict__ mu) {
+    const uint32_t* __restrict__ mu, uint32_t sample_min) {
   const uint32_t lane = lane_id();
   const unsigned long long total = spref[m];
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -827,7 +836,7 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
         // per lane (gathered once per edge, then shuffles), leaving ~1/64 of it
         // to search
         const uint32_t flen = fle - flb;
-        const bool sampled = flen >= kSampledList;
+        const bool sampled = flen >= sample_min;
         const uint32_t smp = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane) * flen) >> 6)) : 0u;
         const uint32_t smp1 = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane + 1) * flen) >> 6)) : 0u;
         do {
@@ -1218,7 +1227,7 @@ struct WaveArgs {
 };
 
 // Rows of frontier edge x in the working CSR: {shorter row start, its length,
-// longer row begin, longer row end}, or {.., .., kHubDesc | hub index, 0} when
+// longer row begin, longer row end}, or {.., .., kHubDesc, hub map base} when
 // the longer row's vertex has a hub map.  The length is the edge's work.
 __device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x) {
   const uint32_t u = __ldg(U.osrc + x), v = __ldg(U.ocol + x);
@@ -1227,7 +1236,10 @@ __device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x) {
   const bool u_short = ue - ub <= ve - vb;
   if (U.hub_slot) {
     const uint32_t hs = __ldg(U.hub_slot + (u_short ? v : u));
-    if (hs != kInvalid) return u_short ? make_uint4(ub, ue - ub, kHubDesc | hs, 0) : make_uint4(vb, ve - vb, kHubDesc | hs, 0);
+    if (hs != kInvalid) {
+      const uint32_t base = __ldg(U.hub_base + hs);
+      return u_short ? make_uint4(ub, ue - ub, kHubDesc, base) : make_uint4(vb, ve - vb, kHubDesc, base);
+    }
   }
   return u_short ? make_uint4(ub, ue - ub, vb, ve) : make_uint4(vb, ve - vb, ub, ue);
 }
@@ -1523,10 +1535,12 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
       if (e) { done = 1; reason = kExitError; }
       if (ctl->waves_run > ctl->max_waves) { atomicOr(err, kErrWaves); done = 1; reason = kExitError; }
       if (globaltimer() - ctl->t_start > ctl->timeout_ns) { atomicOr(err, kErrTimeout); done = 1; reason = kExitError; }
-      // live edges fill at most 85% of the working rows: stop so the host can
-      // compact them (a compaction is a few passes over the rows, which the
-      // shorter rows repay at this fill; 78% and 90% measured slower)
-      if (!done && ctl->csr_slots >= ctl->compact_min && 200 * s_live_edges <= 85 * ctl->csr_slots) {
+      // live edges fill at most compact_pct % of the working rows (85 unless
+      // tuned): stop so the host can compact them (a compaction is a few passes
+      // over the rows, which the shorter rows repay at this fill; 78% and 90%
+      // measured slower on R-MAT-22)
+      if (!done && ctl->csr_slots >= ctl->compact_min &&
+          200 * s_live_edges <= (unsigned long long)ctl->compact_pct * ctl->csr_slots) {
         done = 1;
         reason = kExitCompact;
       }
@@ -1654,7 +1668,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           const uint32_t s_len0 = __shfl_sync(kFull, slen, 0);
           const bool one_edge = __all_sync(kFull, !valid || e == e0);
           const bool hub0 = hubs && (L_beg & kHubDesc);
-          if (one_edge && !hub0 && (L_end - L_beg) <= 8u * s_len0) {
+          if (one_edge && !hub0 && (L_end - L_beg) <= a.arr.merge_ratio * s_len0) {
             // similar row lengths: walk the longer row with a warp-wide cursor;
             // every chunk of 32 entries is matched against the 32 sorted
             // elements by a shuffle search
@@ -1716,7 +1730,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
             if (look) {
               if (hubs && (lb & kHubDesc)) {
                 // the longer row's vertex has a hub map: one lookup
-                h = __ldg(U.hub_map + (unsigned long long)(lb & ~kHubDesc) * U.n + w);
+                h = __ldg(U.hub_map + (uint32_t)(le + w));
                 p = h != kInvalid ? 0u : kInvalid;
               } else {
                 p = find_in_row(U.row, lb, le, w);
@@ -1833,21 +1847,34 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
 // Hub maps: the vertices of highest degree (at least `min_deg`, at most the
 // reserved number of maps) get a dense map from neighbour id to edge id, so a
 // frontier element whose longer row is a hub's resolves its triangle with one
-// load instead of a search of the long row.
-//   k_hub_hist    histogram of floor(log2(degree))
+// load instead of a search of the long row.  A hub's map covers its own
+// member's vertex range only, so maps are as small as their graph, and unions
+// of many graphs get maps for the hubs of each.
+//   k_hub_hist    vertices and slots per floor(log2(degree)) (also the
+//                 degree signature the tuning is keyed on)
 //   k_hub_assign  hub index per vertex (kInvalid below the chosen degree)
+//   k_hub_layout  each hub's map base in the pool (a prefix over its member's
+//                 vertex count); hubs past the pool lose their map
 //   k_hub_fill    scatter each hub's row into its map (block per hub)
 __global__ void __launch_bounds__(256) k_hub_hist(const uint32_t* __restrict__ off, uint32_t n,
-                                                  uint32_t* __restrict__ hist) {
+                                                  uint32_t* __restrict__ hist,
+                                                  unsigned long long* __restrict__ hist_slots) {
   __shared__ uint32_t sh[33];
-  if (threadIdx.x < 33) sh[threadIdx.x] = 0;
+  __shared__ unsigned long long sl[33];
+  if (threadIdx.x < 33) { sh[threadIdx.x] = 0; sl[threadIdx.x] = 0; }
   __syncthreads();
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
     const uint32_t d = __ldg(off + u + 1) - __ldg(off + u);
-    if (d) atomicAdd(&sh[32 - __clz(d)], 1u);
+    if (d) {
+      atomicAdd(&sh[32 - __clz(d)], 1u);
+      atomicAdd(&sl[32 - __clz(d)], (unsigned long long)d);
+    }
   }
   __syncthreads();
-  if (threadIdx.x < 33 && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+  if (threadIdx.x < 33 && sh[threadIdx.x]) {
+    atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+    atomicAdd(&hist_slots[threadIdx.x], sl[threadIdx.x]);
+  }
 }
 
 __global__ void __launch_bounds__(256) k_hub_assign(const uint32_t* __restrict__ off, uint32_t n,
@@ -1867,18 +1894,53 @@ __global__ void __launch_bounds__(256) k_hub_assign(const uint32_t* __restrict__
   }
 }
 
+// One block: base of each hub's map = exclusive prefix of its member's vertex
+// count, minus the member's first vertex; a hub whose map would end past
+// `pool` entries gets none (hub_slot back to kInvalid).
+__global__ void __launch_bounds__(1024) k_hub_layout(const uint32_t* __restrict__ hub_vertex, uint32_t hubs,
+                                                     const Member* __restrict__ mem, uint32_t G,
+                                                     unsigned long long pool, uint32_t* __restrict__ hub_base,
+                                                     uint32_t* __restrict__ hub_slot) {
+  __shared__ unsigned long long sw[32];
+  unsigned long long carry = 0;
+  for (uint32_t b = 0; b < hubs; b += blockDim.x) {
+    const uint32_t k = b + threadIdx.x;
+    unsigned long long size = 0;
+    uint32_t u = 0, vb = 0;
+    if (k < hubs) {
+      u = hub_vertex[k];
+      uint32_t lo = 0, hi = G - 1;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (mem[mid].vb <= u) lo = mid; else hi = mid - 1;
+      }
+      vb = mem[lo].vb;
+      size = mem[lo].n;
+    }
+    unsigned long long total;
+    const unsigned long long at = carry + block_exclusive_scan<unsigned long long>(size, sw, total);
+    if (k < hubs) {
+      if (at + size <= pool) hub_base[k] = (uint32_t)at - vb;
+      else hub_slot[u] = kInvalid;
+    }
+    carry += total;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_hub_fill(const uint32_t* __restrict__ off,
-                                                  const unsigned long long* __restrict__ row0, uint32_t n,
+                                                  const unsigned long long* __restrict__ row0,
                                                   const uint32_t* __restrict__ hub_vertex, uint32_t hubs,
+                                                  const uint32_t* __restrict__ hub_slot,
+                                                  const uint32_t* __restrict__ hub_base,
                                                   uint32_t* __restrict__ hub_map) {
   for (uint32_t k = blockIdx.x; k < hubs; k += gridDim.x) {
     const uint32_t u = hub_vertex[k];
-    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
-    uint32_t* map = hub_map + (unsigned long long)k * n;
+    if (__ldg(hub_slot + u) != k) continue;  // no room in the pool
+    const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1), base = __ldg(hub_base + k);
     for (uint32_t s = b + threadIdx.x; s < e; s += blockDim.x) {
       const unsigned long long pr = __ldg(row0 + s);
-      const uint32_t id = (uint32_t)pr;
-      if (id < n) map[id] = (uint32_t)(pr >> 32);
+      const uint32_t id = (uint32_t)pr, eid = (uint32_t)(pr >> 32);
+      if (eid != kInvalid) hub_map[(uint32_t)(base + id)] = eid;
     }
   }
 }

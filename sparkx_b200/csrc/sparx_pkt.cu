@@ -15,6 +15,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -58,6 +59,100 @@ int status_from_flags(uint32_t f) {
   return SPARX_E_CUDA;
 }
 
+// ---------------------------------------------------------------------------
+// Tuning: the engine's performance knobs, picked per launch from a cache keyed
+// on the graph's degree distribution (filled by the autotuner, sparx_autotune;
+// defaults otherwise).  None of them changes a result, only the time.
+struct Tuning {
+  uint32_t merge_ratio = 8;        // peel: merge the rows when the longer is <= ratio x the shorter
+  uint32_t hub_min_degree = 1024;  // dense hub maps for vertices of at least this degree (0: none)
+  uint32_t sample_min = 64;        // support: longer out-lists from this length go through 64 samples
+  uint32_t support_kernel = 1;     // 1 balanced edge form, 2 vertex form
+  uint32_t compact_pct = 85;       // rebuild the peel's rows when live entries fill <= this % of them
+};
+
+// Degree-distribution signature: log2 of the slot count, log2 bucket of the
+// largest degree, and the share (in eighths) of slots in rows of degree >= 256.
+// hist_cnt[b] / hist_slots[b]: vertices / slots with degree in [2^(b-1), 2^b).
+struct TuneKey {
+  uint32_t log_w = 0, log_dmax = 0, skew8 = 0;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(log_w, log_dmax, skew8) < std::tie(o.log_w, o.log_dmax, o.skew8);
+  }
+};
+
+TuneKey tune_key(const uint32_t* hist_cnt, const unsigned long long* hist_slots, uint64_t W) {
+  TuneKey k;
+  k.log_w = W ? 63 - __builtin_clzll(W) : 0;
+  unsigned long long heavy = 0, total = 0;
+  for (int b = 1; b <= 32; ++b) {
+    if (hist_cnt[b]) k.log_dmax = (uint32_t)b;
+    total += hist_slots[b];
+    if (b >= 9) heavy += hist_slots[b];
+  }
+  k.skew8 = total ? (uint32_t)std::min<unsigned long long>(7, 8 * heavy / total) : 0;
+  return k;
+}
+
+std::mutex g_tune_mu;
+std::map<TuneKey, Tuning> g_tune;
+bool g_tune_loaded = false;
+thread_local const Tuning* g_tune_force = nullptr;  // the autotuner's candidate under test
+thread_local Tuning g_tune_last;                    // what the last launch on this thread used
+thread_local TuneKey g_tune_last_key;
+
+bool valid_tuning(const Tuning& t) {
+  return t.merge_ratio >= 1 && t.merge_ratio <= 1024 && (t.hub_min_degree == 0 || t.hub_min_degree >= 256) &&
+         t.sample_min >= 2 && (t.support_kernel == 1 || t.support_kernel == 2) && t.compact_pct >= 10 &&
+         t.compact_pct <= 100;
+}
+
+// Text cache: one line per key, "log_w log_dmax skew8 merge hub sample kernel compact".
+int tune_load_locked(const char* path) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return SPARX_E_NOT_FOUND;
+  unsigned a, b, c, d, e, g, h, i;
+  while (std::fscanf(f, "%u %u %u %u %u %u %u %u", &a, &b, &c, &d, &e, &g, &h, &i) == 8) {
+    Tuning t{d, e, g, h, i};
+    if (valid_tuning(t)) g_tune[TuneKey{a, b, c}] = t;
+  }
+  std::fclose(f);
+  return SPARX_OK;
+}
+
+int tune_save_locked(const char* path) {
+  FILE* f = std::fopen(path, "w");
+  if (!f) return SPARX_E_ARG;
+  for (const auto& kv : g_tune)
+    std::fprintf(f, "%u %u %u %u %u %u %u %u\n", kv.first.log_w, kv.first.log_dmax, kv.first.skew8,
+                 kv.second.merge_ratio, kv.second.hub_min_degree, kv.second.sample_min, kv.second.support_kernel,
+                 kv.second.compact_pct);
+  std::fclose(f);
+  return SPARX_OK;
+}
+
+// The tuning a launch uses: the autotuner's candidate, else the cached choice
+// for the key (the file named by SPARX_TUNE_FILE is read on first use), else
+// the defaults.
+Tuning resolve_tuning(const TuneKey& key) {
+  Tuning t;
+  if (g_tune_force) {
+    t = *g_tune_force;
+  } else {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (!g_tune_loaded) {
+      g_tune_loaded = true;
+      const char* path = std::getenv("SPARX_TUNE_FILE");
+      if (path && *path) tune_load_locked(path);
+    }
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) t = it->second;
+  }
+  g_tune_last = t;
+  g_tune_last_key = key;
+  return t;
+}
+
 struct Counters {  // device scalars
   uint32_t err;
   uint32_t kmax;
@@ -82,26 +177,28 @@ struct Layout {
   size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
   size_t alive;                   // compaction: one bit per edge, set while it is unprocessed
   size_t big;                     // compaction: rows longer than kWarpRow (a block each)
-  size_t hub_slot, hub_vertex, hub_hist, hub_map;  // hub maps (hub_cap == 0: none)
+  size_t hub_slot, hub_vertex, hub_base, hub_hist, hub_map;  // hub maps (hub_cap == 0: none)
   uint32_t hub_cap;
+  unsigned long long hub_pool;    // map entries reserved for all hubs together
   size_t tiles, ctl, mem, st, wpref, cnt, mem_tri, mem_maxsup, uni;
   size_t total;
 };
 
-// Hub maps (single-graph launches): at most kHubMaxCount maps of N u32
-// entries within kHubBudgetBytes, for vertices of degree >= kHubMinDegree
-// (so never more than W / kHubMinDegree of them).
+// Hub maps: at most kHubMaxCount maps, each of its member's vertex count in
+// u32 entries, within kHubBudgetBytes, for vertices of degree >= the tuned
+// floor (never below kHubFloor, so never more than W / kHubFloor of them).
 constexpr uint64_t kHubBudgetBytes = 4ull << 30;
-constexpr uint32_t kHubMinDegree = 1024;
+constexpr uint32_t kHubFloor = 256;
 constexpr uint32_t kHubMaxCount = 1024;
 
-uint32_t hub_capacity(uint64_t N, uint64_t W, uint32_t G) {
-  if (G != 1 || N == 0 || W >= (1ull << 31)) return 0;
-  const uint64_t k = std::min<uint64_t>({kHubMaxCount, W / kHubMinDegree, kHubBudgetBytes / (4 * N)});
+// maps reserved for a union whose largest member has `max_n` vertices
+uint32_t hub_capacity(uint64_t max_n, uint64_t W) {
+  if (max_n == 0 || W >= (1ull << 31)) return 0;
+  const uint64_t k = std::min<uint64_t>({kHubMaxCount, W / kHubFloor, kHubBudgetBytes / (4 * max_n)});
   return (uint32_t)k;
 }
 
-Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_bytes) {
+Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_bytes, uint64_t max_n = 0) {
   Layout L{};
   size_t p = 0;
   auto take = [&](size_t bytes) {
@@ -131,12 +228,15 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   L.rowB = take(8 * W);
   L.alive = take(4 * ((M + 31) / 32));
   L.big = take(4 * (W / kWarpRow + 1));
-  L.hub_cap = hub_capacity(N, W, G);
+  if (max_n == 0) max_n = N;
+  L.hub_cap = hub_capacity(max_n, W);
+  L.hub_hist = take(4 * 34 + 8 * 34);  // vertices, then slots, per log2 degree (always: the tuning key)
   if (L.hub_cap) {
+    L.hub_pool = std::min<unsigned long long>(4ull * L.hub_cap * max_n, kHubBudgetBytes) / 4;
     L.hub_slot = take(4 * N);
     L.hub_vertex = take(4ull * L.hub_cap);
-    L.hub_hist = take(4 * 34);
-    L.hub_map = take(4ull * L.hub_cap * N);
+    L.hub_base = take(4ull * L.hub_cap);
+    L.hub_map = take(4ull * L.hub_pool);
   }
   L.stage0 = take(kStageBytes);
   L.stage1 = take(kStageBytes);
@@ -348,7 +448,7 @@ int launch_support(int sm_count, uint32_t support_kernel, uint32_t n, uint64_t m
                    const uint32_t* opos, const uint32_t* ocol, const uint32_t* osrc, int2* es,
                    unsigned long long* spref, unsigned long long* tiles, Counters* cnt, uint32_t* heavy_list,
                    cudaStream_t s, uint32_t* launches, unsigned long long* support_elements,
-                   const uint32_t* mu = nullptr) {
+                   const uint32_t* mu = nullptr, uint32_t sample_min = Tuning{}.sample_min) {
   if (m == 0) return SPARX_OK;
   uint32_t slots = 8;
   while (slots < 2 * max_dplus) slots <<= 1;
@@ -369,10 +469,10 @@ int launch_support(int sm_count, uint32_t support_kernel, uint32_t n, uint64_t m
   exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, tiles, &cnt->grand, s);
   if (mu)
     k_support_balanced<true><<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri,
-                                                          &cnt->err, mu);
+                                                          &cnt->err, mu, sample_min);
   else
     k_support_balanced<false><<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri,
-                                                           &cnt->err, nullptr);
+                                                           &cnt->err, nullptr, sample_min);
   *launches += 4;
   CU(cudaMemcpyAsync(support_elements, spref + m, 8, cudaMemcpyDeviceToHost, s));
   return SPARX_OK;
@@ -442,6 +542,7 @@ struct UnionJob {
   uint32_t launches = 0;
   unsigned long long support_elements = 0;
   uint32_t hubs = 0;  // hub maps built
+  Tuning tuning;      // the knobs this launch used
   Control ctl{};
 };
 
@@ -461,8 +562,10 @@ PeelArrays peel_arrays(const Union& U) {
   a.qd1 = U.qd[1];
   a.hub_slot = U.hub_slot;
   a.hub_map = U.hub_map;
+  a.hub_base = U.hub_base;
   a.mu = nullptr;
   a.n = U.n;
+  a.merge_ratio = Tuning{}.merge_ratio;
   return a;
 }
 
@@ -552,7 +655,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   }
   // -- orientation (Kernel B) --
   const bool hubs_possible = L.hub_cap > 0 && !J.support_only;
-  uint32_t* hub_hist = hubs_possible ? at<uint32_t>(E, L.hub_hist) : nullptr;
+  uint32_t* hub_hist = at<uint32_t>(E, L.hub_hist);  // degree signature (tuning key) and hub choice
+  unsigned long long* hub_hist_slots = reinterpret_cast<unsigned long long*>(hub_hist + 34);
   uint32_t* big = at<uint32_t>(E, L.big);
   // multigraphs: deduplicated rows, copies per slot, caller slot -> slot and
   // multiplicity per edge id (in the second workspace), filled by pass 0
@@ -563,12 +667,11 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   Counters hc;
   uint32_t m32 = 0;
   uint32_t hist[34] = {};
+  unsigned long long hist_slots[34] = {};
   for (int pass = 0;; ++pass) {
-    if (hubs_possible) {
-      CU(cudaMemsetAsync(hub_hist, 0, 4 * 34, s));
-      k_hub_hist<<<grid_for(N, 256, E.sm_count * 4), 256, 0, s>>>(J.off, N, hub_hist);
-      J.launches += 1;
-    }
+    CU(cudaMemsetAsync(hub_hist, 0, 4 * 34 + 8 * 34, s));
+    k_hub_hist<<<grid_for(N, 256, E.sm_count * 4), 256, 0, s>>>(J.off, N, hub_hist, hub_hist_slots);
+    J.launches += 1;
     // rows orientation and compaction give a block each (listed by original degree)
     CU(cudaMemsetAsync(&cnt->big_count, 0, 4, s));
     k_big_rows<<<grid_for(N, 256, E.sm_count * 8), 256, 0, s>>>(J.off, N, big, &cnt->big_count);
@@ -583,7 +686,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaMemcpyAsync(J.members.data(), dmem, sizeof(Member) * G, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(&m32, opos + N, 4, cudaMemcpyDeviceToHost, s));
-    if (hubs_possible) CU(cudaMemcpyAsync(hist, hub_hist, 4 * 33, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(hist, hub_hist, 4 * 34, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(hist_slots, hub_hist_slots, 8 * 34, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     if (pass == 0) J.slot_self_loops = hc.self_loops;
     if (pass > 0 || hc.err != kErrMulti) break;
@@ -640,12 +744,15 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   J.launches += 2;
   // hub maps: the smallest power-of-two degree bound (>= kHubMinDegree) whose
   // vertices fit the reserved maps; hist[b] counts degrees in [2^(b-1), 2^b)
+  const Tuning T = resolve_tuning(tune_key(hist, hist_slots, Ws));
+  J.tuning = T;
   uint32_t hubs = 0, hub_min_deg = 0;
-  if (hubs_possible) {
+  if (hubs_possible && T.hub_min_degree) {
     uint64_t above = 0;
+    const uint64_t floor_deg = std::max<uint32_t>(T.hub_min_degree, kHubFloor);
     for (int b = 32; b >= 1; --b) {
       const uint64_t lo = 1ull << (b - 1);
-      if (lo < kHubMinDegree || above + hist[b] > L.hub_cap) break;
+      if (lo < floor_deg || above + hist[b] > L.hub_cap) break;
       above += hist[b];
       hub_min_deg = (uint32_t)lo;
     }
@@ -653,18 +760,25 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   }
   const uint32_t* d_hub_slot = nullptr;
   const uint32_t* d_hub_map = nullptr;
+  const uint32_t* d_hub_base = nullptr;
   if (hubs) {
     uint32_t* hslot = at<uint32_t>(E, L.hub_slot);
     uint32_t* hvert = at<uint32_t>(E, L.hub_vertex);
+    uint32_t* hbase = at<uint32_t>(E, L.hub_base);
     uint32_t* hmap = at<uint32_t>(E, L.hub_map);
+    uint64_t max_n = 0;
+    for (const Member& M : J.members) max_n = std::max<uint64_t>(max_n, M.n);
     CU(cudaMemsetAsync(&cnt->hub_count, 0, 4, s));
     k_hub_assign<<<grid_for(N, 256, E.sm_count * 8), 256, 0, s>>>(J.off, N, hub_min_deg, hubs, hslot, hvert,
                                                                   &cnt->hub_count);
-    CU(cudaMemsetAsync(hmap, 0xFF, 4ull * hubs * N, s));
-    k_hub_fill<<<std::min<uint32_t>(hubs, E.sm_count * 8), 256, 0, s>>>(J.off, row0, N, hvert, hubs, hmap);
-    J.launches += 2;
+    k_hub_layout<<<1, 1024, 0, s>>>(hvert, hubs, dmem, G, L.hub_pool, hbase, hslot);
+    CU(cudaMemsetAsync(hmap, 0xFF, 4ull * std::min<unsigned long long>(L.hub_pool, hubs * max_n), s));
+    k_hub_fill<<<std::min<uint32_t>(hubs, E.sm_count * 8), 256, 0, s>>>(J.off, row0, hvert, hubs, hslot, hbase,
+                                                                        hmap);
+    J.launches += 3;
     d_hub_slot = hslot;
     d_hub_map = hmap;
+    d_hub_base = hbase;
   }
   J.hubs = hubs;
   CU(cudaEventRecord(E.tev[2], s));
@@ -672,9 +786,10 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   // -- support (Kernel C) --
   CU(cudaMemsetAsync(es, 0, 8 * std::max<uint64_t>(m, 1), s));
   {
-    int rc = launch_support(E.sm_count, O.support_kernel, N, m, hc.max_dplus, opos, ocol, osrc, es,
-                            at<unsigned long long>(E, L.q0), at<unsigned long long>(E, L.tiles), cnt,
-                            at<uint32_t>(E, L.act0), s, &J.launches, &J.support_elements, mu);
+    int rc = launch_support(E.sm_count, O.support_kernel ? O.support_kernel : T.support_kernel, N, m,
+                            hc.max_dplus, opos, ocol, osrc, es, at<unsigned long long>(E, L.q0),
+                            at<unsigned long long>(E, L.tiles), cnt, at<uint32_t>(E, L.act0), s, &J.launches,
+                            &J.support_elements, mu, T.sample_min);
     if (rc) return rc;
   }
   CU(cudaEventRecord(E.tev[3], s));
@@ -708,6 +823,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     U.qd[1] = at<uint4>(E, L.qd1);
     U.hub_slot = d_hub_slot;
     U.hub_map = d_hub_map;
+    U.hub_base = d_hub_base;
     U.n = N;
     U.m = (uint32_t)m;
     U.width = (uint32_t)W;
@@ -721,6 +837,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     c0.timeout_ns = O.timeout_ms * 1000000ull;
     c0.csr_slots = Ws;
     c0.compact_min = kCompactMinSlots;
+    c0.compact_pct = T.compact_pct;
     // wave trace: when SPARX_TRACE_FILE names a file, the planner records
     // each wave's start time and work there (first 2^20 waves)
     const char* trace_path = std::getenv("SPARX_TRACE_FILE");
@@ -743,6 +860,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     wa.Up = at<Union>(E, L.uni);
     wa.arr = peel_arrays(U);
     wa.arr.mu = mu;
+    wa.arr.merge_ratio = T.merge_ratio;
     wa.mem = dmem;
     wa.st = at<MemberState>(E, L.st);
     wa.ctl = at<Control>(E, L.ctl);
@@ -1201,16 +1319,17 @@ int run_batch_union(Engine& E, std::vector<HostMember>& hm, const Opts& O, int* 
                     sparx_pkt_stats* stats_out, int* first_fail) {
   const size_t G = hm.size();
   UnionJob J;
-  uint64_t N = 0, Wt = 0;
+  uint64_t N = 0, Wt = 0, max_n = 0;
   for (const HostMember& h : hm) {
     J.members.push_back(Member{(uint32_t)N, (uint32_t)h.n, (uint32_t)Wt, (uint32_t)h.w, 0, 0});
     N += h.n;
     Wt += h.w;
+    max_n = std::max<uint64_t>(max_n, h.n);
   }
   J.N = N;
   J.W = Wt;
   const size_t out_bytes = (O.out_bits / 8) * Wt;
-  J.L = make_layout(N, Wt, (uint32_t)G, true, out_bytes);
+  J.L = make_layout(N, Wt, (uint32_t)G, true, out_bytes, max_n);
   int rc = ensure_ws(E, J.L.total);
   auto fail_all = [&](int code) {
     for (size_t g = 0; g < G; ++g) {
@@ -1319,11 +1438,12 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
   size_t at_i = 0;
   while (at_i < valid.size()) {
     std::vector<HostMember> wave;
-    uint64_t N = 0, Wt = 0;
+    uint64_t N = 0, Wt = 0, max_n = 0;
     while (at_i < valid.size()) {
       const HostMember& h = valid[at_i];
-      const uint64_t N2 = N + h.n, W2 = Wt + h.w;
-      const size_t bytes = make_layout(N2, W2, (uint32_t)wave.size() + 1, true, (O.out_bits / 8) * W2).total;
+      const uint64_t N2 = N + h.n, W2 = Wt + h.w, mx2 = std::max<uint64_t>(max_n, h.n);
+      const size_t bytes =
+          make_layout(N2, W2, (uint32_t)wave.size() + 1, true, (O.out_bits / 8) * W2, mx2).total;
       const bool fits = N2 < 0xFFFFFFFFull && W2 < 0xFFFFFFFFull && bytes <= budget && wave.size() < 65536;
       if (!fits && !wave.empty()) break;
       if (!fits) {  // a single graph over the budget
@@ -1335,6 +1455,7 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
       wave.push_back(h);
       N = N2;
       Wt = W2;
+      max_n = mx2;
       ++at_i;
     }
     if (!wave.empty()) run_batch_union(E, wave, O, status_out, stats_out, &first_fail);
@@ -1421,11 +1542,11 @@ void server_worker(sparx_server* S, int lane) {
         if (S->stop) return;
         continue;
       }
-      uint64_t N = 0, W = 0;
+      uint64_t N = 0, W = 0, max_n = 0;
       while (!S->queue.empty() && batch.size() < kServerMaxMembers) {
         ServerReq* r = S->queue.front();
-        const uint64_t N2 = N + r->h.n, W2 = W + r->h.w;
-        const size_t bytes = make_layout(N2, W2, (uint32_t)batch.size() + 1, true, esz * W2).total;
+        const uint64_t N2 = N + r->h.n, W2 = W + r->h.w, mx2 = std::max<uint64_t>(max_n, r->h.n);
+        const size_t bytes = make_layout(N2, W2, (uint32_t)batch.size() + 1, true, esz * W2, mx2).total;
         const bool fits = bytes <= S->lane_budget && N2 < 0xFFFFFFFFull && W2 < 0xFFFFFFFFull;
         if (!fits) {
           if (batch.empty()) {  // never fits a lane on its own
@@ -1442,6 +1563,7 @@ void server_worker(sparx_server* S, int lane) {
         batch.push_back(r);
         N = N2;
         W = W2;
+        max_n = mx2;
       }
     }
     if (batch.empty()) continue;
@@ -1608,6 +1730,242 @@ int sparx_server_destroy(sparx_server* S) {
   return SPARX_OK;
 }
 
+
+// ---- tuning and the autotuner ------------------------------------------------
+
+int sparx_tuning_default(sparx_tuning* t) {
+  if (!t) return SPARX_E_ARG;
+  const Tuning d;
+  t->struct_size = sizeof(sparx_tuning);
+  t->merge_ratio = d.merge_ratio;
+  t->hub_min_degree = d.hub_min_degree;
+  t->sample_min = d.sample_min;
+  t->support_kernel = d.support_kernel;
+  t->compact_pct = d.compact_pct;
+  return SPARX_OK;
+}
+
+int sparx_tuning_signature(const uint64_t* offsets, uint64_t n_plus_1, uint32_t key[3]) {
+  if (!offsets || !key || n_plus_1 < 1) return SPARX_E_ARG;
+  uint32_t cnt[34] = {};
+  unsigned long long slots[34] = {};
+  for (uint64_t u = 0; u + 1 < n_plus_1; ++u) {
+    const uint64_t d = offsets[u + 1] - offsets[u];
+    if (!d || d > 0xFFFFFFFFull) continue;
+    const int b = 32 - __builtin_clz((uint32_t)d);
+    cnt[b]++;
+    slots[b] += d;
+  }
+  const TuneKey k = tune_key(cnt, slots, offsets[n_plus_1 - 1] - offsets[0]);
+  key[0] = k.log_w;
+  key[1] = k.log_dmax;
+  key[2] = k.skew8;
+  return SPARX_OK;
+}
+
+namespace {
+Tuning from_c(const sparx_tuning* t) {
+  return Tuning{t->merge_ratio, t->hub_min_degree, t->sample_min, t->support_kernel, t->compact_pct};
+}
+void to_c(const Tuning& t, sparx_tuning* o) {
+  o->struct_size = sizeof(sparx_tuning);
+  o->merge_ratio = t.merge_ratio;
+  o->hub_min_degree = t.hub_min_degree;
+  o->sample_min = t.sample_min;
+  o->support_kernel = t.support_kernel;
+  o->compact_pct = t.compact_pct;
+}
+}  // namespace
+
+int sparx_tuning_lookup(const uint32_t key[3], sparx_tuning* out, int* found) {
+  if (!key || !out) return SPARX_E_ARG;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(TuneKey{key[0], key[1], key[2]});
+  if (found) *found = it != g_tune.end();
+  to_c(it != g_tune.end() ? it->second : Tuning{}, out);
+  return SPARX_OK;
+}
+
+int sparx_tuning_store(const uint32_t key[3], const sparx_tuning* t) {
+  if (!key || !t || (t->struct_size && t->struct_size < sizeof(sparx_tuning))) return SPARX_E_ARG;
+  const Tuning v = from_c(t);
+  if (!valid_tuning(v)) { g_last_error = "tuning value out of range"; return SPARX_E_ARG; }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[TuneKey{key[0], key[1], key[2]}] = v;
+  return SPARX_OK;
+}
+
+int sparx_tuning_clear(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
+  g_tune_loaded = true;  // an explicit clear also drops what SPARX_TUNE_FILE would add
+  return SPARX_OK;
+}
+
+int sparx_tuning_last(sparx_tuning* used, uint32_t key[3]) {
+  if (used) to_c(g_tune_last, used);
+  if (key) {
+    key[0] = g_tune_last_key.log_w;
+    key[1] = g_tune_last_key.log_dmax;
+    key[2] = g_tune_last_key.skew8;
+  }
+  return SPARX_OK;
+}
+
+int sparx_tuning_save(const char* path) {
+  if (!path) return SPARX_E_ARG;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return tune_save_locked(path);
+}
+
+int sparx_tuning_load(const char* path) {
+  if (!path) return SPARX_E_ARG;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_loaded = true;
+  return tune_load_locked(path);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Coordinate descent over the knobs, one group at a time from the defaults:
+// the support form and sampling threshold by the support pass's device time,
+// then the hub-map floor (orientation + peel, since the maps are built with
+// the orientation), the merge ratio and the compaction fill by the peel's.
+// `run(t, &ms_support, &ms_rest)` decomposes the sample once with knobs t.
+// The best knobs are stored under the sample's key (and written to the file
+// SPARX_TUNE_FILE names, if any).
+template <class RunF>
+int autotune_core(RunF run, uint32_t repeats, Tuning* best_out, TuneKey* key_out) {
+  repeats = std::max<uint32_t>(1, std::min<uint32_t>(repeats, 15));
+  auto measure = [&](const Tuning& t, double* sup, double* rest) -> int {
+    std::vector<double> a, b;
+    g_tune_force = &t;
+    int rc = SPARX_OK;
+    for (uint32_t r = 0; r < repeats && !rc; ++r) {
+      double x = 0, y = 0;
+      rc = run(&x, &y);
+      a.push_back(x);
+      b.push_back(y);
+    }
+    g_tune_force = nullptr;
+    if (rc) return rc;
+    std::sort(a.begin(), a.end());
+    std::sort(b.begin(), b.end());
+    *sup = a[a.size() / 2];
+    *rest = b[b.size() / 2];
+    return SPARX_OK;
+  };
+  Tuning cur;
+  double sup = 0, rest = 0;
+  int rc = measure(cur, &sup, &rest);  // also warms the engine for this size
+  if (rc) return rc;
+  rc = measure(cur, &sup, &rest);
+  if (rc) return rc;
+  const TuneKey key = g_tune_last_key;
+  auto try_group = [&](std::vector<Tuning> cands, bool support_time) -> int {
+    double best = support_time ? sup : rest;
+    for (const Tuning& c : cands) {
+      double x = 0, y = 0;
+      const int r = measure(c, &x, &y);
+      if (r) return r;
+      const double v = support_time ? x : y;
+      if (v < best * 0.98) {  // a 2% margin keeps noise from flipping a knob
+        best = v;
+        cur = c;
+        sup = x;
+        rest = y;
+      }
+    }
+    return SPARX_OK;
+  };
+  std::vector<Tuning> c1;
+  for (uint32_t smp : {32u, 128u, 256u}) { Tuning t = cur; t.sample_min = smp; c1.push_back(t); }
+  { Tuning t = cur; t.support_kernel = 2; c1.push_back(t); }
+  if ((rc = try_group(c1, true))) return rc;
+  std::vector<Tuning> c2;
+  for (uint32_t h : {0u, 512u, 4096u}) { Tuning t = cur; t.hub_min_degree = h; c2.push_back(t); }
+  if ((rc = try_group(c2, false))) return rc;
+  std::vector<Tuning> c3;
+  for (uint32_t mr : {4u, 16u}) { Tuning t = cur; t.merge_ratio = mr; c3.push_back(t); }
+  if ((rc = try_group(c3, false))) return rc;
+  std::vector<Tuning> c4;
+  for (uint32_t cp : {75u, 95u}) { Tuning t = cur; t.compact_pct = cp; c4.push_back(t); }
+  if ((rc = try_group(c4, false))) return rc;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = cur;
+    const char* path = std::getenv("SPARX_TUNE_FILE");
+    if (path && *path) tune_save_locked(path);
+  }
+  *best_out = cur;
+  *key_out = key;
+  return SPARX_OK;
+}
+
+void key_to_c(const TuneKey& k, uint32_t key[3]) {
+  if (!key) return;
+  key[0] = k.log_w;
+  key[1] = k.log_dmax;
+  key[2] = k.skew8;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sparx_autotune(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,
+                   const sparx_pkt_opts* opts, uint32_t repeats, sparx_tuning* best, uint32_t key[3]) {
+  g_last_error.clear();
+  if (!offsets || !neighbours || !best) { set_error("null pointer"); return SPARX_E_ARG; }
+  sparx_pkt_opts o;
+  if (opts) o = *opts; else sparx_pkt_default_opts(&o);
+  o.struct_size = sizeof(o);
+  o.out_bits = 32;
+  o.support_kernel = 0;  // the tuning picks the support form
+  std::vector<uint32_t> out(std::max<uint64_t>(width, 1));
+  auto run = [&](double* sup, double* rest) -> int {
+    sparx_pkt_stats st;
+    const int rc = run_host(offsets, n_plus_1, neighbours, 64, width, out.data(), false, &o, &st);
+    *sup = st.ms_support;
+    *rest = st.ms_orient + st.ms_peel;
+    return rc;
+  };
+  Tuning t;
+  TuneKey k;
+  const int rc = autotune_core(run, repeats, &t, &k);
+  if (rc) return rc;
+  to_c(t, best);
+  key_to_c(k, key);
+  return SPARX_OK;
+}
+
+int sparx_autotune_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
+                         const sparx_pkt_opts* opts, uint32_t repeats, sparx_tuning* best, uint32_t key[3]) {
+  g_last_error.clear();
+  if (!graphs || !count || !best) { set_error("null or empty graph list"); return SPARX_E_ARG; }
+  sparx_pkt_opts o;
+  if (opts) o = *opts; else sparx_pkt_default_opts(&o);
+  o.struct_size = sizeof(o);
+  o.support_kernel = 0;
+  std::vector<sparx_pkt_stats> st(count);
+  std::vector<int> status(count);
+  auto run = [&](double* sup, double* rest) -> int {
+    const int rc = run_batch(graphs, count, hbm_budget_bytes, &o, status.data(), st.data());
+    // the first union's phases (members of a union share them)
+    *sup = st[0].ms_support;
+    *rest = st[0].ms_orient + st[0].ms_peel;
+    return rc;
+  };
+  Tuning t;
+  TuneKey k;
+  const int rc = autotune_core(run, repeats, &t, &k);
+  if (rc) return rc;
+  to_c(t, best);
+  key_to_c(k, key);
+  return SPARX_OK;
+}
 
 int sparx_pkt_default_opts(sparx_pkt_opts* o) {
   if (!o) return SPARX_E_ARG;
@@ -1940,6 +2298,7 @@ int run_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1, const uint32_t* d_
   c0.timeout_ns = kDefaultTimeoutMs * 1000000ull;
   c0.csr_slots = width;
   c0.compact_min = ~0ull;  // no compaction buffers in the fixed scratch
+  c0.compact_pct = Tuning{}.compact_pct;
   Union* dU = (Union*)P(L.uni);
   Member* dM = (Member*)P(L.mem);
   Control* dC = (Control*)P(L.ctl);

@@ -85,6 +85,11 @@ class _GraphView(ctypes.Structure):
     ]
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint32) for name in
+                ("struct_size", "merge_ratio", "hub_min_degree", "sample_min", "support_kernel", "compact_pct")]
+
+
 EXPORTS = [
     "sparx_pkt_default_opts", "sparx_strerror", "sparx_last_error", "sparx_pkt_run",
     "sparx_pkt_run_u32", "sparx_pkt_run_device", "sparx_triangles_run", "sparx_clustering_run",
@@ -125,6 +130,21 @@ def lib():
     if hasattr(L, "sparx_pkt_run_batch"):
         L.sparx_pkt_run_batch.restype = i32
         L.sparx_pkt_run_batch.argtypes = [P(_GraphView), u64, u64, P(_Opts), P(ctypes.c_int), P(_Stats)]
+    key3 = P(ctypes.c_uint32)
+    for name, args in (("sparx_tuning_default", [P(_Tuning)]),
+                       ("sparx_tuning_signature", [vp, u64, key3]),
+                       ("sparx_tuning_lookup", [key3, P(_Tuning), P(ctypes.c_int)]),
+                       ("sparx_tuning_store", [key3, P(_Tuning)]),
+                       ("sparx_tuning_clear", []),
+                       ("sparx_tuning_last", [P(_Tuning), key3]),
+                       ("sparx_tuning_save", [ctypes.c_char_p]),
+                       ("sparx_tuning_load", [ctypes.c_char_p]),
+                       ("sparx_autotune", [vp, u64, vp, u64, P(_Opts), ctypes.c_uint32, P(_Tuning), key3]),
+                       ("sparx_autotune_batch", [P(_GraphView), u64, u64, P(_Opts), ctypes.c_uint32, P(_Tuning),
+                                                 key3])):
+        f = getattr(L, name)
+        f.restype = i32
+        f.argtypes = args
     L._sparx_typed = True
     return L
 
@@ -511,3 +531,106 @@ def run_pkt_device_noalloc(d_offsets: int, n_plus_1: int, d_neighbours: int, wid
     graph must fit it and calls must not overlap on the GPU."""
     _check(lib().sparx_pkt_run_device_noalloc(d_offsets, n_plus_1, d_neighbours, width, d_out, device,
                                               stream or None))
+
+
+# ---- tuning ----------------------------------------------------------------------------------
+
+@dataclasses.dataclass(frozen=True)
+class PktTuning:
+    """The engine's performance knobs (``sparx_tuning``); none changes a result."""
+    merge_ratio: int = 8
+    hub_min_degree: int = 1024
+    sample_min: int = 64
+    support_kernel: int = 1
+    compact_pct: int = 85
+
+    def c(self) -> _Tuning:
+        t = _Tuning()
+        t.struct_size = ctypes.sizeof(_Tuning)
+        for f in dataclasses.fields(self):
+            setattr(t, f.name, getattr(self, f.name))
+        return t
+
+    @classmethod
+    def from_c(cls, t: _Tuning) -> "PktTuning":
+        return cls(**{f.name: getattr(t, f.name) for f in dataclasses.fields(cls)})
+
+
+def _key(key):
+    return (ctypes.c_uint32 * 3)(*key)
+
+
+def tuning_signature(offsets) -> tuple:
+    """Degree signature (log2 slots, log2 bucket of the max degree, eighths of slots in rows of
+    degree >= 256) under which tuned knobs are cached."""
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    k = (ctypes.c_uint32 * 3)()
+    _check(lib().sparx_tuning_signature(off.ctypes.data, off.shape[0], k))
+    return tuple(k)
+
+
+def tuning_lookup(key) -> tuple[PktTuning, bool]:
+    t, found = _Tuning(), ctypes.c_int()
+    _check(lib().sparx_tuning_lookup(_key(key), ctypes.byref(t), ctypes.byref(found)))
+    return PktTuning.from_c(t), bool(found.value)
+
+
+def tuning_store(key, tuning: PktTuning) -> None:
+    t = tuning.c()
+    _check(lib().sparx_tuning_store(_key(key), ctypes.byref(t)))
+
+
+def tuning_clear() -> None:
+    _check(lib().sparx_tuning_clear())
+
+
+def tuning_last() -> tuple[PktTuning, tuple]:
+    """Knobs and key the last launch on this thread used."""
+    t, k = _Tuning(), (ctypes.c_uint32 * 3)()
+    _check(lib().sparx_tuning_last(ctypes.byref(t), k))
+    return PktTuning.from_c(t), tuple(k)
+
+
+def tuning_save(path: str) -> None:
+    _check(lib().sparx_tuning_save(path.encode()))
+
+
+def tuning_load(path: str) -> None:
+    _check(lib().sparx_tuning_load(path.encode()))
+
+
+def autotune(offsets, neighbours, opts: PktOptions | None = None, repeats: int = 3) -> tuple[PktTuning, tuple]:
+    """Measure candidate knobs on one sample graph and cache the best under its key."""
+    opts = opts or PktOptions(out_bits=32)
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    nbr = np.ascontiguousarray(neighbours, dtype=np.uint64)
+    t, k = _Tuning(), (ctypes.c_uint32 * 3)()
+    o = opts.c()
+    _check(lib().sparx_autotune(off.ctypes.data, off.shape[0], nbr.ctypes.data, nbr.shape[0], ctypes.byref(o),
+                                repeats, ctypes.byref(t), k))
+    return PktTuning.from_c(t), tuple(k)
+
+
+def autotune_batch(graphs, opts: PktOptions | None = None, repeats: int = 3,
+                   hbm_budget_bytes: int = 0) -> tuple[PktTuning, tuple]:
+    """Autotune on a batch sample (timed on its first union, whose key gets the winner)."""
+    opts = opts or PktOptions(out_bits=32)
+    views = (_GraphView * len(graphs))()
+    keep = []
+    for i, (off, nbr) in enumerate(graphs):
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        nbr = np.ascontiguousarray(nbr)
+        if nbr.dtype not in (np.uint64, np.uint32):
+            nbr = nbr.astype(np.uint64)
+        out = np.empty(nbr.shape[0], dtype=np.uint8 if opts.out_bits == 8 else np.uint32)
+        keep += [off, nbr, out]
+        v = views[i]
+        v.offsets, v.n_plus_1 = off.ctypes.data, off.shape[0]
+        v.neighbours, v.width = nbr.ctypes.data, nbr.shape[0]
+        v.neighbour_bits = 64 if nbr.dtype == np.uint64 else 32
+        v.truss_out = out.ctypes.data
+    t, k = _Tuning(), (ctypes.c_uint32 * 3)()
+    o = opts.c()
+    _check(lib().sparx_autotune_batch(views, len(graphs), hbm_budget_bytes, ctypes.byref(o), repeats,
+                                      ctypes.byref(t), k))
+    return PktTuning.from_c(t), tuple(k)

@@ -1,0 +1,53 @@
+"""The tuning cache on the CPU: the degree signature, store / lookup / clear,
+and the text file the autotuner writes (no GPU: nothing here launches work)."""
+import numpy as np
+import pytest
+
+from sparkx_b200 import build, gen
+import sparkx_b200.pkt as P
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    build.build_engine()
+    P.lib()
+    yield
+    P.tuning_clear()
+
+
+def _signature(g):
+    d = np.diff(g.offsets.astype(np.int64))
+    d = d[d > 0]
+    b = np.floor(np.log2(d)).astype(np.int64) + 1
+    slots = np.bincount(b, weights=d, minlength=34)
+    heavy = slots[9:].sum()
+    total = slots.sum()
+    return (int(np.log2(g.width)) if g.width else 0, int(b.max()) if b.size else 0,
+            int(min(7, 8 * heavy // total)) if total else 0)
+
+
+def test_signature_matches_the_degree_histogram():
+    for g in (gen.rmat(12, 16, seed=2), gen.erdos_renyi(5000, 40000, 1), gen.rmat(14, 8, seed=3),
+              gen.from_edges(3, [(0, 1)])):
+        assert P.tuning_signature(g.offsets) == _signature(g)
+
+
+def test_store_lookup_save_load(tmp_path):
+    P.tuning_clear()
+    key = (20, 12, 3)
+    t, found = P.tuning_lookup(key)
+    assert not found and t == P.PktTuning()
+    mine = P.PktTuning(merge_ratio=4, hub_min_degree=512, sample_min=128, support_kernel=2, compact_pct=75)
+    P.tuning_store(key, mine)
+    assert P.tuning_lookup(key) == (mine, True)
+    path = str(tmp_path / "tune.txt")
+    P.tuning_save(path)
+    P.tuning_clear()
+    assert not P.tuning_lookup(key)[1]
+    P.tuning_load(path)
+    assert P.tuning_lookup(key) == (mine, True)
+    with pytest.raises(P.PktError):
+        P.tuning_store(key, P.PktTuning(compact_pct=5))   # out of range
+    with pytest.raises(P.PktError):
+        P.tuning_store(key, P.PktTuning(hub_min_degree=100))
+    P.tuning_clear()

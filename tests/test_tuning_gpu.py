@@ -1,0 +1,80 @@
+"""The tuned knobs change time only: every candidate the autotuner can pick
+gives the oracle's truss numbers bit for bit, on single graphs and on batched
+unions (whose members now get hub maps of their own); the autotuner stores a
+valid choice that later launches with the same key use."""
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from sparkx_b200 import gen
+import sparkx_b200.pkt as P
+
+pytestmark = pytest.mark.gpu
+O32 = P.PktOptions(out_bits=32, timeout_ms=120_000)
+
+CANDIDATES = [P.PktTuning(merge_ratio=mr, hub_min_degree=h, sample_min=smp, support_kernel=sk, compact_pct=cp)
+              for mr, h, smp, sk, cp in itertools.product((4, 16), (0, 256, 4096), (32, 256), (1, 2), (75, 95))]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _engine():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    from sparkx_b200 import build
+    build.build_engine()
+    P.tuning_clear()
+    yield
+    P.tuning_clear()
+
+
+def _with_tuning(t, fn):
+    """Run fn once to learn its launch key, then again with t stored under that key."""
+    fn()
+    _, key = P.tuning_last()
+    P.tuning_store(key, t)
+    try:
+        out = fn()
+        used, _ = P.tuning_last()
+        assert used == t
+        return out
+    finally:
+        P.tuning_clear()
+
+
+def test_every_candidate_gives_the_same_truss():
+    # R-MAT-16 has rows past 1024 and 4096 entries (hub maps) and is big enough to compact
+    g = gen.rmat(16, 16, seed=2)
+    want = O.fast_truss(g.offsets, g.neighbours)[0]
+    for t in CANDIDATES[::3]:
+        got, st = _with_tuning(t, lambda: P.run_pkt(g.offsets, g.neighbours, O32))
+        assert np.array_equal(got, want), t
+        assert (st.hub_maps > 0) == (t.hub_min_degree in (256, 4096)), (t, st.hub_maps)
+
+
+def test_batched_unions_get_member_hub_maps():
+    members = [gen.rmat(13, 16, seed=s) for s in range(3)] + [gen.erdos_renyi(4000, 40000, 5),
+                                                              gen.rmat(12, 32, seed=9)]
+    want = [O.fast_truss(m.offsets, m.neighbours)[0] for m in members]
+    pairs = [(m.offsets, m.neighbours) for m in members]
+    for t in (P.PktTuning(hub_min_degree=256), P.PktTuning(hub_min_degree=256, merge_ratio=4, compact_pct=95),
+              P.PktTuning(hub_min_degree=0)):
+        res = _with_tuning(t, lambda: P.run_batch(pairs, O32))
+        for w, (truss, st, status) in zip(want, res):
+            assert status == 0 and np.array_equal(truss, w), t
+
+
+def test_autotune_stores_a_choice_the_next_launch_uses(tmp_path, monkeypatch):
+    g = gen.rmat(15, 16, seed=4)
+    best, key = P.autotune(g.offsets, g.neighbours, repeats=1)
+    assert key == P.tuning_signature(g.offsets)
+    assert P.tuning_lookup(key) == (best, True)
+    truss, _ = P.run_pkt(g.offsets, g.neighbours, O32)
+    assert P.tuning_last() == (best, key)
+    assert np.array_equal(truss, O.fast_truss(g.offsets, g.neighbours)[0])
+    # a batch sample: the winner goes to its union's key
+    members = [gen.mix_graph(gen.mix_member(i)) for i in range(6)]
+    best_b, key_b = P.autotune_batch([(m.offsets, m.neighbours) for m in members], repeats=1)
+    assert P.tuning_lookup(key_b) == (best_b, True)
+    P.tuning_clear()
