@@ -44,6 +44,7 @@ extern "C" {
 #define SPARX_E_ARG           8  /* bad argument */
 #define SPARX_E_NOT_FOUND     9  /* unknown ticket */
 #define SPARX_E_CANCELLED    10  /* request cancelled before completion */
+#define SPARX_E_PARSE        11  /* malformed MatrixMarket text (see sparx_last_error) */
 
 /* ---- options ---------------------------------------------------------- */
 #define SPARX_SUPPORT_WIDE 0u  /* u32 triangle counters: the defined truss */
@@ -198,6 +199,29 @@ int sparx_clustering_run(const uint64_t* offsets, uint64_t n_plus_1, const uint6
 int sparx_pkt_run_device_noalloc(const uint64_t* d_offsets, uint64_t n_plus_1,
                                  const uint32_t* d_neighbours, uint64_t width, uint32_t* d_truss_out,
                                  int device, void* cuda_stream);
+
+/* ---- input ------------------------------------------------------------- */
+/*
+ * MatrixMarket text -> CSR in the reference's layout, on the GPU.  Replaces
+ * GraphCache::from_mtx_file (graph/cache/parser_mtx/mod.rs:34-162) with its
+ * semantics: header "%%MatrixMarket matrix coordinate pattern|integer
+ * symmetric|skew-symmetric|general" (case-insensitive), '%' and blank lines
+ * skipped, size line "nrows ncols nnz" with nrows == ncols; every entry line
+ * with at least two tokens i j (1-based; a third, the integer value, is
+ * ignored) adds slot j-1 to row i-1 and, unless the header says general and
+ * when i != j, slot i-1 to row j-1 (parser_mtx/producers.rs:139-240);
+ * duplicates stay (parallel edges); rows are sorted ascending
+ * (impl_sort.rs:10-51).  Every entry line of the text is read, whatever nnz
+ * the size line declares.  An index of 0, beyond nrows or not an unsigned
+ * integer returns SPARX_E_PARSE (sparx_last_error names the line).
+ *   text, len          the file's bytes (host memory)
+ *   offsets_out        u64[n+1], neighbours_out u64[width] (host), or NULL:
+ *                      then only *n_out and *width_out are set, so a caller
+ *                      can size its buffers and call again
+ */
+int sparx_mtx_to_csr(const char* text, uint64_t len, uint64_t* offsets_out, uint64_t offsets_cap,
+                     uint64_t* neighbours_out, uint64_t neighbours_cap, uint64_t* n_out, uint64_t* width_out,
+                     const sparx_pkt_opts* opts);
 
 /* ---- tuning ------------------------------------------------------------ */
 /*

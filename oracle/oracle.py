@@ -299,3 +299,99 @@ def support_definition(off, nbr):
             if v != u:
                 out[s] = sum(c * cnt[v][w] for w, c in cnt[u].items() if w in cnt[v] and w != v)
     return out
+
+
+def _mtx_usize(tok: str) -> int:
+    """Rust's usize::from_str: an optional '+', then ASCII digits (64-bit)."""
+    t = tok[1:] if tok.startswith("+") else tok
+    if not t or not all("0" <= c <= "9" for c in t):
+        raise OracleError(f"not an unsigned integer: {tok!r}")
+    v = int(t)
+    if v >= 1 << 64:
+        raise OracleError(f"integer overflow: {tok!r}")
+    return v
+
+
+def mtx_to_csr(data: bytes):
+    """CSR (offsets u64[n+1], neighbours u64[width]) from MatrixMarket text, restating
+    GraphCache::from_mtx_file (graph/cache/parser_mtx/mod.rs:34-162): the header checks and size
+    line of parse_mtx_header (producers.rs:139-176), the entry lines of
+    parallel_no_labels_parse_mtx_with (producers.rs:217-240: blank and '%' lines skipped, a line
+    with fewer than two tokens skipped, 1-based indices, 0 or >= nrows an error, the mirror of
+    (i, j) added unless the header says general or i == j), degree count and scatter
+    (mod.rs:74-155) and the per-row sort (impl_sort.rs:10-51).  Duplicates stay.  The reference
+    stops reading once its threads have seen nnz entries (checked per thread chunk); a text with
+    exactly nnz entries is read in full, as here, where every entry line is read."""
+    text = data.decode("latin-1")
+    lines = text.split("\n")
+    if not lines or not lines[0].startswith("%%MatrixMarket"):
+        raise OracleError("invalid MatrixMarket header")
+    toks = lines[0].split()
+    if len(toks) < 5:
+        raise OracleError("malformed MatrixMarket header")
+    low = [t.lower() for t in toks]
+    if (low[1] != "matrix" or low[2] != "coordinate" or low[3] not in ("pattern", "integer")
+            or low[4] not in ("symmetric", "skew-symmetric", "general")):
+        raise OracleError("unsupported MatrixMarket header")
+    symmetric = low[4] != "general"
+    k = 1
+    while True:
+        if k >= len(lines):
+            raise OracleError("unexpected end before the size line")
+        t = lines[k].strip()
+        k += 1
+        if not t or t.startswith("%"):
+            continue
+        parts = t.split()
+        if len(parts) < 3:
+            raise OracleError("malformed size line")
+        nr, nc = _mtx_usize(parts[0]), _mtx_usize(parts[1])
+        _mtx_usize(parts[2])
+        if nr != nc:
+            raise OracleError("nrows != ncols")
+        n = nr
+        break
+    rows = [[] for _ in range(n)]
+    for line in lines[k:]:
+        t = line.strip()
+        if not t or t.startswith("%"):
+            continue
+        parts = t.split()
+        if len(parts) < 2:
+            continue
+        i1, j1 = _mtx_usize(parts[0]), _mtx_usize(parts[1])
+        if i1 == 0 or j1 == 0:
+            raise OracleError("MatrixMarket indices are 1-based")
+        i, j = i1 - 1, j1 - 1
+        if i >= n or j >= n:
+            raise OracleError("entry out of bounds")
+        rows[i].append(j)
+        if symmetric and i != j:
+            rows[j].append(i)
+    off = np.zeros(n + 1, dtype=np.uint64)
+    nbr = []
+    for u in range(n):
+        r = sorted(rows[u])
+        nbr.extend(r)
+        off[u + 1] = off[u] + len(r)
+    return off, np.asarray(nbr, dtype=np.uint64)
+
+
+def csr_to_mtx(offsets, neighbours, field: str = "pattern", comments: bool = True) -> bytes:
+    """A symmetric MatrixMarket text listing each undirected pair once per copy (i >= j, the
+    lower triangle), from which mtx_to_csr rebuilds the same CSR (test input)."""
+    off = np.asarray(offsets, dtype=np.int64)
+    nbr = np.asarray(neighbours, dtype=np.int64)
+    n = len(off) - 1
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+    low = src >= nbr
+    i, j = src[low] + 1, nbr[low] + 1
+    head = f"%%MatrixMarket matrix coordinate {field} symmetric\n"
+    if comments:
+        head += "% written by the oracle for a round-trip test\n%\n"
+    head += f"{n} {n} {i.shape[0]}\n"
+    if field == "integer":
+        body = "\n".join(f"{a} {b} 1" for a, b in zip(i.tolist(), j.tolist()))
+    else:
+        body = "\n".join(f"{a} {b}" for a, b in zip(i.tolist(), j.tolist()))
+    return (head + body + ("\n" if body else "")).encode()

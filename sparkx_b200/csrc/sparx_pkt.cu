@@ -3,6 +3,7 @@
 // device-resident peel loop (a CUDA graph with a conditional WHILE node whose
 // body is four wave kernels; the last block of each wave plans the next).
 #include <algorithm>
+#include <cctype>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -23,6 +24,7 @@
 
 #include "../../include/sparx_pkt.h"
 #include "pkt_kernels.cuh"
+#include "mtx_kernels.cuh"
 
 using namespace sparx;
 
@@ -1605,6 +1607,249 @@ int server_result(ServerReq* r, int* status, sparx_pkt_stats* stats) {
 
 }  // namespace
 
+namespace {
+
+// ---------------------------------------------------------------------------
+// MatrixMarket -> CSR (GraphCache::from_mtx_file, parser_mtx/mod.rs:34-162):
+// the header and size line are read on the host (parser_mtx/producers.rs:
+// 139-176: "%%MatrixMarket matrix coordinate pattern|integer
+// symmetric|skew-symmetric|general", comment lines skipped, nrows == ncols),
+// the body on the device (mtx_kernels.cuh).
+
+bool ieq(const std::string& a, const char* b) {
+  if (a.size() != std::strlen(b)) return false;
+  for (size_t i = 0; i < a.size(); ++i)
+    if (std::tolower((unsigned char)a[i]) != b[i]) return false;
+  return true;
+}
+
+std::vector<std::string> split_ws(const std::string& line) {
+  std::vector<std::string> t;
+  size_t i = 0;
+  auto ws = [](char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == 0x0B || c == 0x0C; };
+  while (i < line.size()) {
+    while (i < line.size() && ws(line[i])) ++i;
+    size_t j = i;
+    while (j < line.size() && !ws(line[j])) ++j;
+    if (j > i) t.push_back(line.substr(i, j - i));
+    i = j;
+  }
+  return t;
+}
+
+bool parse_usize(const std::string& t, uint64_t* out) {
+  size_t i = 0;
+  if (i < t.size() && t[i] == '+') ++i;
+  if (i >= t.size()) return false;
+  uint64_t v = 0;
+  for (; i < t.size(); ++i) {
+    const unsigned c = (unsigned char)t[i] - '0';
+    if (c > 9 || v > (~0ull - c) / 10) return false;
+    v = v * 10 + c;
+  }
+  *out = v;
+  return true;
+}
+
+struct MtxHeader {
+  uint64_t n = 0, nnz = 0, body = 0, header_lines = 0;
+  bool symmetric = true;
+};
+
+int mtx_header(const char* text, uint64_t len, MtxHeader* h) {
+  uint64_t p = 0, lines = 0;
+  auto next_line = [&](std::string* out) -> bool {
+    if (p >= len) return false;
+    uint64_t e = p;
+    while (e < len && text[e] != '\n') ++e;
+    out->assign(text + p, e - p);
+    p = e < len ? e + 1 : e;
+    ++lines;
+    return true;
+  };
+  std::string line;
+  if (!next_line(&line) || line.compare(0, 14, "%%MatrixMarket") != 0) {
+    set_error("invalid MatrixMarket header");
+    return SPARX_E_PARSE;
+  }
+  const auto tok = split_ws(line);
+  if (tok.size() < 5) { set_error("malformed MatrixMarket header"); return SPARX_E_PARSE; }
+  if (!ieq(tok[1], "matrix") || !ieq(tok[2], "coordinate") || !(ieq(tok[3], "pattern") || ieq(tok[3], "integer")) ||
+      !(ieq(tok[4], "symmetric") || ieq(tok[4], "skew-symmetric") || ieq(tok[4], "general"))) {
+    set_error("only 'matrix coordinate pattern/integer symmetric|skew-symmetric|general' is supported");
+    return SPARX_E_PARSE;
+  }
+  h->symmetric = !ieq(tok[4], "general");
+  for (;;) {
+    if (!next_line(&line)) { set_error("unexpected end of text before the size line"); return SPARX_E_PARSE; }
+    const auto t = split_ws(line);
+    if (t.empty() || t[0][0] == '%') continue;
+    uint64_t nr = 0, nc = 0, nnz = 0;
+    if (t.size() < 3 || !parse_usize(t[0], &nr) || !parse_usize(t[1], &nc) || !parse_usize(t[2], &nnz)) {
+      set_error("malformed size line");
+      return SPARX_E_PARSE;
+    }
+    if (nr != nc) { set_error("only square matrices are supported (nrows != ncols)"); return SPARX_E_PARSE; }
+    h->n = nr;
+    h->nnz = nnz;
+    break;
+  }
+  h->body = p;
+  h->header_lines = lines;
+  return SPARX_OK;
+}
+
+int mtx_to_csr(const char* text, uint64_t len, uint64_t* offsets_out, uint64_t offsets_cap,
+               uint64_t* neighbours_out, uint64_t neighbours_cap, uint64_t* n_out, uint64_t* width_out,
+               const sparx_pkt_opts* opts) {
+  g_last_error.clear();
+  if (!text || !n_out || !width_out) { set_error("null pointer"); return SPARX_E_ARG; }
+  MtxHeader H;
+  int rc = mtx_header(text, len, &H);
+  if (rc) return rc;
+  if (H.n >= 0xFFFFFFFFull) { set_error("more than 2^32 - 2 vertices"); return SPARX_E_TOO_LARGE; }
+  Opts O;
+  rc = read_opts(opts, &O);
+  if (rc) return rc;
+  Engine* Ep;
+  rc = get_engine(O.device, &Ep);
+  if (rc) return rc;
+  Engine& E = *Ep;
+  std::lock_guard<std::mutex> lk(E.mu);
+  CU(cudaSetDevice(E.device));
+  cudaStream_t s = E.stream;
+  const uint64_t blen = len - H.body;
+  const uint64_t chunks = (blen + 15) / 16;
+  // lines of the body (a line starts at byte 0 and after every '\n' but the last byte)
+  unsigned long long lines = 0;
+  if (blen) {
+    const char* bp = text + H.body;
+    long long nl = 0;
+#pragma omp parallel for reduction(+ : nl) schedule(static)
+    for (long long i = 0; i < (long long)blen - 1; ++i) nl += bp[i] == '\n';
+    lines = 1 + (unsigned long long)nl;
+  }
+  // one workspace: body, line starts and counts, keys (two per line at most,
+  // ping-pong), radix histograms, degrees, offsets and neighbours
+  size_t p = 0;
+  auto take = [&](size_t bytes) { size_t r = p; p = align_up(p + std::max<size_t>(bytes, 1)); return r; };
+  const uint64_t edges_max = 2 * lines;
+  const uint32_t rblocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(E.sm_count * 4ull,
+                                                                              (edges_max + 4095) / 4096));
+  const uint64_t scan_items = std::max<uint64_t>({chunks, lines, H.n, 256ull * rblocks, 1});
+  const size_t o_body = take(blen), o_cpref = take(8 * (chunks + 1)),
+               o_tiles = take(8 * ((scan_items + kScanTile - 1) / kScanTile + 2)), o_cnt = take(64),
+               o_starts = take(8 * lines), o_count = take(4 * lines), o_at = take(8 * (lines + 1)),
+               o_ka = take(8 * edges_max), o_kb = take(8 * edges_max), o_hist = take(4ull * 256 * rblocks),
+               o_start = take(4ull * 256 * rblocks + 4), o_deg = take(4 * (H.n + 1)), o_off = take(8 * (H.n + 1)),
+               o_nbr = take(8 * edges_max);
+  rc = ensure_ws(E, p);
+  if (rc) return rc;
+  unsigned char* body = at<unsigned char>(E, o_body);
+  unsigned long long* cpref = at<unsigned long long>(E, o_cpref);
+  unsigned long long* tiles = at<unsigned long long>(E, o_tiles);
+  unsigned long long* dcnt = at<unsigned long long>(E, o_cnt);  // [0] scan total, [1] first bad line
+  uint32_t* derr = (uint32_t*)(dcnt + 2);
+  // body -> device through the pinned staging buffers
+  for (uint64_t c = 0, a = 0; a < blen; ++c, a += kStageBytes) {
+    const int slot = (int)(c & 1);
+    const uint64_t k = std::min<uint64_t>(kStageBytes, blen - a);
+    CU(cudaEventSynchronize(E.pin_ev[slot]));
+    parallel_copy(E.pinned[slot], text + H.body + a, k);
+    CU(cudaMemcpyAsync(body + a, E.pinned[slot], k, cudaMemcpyHostToDevice, s));
+    CU(cudaEventRecord(E.pin_ev[slot], s));
+  }
+  CU(cudaMemsetAsync(dcnt, 0, 64, s));
+  CU(cudaMemsetAsync(dcnt + 1, 0xFF, 8, s));
+  if (chunks) {
+    unsigned long long dl = 0;
+    exclusive_scan<unsigned long long>(MtxLineCount{body, blen}, chunks, cpref, tiles, dcnt, s);
+    CU(cudaMemcpyAsync(&dl, cpref + chunks, 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (dl != lines) { set_error("line count mismatch"); return SPARX_E_CUDA; }
+  }
+  unsigned long long* starts = at<unsigned long long>(E, o_starts);
+  uint32_t* count = at<uint32_t>(E, o_count);
+  unsigned long long* atp = at<unsigned long long>(E, o_at);
+  const int pgrid = grid_for(lines, 256, E.sm_count * 16);
+  if (lines) {
+    k_mtx_fill_lines<<<grid_for(chunks, 256, E.sm_count * 16), 256, 0, s>>>(body, blen, cpref, starts);
+    k_mtx_parse<false><<<pgrid, 256, 0, s>>>(body, blen, starts, lines, H.n, H.symmetric, count, nullptr, nullptr,
+                                             derr, dcnt + 1);
+  }
+  uint32_t herr = 0;
+  unsigned long long bad = 0, edges = 0;
+  CU(cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(&bad, dcnt + 1, 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (herr) {
+    const char* what = (herr & kMtxBadNumber) ? "an index that is not an unsigned integer"
+                       : (herr & kMtxZeroIndex) ? "an index of 0 (MatrixMarket indices are 1-based)"
+                                                : "an index beyond the size line";
+    set_error(std::string("line ") + std::to_string(H.header_lines + bad + 1) + ": " + what);
+    return SPARX_E_PARSE;
+  }
+  if (lines) {
+    exclusive_scan<unsigned long long>(LoadCount{count}, lines, atp, tiles, dcnt, s);
+    CU(cudaMemcpyAsync(&edges, atp + lines, 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+  }
+  if (edges >= 0xFFFFFFFFull) { set_error("more than 2^32 - 2 entries after mirroring"); return SPARX_E_TOO_LARGE; }
+  *n_out = H.n;
+  *width_out = edges;
+  if (!offsets_out || !neighbours_out) return SPARX_OK;  // sizes only
+  if (offsets_cap < H.n + 1 || neighbours_cap < edges) {
+    set_error("output buffers too small (need n + 1 offsets and width neighbours)");
+    return SPARX_E_ARG;
+  }
+  unsigned long long* ka = at<unsigned long long>(E, o_ka);
+  unsigned long long* kb = at<unsigned long long>(E, o_kb);
+  uint32_t* hist = at<uint32_t>(E, o_hist);
+  uint32_t* hstart = at<uint32_t>(E, o_start);
+  uint32_t* deg = at<uint32_t>(E, o_deg);
+  unsigned long long* doff = at<unsigned long long>(E, o_off);
+  unsigned long long* dnbr = at<unsigned long long>(E, o_nbr);
+  if (lines)
+    k_mtx_parse<true><<<pgrid, 256, 0, s>>>(body, blen, starts, lines, H.n, H.symmetric, nullptr, atp, ka, derr,
+                                            dcnt + 1);
+  // sort by (row, column): the low 32 bits (columns), then the high (rows),
+  // only the bits that vertex ids < n use
+  const int bits = H.n > 1 ? 64 - __builtin_clzll(H.n - 1) : 1;
+  std::vector<int> shifts;
+  for (int b = 0; b < bits; b += 8) shifts.push_back(b);
+  for (int b = 0; b < bits; b += 8) shifts.push_back(32 + b);
+  const uint32_t blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(rblocks, (edges + 4095) / 4096));
+  unsigned long long *src = ka, *dst = kb;
+  if (edges > 1) {
+    for (int sh : shifts) {
+      k_radix_hist<<<blocks, kRadixThreads, 0, s>>>(src, edges, sh, hist);
+      exclusive_scan<uint32_t>(LoadU32{hist}, 256ull * blocks, hstart, (uint32_t*)tiles, (uint32_t*)dcnt, s);
+      k_radix_scatter<<<blocks, kRadixThreads, 0, s>>>(src, dst, edges, sh, hstart);
+      std::swap(src, dst);
+    }
+  }
+  CU(cudaMemsetAsync(deg, 0, 4 * (H.n + 1), s));
+  if (edges) k_mtx_rows<<<grid_for(edges, 256, E.sm_count * 16), 256, 0, s>>>(src, edges, deg);
+  exclusive_scan<unsigned long long>(LoadCount{deg}, H.n, doff, tiles, dcnt, s);
+  if (edges) k_mtx_columns<<<grid_for(edges, 256, E.sm_count * 16), 256, 0, s>>>(src, edges, dnbr);
+  if (H.n == 0) CU(cudaMemsetAsync(doff, 0, 8, s));
+  rc = download(E, offsets_out, doff, 8 * (H.n + 1), s);
+  if (rc) return rc;
+  rc = download(E, neighbours_out, dnbr, 8 * edges, s);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s));
+  CU(cudaGetLastError());
+  return SPARX_OK;
+}
+
+}  // namespace
+
+extern "C" int sparx_mtx_to_csr(const char* text, uint64_t len, uint64_t* offsets_out, uint64_t offsets_cap,
+                                uint64_t* neighbours_out, uint64_t neighbours_cap, uint64_t* n_out,
+                                uint64_t* width_out, const sparx_pkt_opts* opts) {
+  return mtx_to_csr(text, len, offsets_out, offsets_cap, neighbours_out, neighbours_cap, n_out, width_out, opts);
+}
+
 extern "C" {
 
 int sparx_pkt_run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t hbm_budget_bytes,
@@ -1993,6 +2238,7 @@ const char* sparx_strerror(int s) {
     case SPARX_E_ARG: return "bad argument";
     case SPARX_E_NOT_FOUND: return "unknown ticket";
     case SPARX_E_CANCELLED: return "request cancelled";
+    case SPARX_E_PARSE: return "malformed MatrixMarket text";
     default: return "unknown status";
   }
 }

@@ -49,6 +49,16 @@ class GraphMemoryMap:
         return cls.from_arrays(csr.offsets, csr.neighbours, thread_count, csr.name or None)
 
     @classmethod
+    def from_mtx_file(cls, path: str, thread_count: int = 1, device: int = -1):
+        """Build the CSR from a MatrixMarket file on the GPU, as ``GraphCache::from_mtx_file``
+        builds its cache (``graph/cache/parser_mtx/mod.rs:34-162``): see ``mtx_to_csr``."""
+        from .pkt import mtx_to_csr
+        with open(path, "rb") as f:
+            data = f.read()
+        off, nbr = mtx_to_csr(data, device=device)
+        return cls(off, nbr, thread_count, os.path.basename(path), path)
+
+    @classmethod
     def open(cls, offsets_path: str, neighbours_path: str, thread_count: int = 1):
         """Map an existing cache entry (raw u64 offsets file + raw u64 neighbours file)."""
         off = np.memmap(offsets_path, dtype=np.uint64, mode="r")

@@ -38,6 +38,7 @@ E_TOO_LARGE = 7
 E_ARG = 8
 E_NOT_FOUND = 9
 E_CANCELLED = 10
+E_PARSE = 11
 
 SUPPORT_WIDE = 0
 SUPPORT_U8 = 1
@@ -130,6 +131,8 @@ def lib():
     if hasattr(L, "sparx_pkt_run_batch"):
         L.sparx_pkt_run_batch.restype = i32
         L.sparx_pkt_run_batch.argtypes = [P(_GraphView), u64, u64, P(_Opts), P(ctypes.c_int), P(_Stats)]
+    L.sparx_mtx_to_csr.restype = i32
+    L.sparx_mtx_to_csr.argtypes = [ctypes.c_char_p, u64, vp, u64, vp, u64, P(u64), P(u64), P(_Opts)]
     key3 = P(ctypes.c_uint32)
     for name, args in (("sparx_tuning_default", [P(_Tuning)]),
                        ("sparx_tuning_signature", [vp, u64, key3]),
@@ -634,3 +637,21 @@ def autotune_batch(graphs, opts: PktOptions | None = None, repeats: int = 3,
     _check(lib().sparx_autotune_batch(views, len(graphs), hbm_budget_bytes, ctypes.byref(o), repeats,
                                       ctypes.byref(t), k))
     return PktTuning.from_c(t), tuple(k)
+
+
+# ---- input ------------------------------------------------------------------------------------
+
+def mtx_to_csr(data: bytes, device: int = -1):
+    """MatrixMarket text -> (offsets u64[n+1], neighbours u64[width]) on the GPU, with the
+    semantics of ``GraphCache::from_mtx_file`` (parser_mtx/mod.rs:34-162, producers.rs:139-240,
+    impl_sort.rs:10-51): entries mirrored unless the header says ``general``, duplicates kept,
+    rows sorted.  Raises PktError(E_PARSE) on malformed text."""
+    L = lib()
+    o = PktOptions(device=device).c()
+    n, w = ctypes.c_uint64(), ctypes.c_uint64()
+    _check(L.sparx_mtx_to_csr(data, len(data), None, 0, None, 0, ctypes.byref(n), ctypes.byref(w), ctypes.byref(o)))
+    off = np.empty(n.value + 1, dtype=np.uint64)
+    nbr = np.empty(max(w.value, 1), dtype=np.uint64)
+    _check(L.sparx_mtx_to_csr(data, len(data), off.ctypes.data, off.shape[0], nbr.ctypes.data, nbr.shape[0],
+                              ctypes.byref(n), ctypes.byref(w), ctypes.byref(o)))
+    return off, nbr[: w.value]
