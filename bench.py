@@ -301,6 +301,7 @@ def run_serve(args):
                 assert r.status == 0
                 lat[i] = r.latency_ms
             span = time.perf_counter() - t0
+            info = srv.info()
         # plain: one call at a time in arrival order (FIFO, single stream)
         plain_lat = []
         t0 = time.perf_counter()
@@ -316,13 +317,15 @@ def run_serve(args):
         rows.append({"rate_per_s": rate, "served_graphs_per_s": n / span, "plain_graphs_per_s": n / span_plain,
                      "served_p50_ms": float(np.percentile(lat, 50)), "served_p99_ms": float(np.percentile(lat, 99)),
                      "plain_p50_ms": float(np.percentile(plain_lat, 50)),
-                     "plain_p99_ms": float(np.percentile(plain_lat, 99))})
+                     "plain_p99_ms": float(np.percentile(plain_lat, 99)),
+                     "served_unions": info["unions"], "joined_running_union": info["joined"]})
         log(json.dumps(rows[-1]))
     out = {"metric": "PKT served stream latency/throughput", "n_requests": n, "tail_rmat24": bool(args.tail),
            "rows": rows,
            "config": {"workload": f"{n} requests: first {args.mix_count} members of the config-4 mix"
                                   + (" + 1% R-MAT-24 tail" if args.tail else "") + ", Poisson arrivals",
-                      "budget": "150 GB (4 lanes)"}}
+                      "budget": "150 GB (4 lanes: one of 75 GB, three of 25 GB; requests join running "
+                                "unions at wave boundaries and leave when their own peel ends)"}}
     print(json.dumps(out), flush=True)
     return 0
 

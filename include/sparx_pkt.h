@@ -305,8 +305,16 @@ int sparx_autotune_batch(const sparx_graph_view* graphs, uint64_t count, uint64_
 typedef struct sparx_server sparx_server;
 
 /* Create a server on opts->device with an HBM budget (0 = 150 GB, capped at the
- * device's free memory).  The budget is split over 4 execution lanes; a request
- * needing more than one lane's share completes with SPARX_E_OOM.  Requests stay
+ * device's free memory).  Requests run on 4 execution lanes (the environment
+ * variable SPARX_SERVE_LANES, 1..16, changes the count), each on its own
+ * stream: lane 0 holds half the budget (a large graph fits there), the others
+ * share the rest, and each keeps a fifth of its share to prepare requests that
+ * join it.  An idle lane packs the queued requests that fit into a union sized
+ * to its share; while that union's peel runs, a submitted request stops it at
+ * its next wave, and the requests that fit join the union there (prepared on
+ * the lane's second engine and placed behind the running members); every
+ * member's result goes back as soon as its own peel ends.  A request needing
+ * more than any lane holds completes with SPARX_E_OOM.  Requests stay
  * addressable by ticket until sparx_server_destroy. */
 int sparx_server_create(sparx_server** out, uint64_t hbm_budget_bytes, const sparx_pkt_opts* opts);
 
@@ -324,6 +332,9 @@ int sparx_server_wait(sparx_server* s, uint64_t ticket, uint64_t timeout_ms, int
 
 /* Cancel a queued (not yet admitted) request. */
 int sparx_server_cancel(sparx_server* s, uint64_t ticket);
+
+/* Served unions started, and requests that joined a union already running. */
+int sparx_server_info(sparx_server* s, uint64_t* unions, uint64_t* joined);
 
 /* Drain and free. */
 int sparx_server_destroy(sparx_server* s);

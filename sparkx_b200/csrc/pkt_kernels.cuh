@@ -182,9 +182,15 @@ struct Control {
   // a frontier step, members in a scan}; nullptr = off
   ulonglong4* trace;
   unsigned long long trace_cap;
+  // served unions: stop when a member finishes (its result can go out at
+  // once), and when the host-mapped word `admit` is set (requests wait to
+  // join); nullptr / 0 = off
+  const volatile uint32_t* admit;
+  uint32_t notify_done;
+  uint32_t pad1;
 };
 
-enum : uint32_t { kExitNone = 0, kExitDone = 1, kExitCompact = 2, kExitError = 3 };
+enum : uint32_t { kExitNone = 0, kExitDone = 1, kExitCompact = 2, kExitError = 3, kExitMember = 4, kExitAdmit = 5 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -1132,16 +1138,18 @@ __device__ __forceinline__ void flush_member_stats(uint32_t g, unsigned long lon
 
 // Multigraphs (mu != nullptr): a pair's support is per copy, so its triangle
 // credits are support * mu; a support that wrapped past 2^31 is a capacity error.
+// Edges [e_begin, m): all of them, or those of members that join a served union.
 __global__ void __launch_bounds__(256) k_peel_setup(const Union* __restrict__ Up, const Member* __restrict__ mem,
                                                     int u8mode, unsigned long long* __restrict__ mem_tri,
                                                     uint32_t* __restrict__ mem_maxsup,
-                                                    const uint32_t* __restrict__ mu, uint32_t* __restrict__ err) {
+                                                    const uint32_t* __restrict__ mu, uint32_t* __restrict__ err,
+                                                    uint32_t e_begin = 0) {
   const Union U = *Up;
   const uint32_t G = U.G;
   uint32_t cur = kInvalid;
   unsigned long long sum = 0;
   uint32_t mx = 0;
-  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < U.m; e += gridDim.x * blockDim.x) {
+  for (uint32_t e = e_begin + blockIdx.x * blockDim.x + threadIdx.x; e < U.m; e += gridDim.x * blockDim.x) {
     uint32_t g = 0;
     if (G > 1) {
       uint32_t lo = 0, hi = G - 1;
@@ -1421,6 +1429,7 @@ __device__ __forceinline__ MemberState load_state_cg(const MemberState* p) {
 struct PlanShared {
   unsigned long long sw[32];
   uint32_t live;
+  uint32_t newly_done;  // members that finished in this wave
   unsigned long long proc, scan, edges, live_edges;
 };
 
@@ -1435,7 +1444,7 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
   uint32_t& s_live = ps.live;
   unsigned long long &s_proc = ps.proc, &s_scan = ps.scan, &s_edges = ps.edges, &s_live_edges = ps.live_edges;
   const uint32_t G = ctl->G;
-  if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; s_live_edges = 0; }
+  if (threadIdx.x == 0) { s_live = 0; s_proc = 0; s_scan = 0; s_edges = 0; s_live_edges = 0; ps.newly_done = 0; }
   __syncthreads();
   const bool was_done = ctl->done;
   if (was_done) {
@@ -1451,6 +1460,7 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
     if (g < G && !was_done) {
       MemberState s = load_state_cg(st + g);
       const uint32_t m = mem[g].m;
+      const uint32_t phase_before = s.phase;
       switch (s.phase) {
         case kPhaseScan0:
           s.act_sel ^= 1u;
@@ -1497,6 +1507,7 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
           break;
       }
       if (s.phase != kPhaseDone) s.waves++;
+      else if (phase_before != kPhaseDone) atomicAdd(&ps.newly_done, 1u);
       st[g] = s;
       if (s.phase == kPhaseScan0 || s.phase == kPhaseScan) {
         w = s.act_count;
@@ -1544,6 +1555,8 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
         done = 1;
         reason = kExitCompact;
       }
+      if (!done && ctl->notify_done && ps.newly_done) { done = 1; reason = kExitMember; }
+      if (!done && ctl->admit && *ctl->admit) { done = 1; reason = kExitAdmit; }
       ctl->done = done;
       ctl->exit_reason = reason;
     }
@@ -2261,6 +2274,156 @@ __global__ void __launch_bounds__(256) k_kcore_peel(const uint32_t* __restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// The k-core level loop on the device: one wave kernel runs either the scan of
+// level k (live vertices of degree <= k join the frontier, the smallest degree
+// left is recorded) or one sub-level (a warp per frontier vertex, as
+// k_kcore_peel); the last block of each wave advances the state (the next
+// sub-level, the next level, or a jump past empty levels to the smallest degree
+// left) and sets the CUDA-graph loop condition.  Bounded by a wave count and
+// the device clock, like the PKT peel.
+struct KcState {
+  uint32_t phase;        // 0 scan, 1 sub-level, 2 done
+  uint32_t k;
+  uint32_t count;        // frontier size of the sub-level to run
+  uint32_t next_count;   // wave accumulator: frontier being built
+  uint32_t min_left;     // wave accumulator (scan): smallest degree above k
+  uint32_t sel;          // queue holding the frontier
+  uint32_t levels, subs, kmax;
+  uint32_t blocks_done;
+  uint32_t err;
+  uint32_t pad;
+  unsigned long long remaining;  // live vertices
+  unsigned long long waves_run, max_waves, t_start, timeout_ns;
+};
+
+__global__ void k_kcore_start(KcState* st, unsigned long long max_waves, unsigned long long timeout_ns) {
+  st->phase = st->remaining ? 0u : 2u;
+  st->k = 1;
+  st->count = 0;
+  st->next_count = 0;
+  st->min_left = 0xFFFFFFFFu;
+  st->sel = 0;
+  st->max_waves = max_waves;
+  st->timeout_ns = timeout_ns;
+  st->t_start = globaltimer();
+}
+
+__global__ void __launch_bounds__(256) k_kcore_wave(const uint32_t* __restrict__ off,
+                                                    const uint32_t* __restrict__ nbr, uint32_t n,
+                                                    uint32_t* __restrict__ deg, uint32_t* __restrict__ alive,
+                                                    uint32_t* __restrict__ core, uint32_t* __restrict__ q0,
+                                                    uint32_t* __restrict__ q1, KcState* st,
+                                                    cudaGraphConditionalHandle handle, int use_handle) {
+  const uint32_t phase = st->phase, k = st->k, sel = st->sel, count = st->count;
+  const uint32_t lane = lane_id();
+  if (phase == 0) {
+    uint32_t* frontier = sel ? q1 : q0;
+    uint32_t mn = 0xFFFFFFFFu;
+    for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; b < n; b += gridDim.x * blockDim.x) {
+      const uint32_t u = b + lane;
+      bool take = false;
+      if (u < n && alive[u]) {
+        const uint32_t d = deg[u];
+        if (d <= k) {
+          take = true;
+          alive[u] = 0;
+        } else {
+          mn = min(mn, d);
+        }
+      }
+      const unsigned bal = __ballot_sync(kFull, take);
+      if (bal) {
+        uint32_t at = 0;
+        if (lane == 0) at = atomicAdd(&st->next_count, (uint32_t)__popc(bal));
+        at = __shfl_sync(kFull, at, 0);
+        if (take) frontier[at + __popc(bal & ((1u << lane) - 1))] = u;
+      }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
+    if (lane == 0 && mn != 0xFFFFFFFFu) atomicMin(&st->min_left, mn);
+  } else if (phase == 1) {
+    const uint32_t* frontier = sel ? q1 : q0;
+    uint32_t* next = sel ? q0 : q1;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = warp; i < count; i += nwarps) {
+      const uint32_t u = frontier[i];
+      if (lane == 0) core[u] = k;
+      const uint32_t b = __ldg(off + u), e = __ldg(off + u + 1);
+      for (uint32_t s0 = b; s0 < e; s0 += 32) {
+        const uint32_t s = s0 + lane;
+        bool push = false;
+        uint32_t v = 0;
+        if (s < e) {
+          v = __ldg(nbr + s);
+          uint32_t x = *(volatile uint32_t*)(deg + v);
+          while (x > k) {
+            const uint32_t old = atomicCAS(deg + v, x, x - 1);
+            if (old == x) {
+              push = x == k + 1 && atomicExch(alive + v, 0u) == 1u;
+              break;
+            }
+            x = old;
+          }
+        }
+        const unsigned bal = __ballot_sync(kFull, push);
+        if (bal) {
+          uint32_t at = 0;
+          if (lane == 0) at = atomicAdd(&st->next_count, (uint32_t)__popc(bal));
+          at = __shfl_sync(kFull, at, 0);
+          if (push) next[at + __popc(bal & ((1u << lane) - 1))] = v;
+        }
+      }
+    }
+  }
+  // the last block to finish plans the next wave
+  __shared__ uint32_t s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st->blocks_done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  st->blocks_done = 0;
+  uint32_t done = phase == 2;
+  if (!done) {
+    const uint32_t found = *(volatile uint32_t*)&st->next_count;
+    if (phase == 0) {
+      if (found) {
+        st->count = found;
+        st->phase = 1;
+        st->levels += 1;
+        st->kmax = k;
+      } else {
+        const uint32_t ml = *(volatile uint32_t*)&st->min_left;
+        if (ml == 0xFFFFFFFFu) { st->err |= kErrInternal; done = 1; }  // live vertices, none found
+        else st->k = max(k + 1, ml);
+      }
+    } else {
+      st->remaining -= min(st->remaining, (unsigned long long)count);
+      st->subs += 1;
+      if (found) {
+        st->count = found;
+        st->sel = sel ^ 1u;
+      } else {
+        st->count = 0;
+        st->k = k + 1;
+        st->phase = 0;
+      }
+    }
+    st->next_count = 0;
+    st->min_left = 0xFFFFFFFFu;
+    st->waves_run += 1;
+    if (st->remaining == 0 && st->phase == 0) done = 1;
+    if (st->waves_run > st->max_waves) { st->err |= kErrWaves; done = 1; }
+    if (globaltimer() - st->t_start > st->timeout_ns) { st->err |= kErrTimeout; done = 1; }
+    if (done) st->phase = 2;
+  }
+  if (use_handle) cudaGraphSetConditional(handle, done ? 0u : 1u);
+}
+
 template <typename OutT>
 __global__ void k_kcore_out(const uint32_t* __restrict__ core, uint32_t n, OutT* __restrict__ out) {
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
@@ -2433,6 +2596,84 @@ __global__ void __launch_bounds__(256) k_mult_check(const unsigned long long* __
     if (e != kInvalid && __ldg(owner + s) != kInvalid) bad |= __ldg(mu + e) != __ldg(mult2 + s);
   }
   if (bad) atomicOr(err, kErrAsym);
+}
+
+// ---------------------------------------------------------------------------
+// Served unions: members join a running peel between graph launches.  Their
+// graphs are prepared (narrowed, oriented, supported) as a union of their own,
+// then copied behind the running union's vertices, slots and edge ids with
+// the ids shifted; their states start at the level-0 scan.
+__global__ void k_shift_u32(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                            unsigned long long count, uint32_t add) {
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    dst[i] = src[i] + add;
+}
+
+// row pairs (id | edge id << 32): id + id_add, edge id + eid_add (self-loops keep kInvalid)
+__global__ void k_shift_pairs(unsigned long long* __restrict__ dst, const unsigned long long* __restrict__ src,
+                              unsigned long long count, uint32_t id_add, uint32_t eid_add) {
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long pr = src[i];
+    const uint32_t id = (uint32_t)pr + id_add, e = (uint32_t)(pr >> 32);
+    dst[i] = make_pair(id, e == kInvalid ? kInvalid : e + eid_add);
+  }
+}
+
+// rows longer than kWarpRow among vertices [v0, v1), appended to the list
+__global__ void __launch_bounds__(256) k_big_rows_range(const uint32_t* __restrict__ off0, uint32_t v0, uint32_t v1,
+                                                        uint32_t* __restrict__ list, uint32_t* __restrict__ count) {
+  for (uint32_t u = v0 + blockIdx.x * blockDim.x + threadIdx.x; u < v1; u += gridDim.x * blockDim.x)
+    if (big_row(off0, u)) list[atomicAdd(count, 1u)] = u;
+}
+
+// new members' states (the first wave of a member is its level-0 scan)
+__global__ void k_member_init(const Member* __restrict__ mem, MemberState* __restrict__ st, uint32_t g0,
+                              uint32_t g1) {
+  for (uint32_t g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < g1; g += gridDim.x * blockDim.x) {
+    MemberState s{};
+    s.phase = mem[g].m ? kPhaseScan0 : kPhaseDone;
+    s.act_count = mem[g].m;
+    s.min_kept = 0xFFFFFFFFu;
+    st[g] = s;
+  }
+}
+
+// members joined: the union's member count, wave bound and working-row size grow
+__global__ void k_ctl_join(Control* ctl, uint32_t G, unsigned long long add_waves, unsigned long long add_slots) {
+  ctl->G = G;
+  ctl->max_waves += add_waves;
+  ctl->csr_slots += add_slots;
+}
+
+// One block: the pending wave's layout again (after members joined), no state
+// transitions; restarts the time budget and the loop.
+__global__ void k_replan(const Member* __restrict__ mem, const MemberState* __restrict__ st, Control* ctl,
+                         unsigned long long* __restrict__ wpref) {
+  __shared__ unsigned long long sw[32];
+  const uint32_t G = ctl->G;
+  unsigned long long carry = 0;
+  for (uint32_t b = 0; b < G; b += blockDim.x) {
+    const uint32_t g = b + threadIdx.x;
+    unsigned long long w = 0;
+    if (g < G) {
+      const MemberState s = st[g];
+      if (s.phase == kPhaseScan0 || s.phase == kPhaseScan) w = s.act_count;
+      else if (s.phase == kPhaseProc) w = s.curr & kWorkMask;
+    }
+    unsigned long long total;
+    const unsigned long long ex = block_exclusive_scan<unsigned long long>(w, sw, total);
+    if (g < G) wpref[g] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) {
+    wpref[G] = carry;
+    ctl->total_work = carry;
+    ctl->t_start = globaltimer();
+    ctl->done = 0;
+    ctl->exit_reason = kExitNone;
+  }
 }
 
 }  // namespace sparx

@@ -167,6 +167,7 @@ struct Counters {  // device scalars
   uint32_t heavy_count;  //                      heavy vertices listed
   uint32_t hub_count;    // hub maps assigned
   uint32_t big_count;    // rows compacted by a block each
+  uint32_t fin_err;      // served unions: error flags of one member's finalize
   double cc_possible;    // clustering: sum of d(d - 1)/2 over vertices
   double cc_local;       //             sum of local coefficients
   unsigned long long cc_slots;  //      sum of slot supports
@@ -327,7 +328,7 @@ int get_engine(int device, Engine** out) {
   return SPARX_OK;
 }
 
-int ensure_ws(Engine& E, size_t bytes) {
+int ensure_ws(Engine& E, size_t bytes, bool slack = true) {
   if (E.ws_cap >= bytes) return SPARX_OK;
   if (E.peel.exec) {
     cudaGraphExecDestroy(E.peel.exec);
@@ -335,7 +336,7 @@ int ensure_ws(Engine& E, size_t bytes) {
     E.peel = PeelGraph{};
   }
   if (E.ws) { CU(cudaStreamSynchronize(E.stream)); CU(cudaFree(E.ws)); E.ws = nullptr; E.ws_cap = 0; }
-  size_t cap = align_up(bytes + bytes / 8, 1 << 21);
+  size_t cap = align_up(slack ? bytes + bytes / 8 : bytes, 1 << 21);
   cudaError_t e = cudaMalloc(&E.ws, cap);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -517,8 +518,34 @@ int read_opts(const sparx_pkt_opts* o, Opts* out) {
 }
 
 // A prepared launch: members laid out in one union, CSR already on device.
+struct UnionJob;
+struct Engine;
+// The peel loop's state a served union's hook may change between launches.
+struct PeelCtx {
+  Union U;                        // host copy (working rows, counts)
+  const uint32_t* cur_off;        // working rows in use
+  const unsigned long long* cur_row;
+  unsigned long long csr_slots;   // entries in the working rows
+  uint64_t m;                     // edges in the union
+  uint64_t Ws;                    // slots in the union
+  uint32_t N, G;
+  bool resume = false;            // the hook added members or some are still running
+};
+// Served unions: called at every stop of the peel loop (a member finished,
+// requests wait to join, a compaction, the end); delivers finished members
+// and may append new ones.
+struct ServeHook {
+  virtual ~ServeHook() = default;
+  virtual int at_stop(Engine& E, UnionJob& J, PeelCtx& ctx, uint32_t reason, cudaStream_t s) = 0;
+  const volatile uint32_t* admit_dev = nullptr;  // device view of the lane's admission word
+};
+
 struct UnionJob {
   uint64_t N = 0, W = 0;
+  ServeHook* hook = nullptr;     // served union (members join and leave between graph launches)
+  bool prep_only = false;        // stop after the support pass (members about to join a served union)
+  const uint32_t* smap = nullptr;  // multigraphs: caller slot -> deduplicated slot (device)
+  uint64_t prep_m = 0, prep_Ws = 0;  // prep_only: edges and slots prepared
   std::vector<Member> members;  // vb, n, sb, w set; eb, m filled by the pipeline
   Layout L{};
   uint32_t* off = nullptr;
@@ -721,6 +748,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     Ws = ws32;
     J.off = off2;
     J.nbr = nbr2;
+    J.smap = smap;
   }
   J.self_loops = hc.self_loops;
   if (hc.err) { J.err = hc.err; return status_from_flags(hc.err); }
@@ -796,6 +824,12 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   }
   CU(cudaEventRecord(E.tev[3], s));
 
+  if (J.prep_only) {
+    J.prep_m = m;
+    J.prep_Ws = Ws;
+    CU(cudaStreamSynchronize(s));
+    return J.multi ? SPARX_E_MULTIGRAPH : SPARX_OK;
+  }
   if (J.support_only && J.clustering) {
     k_clustering<<<vgrid, 256, 0, s>>>(J.off, row0, es, N, O.support_mode == SPARX_SUPPORT_U8, (double*)J.out,
                                        &cnt->cc_possible, &cnt->cc_local, &cnt->cc_slots, mult2);
@@ -840,6 +874,10 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     c0.csr_slots = Ws;
     c0.compact_min = kCompactMinSlots;
     c0.compact_pct = T.compact_pct;
+    if (J.hook) {
+      c0.notify_done = 1;
+      c0.admit = J.hook->admit_dev;
+    }
     // wave trace: when SPARX_TRACE_FILE names a file, the planner records
     // each wave's start time and work there (first 2^20 waves)
     const char* trace_path = std::getenv("SPARX_TRACE_FILE");
@@ -863,6 +901,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     wa.arr = peel_arrays(U);
     wa.arr.mu = mu;
     wa.arr.merge_ratio = T.merge_ratio;
+    if (J.hook) wa.arr.n = 0;  // unused by the kernels; a constant keeps the graph across joins
     wa.mem = dmem;
     wa.st = at<MemberState>(E, L.st);
     wa.ctl = at<Control>(E, L.ctl);
@@ -874,6 +913,31 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     const uint32_t* cur_off = J.off;
     const unsigned long long* cur_row = row0;
     int next_buf = 0;
+    // counts a served union's joins change (the rest of the pipeline is done)
+    uint32_t pN = N, pG = G;
+    uint64_t pm = m, pWs = Ws;
+    auto serve_stop = [&](uint32_t reason, bool* resume) -> int {
+      PeelCtx ctx;
+      ctx.U = U;
+      ctx.U.off = cur_off;
+      ctx.U.row = cur_row;
+      ctx.cur_off = cur_off;
+      ctx.cur_row = cur_row;
+      ctx.csr_slots = hctl->csr_slots;
+      ctx.m = pm;
+      ctx.Ws = pWs;
+      ctx.N = pN;
+      ctx.G = pG;
+      int rc = J.hook->at_stop(E, J, ctx, reason, s);
+      if (rc) return rc;
+      U = ctx.U;
+      pm = ctx.m;
+      pWs = ctx.Ws;
+      pN = ctx.N;
+      pG = ctx.G;
+      *resume = ctx.resume;
+      return SPARX_OK;
+    };
     for (;;) {
       if (O.loop == SPARX_LOOP_GRAPH) {
         int rc = build_peel_graph(E, J, wa.arr);
@@ -893,26 +957,47 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
           if (hctl->done) break;
         }
       }
+      if (J.hook && hctl->exit_reason != kExitCompact && hctl->exit_reason != kExitError) {
+        bool resume = false;
+        const int r = serve_stop(hctl->exit_reason, &resume);
+        if (r) return r;
+        if (!resume) break;
+        k_replan<<<1, 1024, 0, s>>>(dmem, at<MemberState>(E, L.st), wa.ctl, wa.wpref);
+        J.launches += 1;
+        continue;
+      }
       if (hctl->exit_reason != kExitCompact) break;
       // drop processed edges from the working rows, then resume the loop
       uint32_t* off2 = at<uint32_t>(E, next_buf ? L.offB : L.offA);
       unsigned long long* row2 = at<unsigned long long>(E, next_buf ? L.rowB : L.rowA);
       uint32_t* alive = at<uint32_t>(E, L.alive);
-      k_compact_mark<<<grid_for((m + 31) / 32 * 32ull, 256, E.sm_count * 16), 256, 0, s>>>(es, (uint32_t)m,
-                                                                                          wa.ctl, alive);
-      k_compact_count<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, dplus, J.off);
+      const int pvgrid = grid_for(pN, 256, E.sm_count * 32);
+      k_compact_mark<<<grid_for((pm + 31) / 32 * 32ull, 256, E.sm_count * 16), 256, 0, s>>>(es, (uint32_t)pm,
+                                                                                           wa.ctl, alive);
+      k_compact_count<<<pvgrid, 256, 0, s>>>(cur_off, cur_row, pN, alive, dplus, J.off);
       k_compact_count_big<<<E.sm_count * 2, 1024, 0, s>>>(cur_off, cur_row, alive, dplus, big, &cnt->big_count);
-      exclusive_scan<uint32_t>(LoadU32{dplus}, N, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
-      k_compact_fill<<<vgrid, 256, 0, s>>>(cur_off, cur_row, N, alive, off2, row2, J.off);
+      exclusive_scan<uint32_t>(LoadU32{dplus}, pN, off2, at<uint32_t>(E, L.tiles), (uint32_t*)&cnt->grand, s);
+      k_compact_fill<<<pvgrid, 256, 0, s>>>(cur_off, cur_row, pN, alive, off2, row2, J.off);
       k_compact_fill_big<<<E.sm_count * 2, 1024, 0, s>>>(cur_off, cur_row, alive, off2, row2, big,
                                                          &cnt->big_count);
-      k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + N, wa.ctl);
-      const uint32_t per = std::max<uint32_t>(1, (uint32_t)(E.sm_count * 8) / std::max<uint32_t>(G, 1));
-      k_refresh_desc<<<G * per, 256, 0, s>>>(wa.Up, dmem, wa.st, G, per);
+      k_compact_commit<<<1, 1, 0, s>>>(at<Union>(E, L.uni), off2, row2, off2 + pN, wa.ctl);
+      const uint32_t per = std::max<uint32_t>(1, (uint32_t)(E.sm_count * 8) / std::max<uint32_t>(pG, 1));
+      k_refresh_desc<<<pG * per, 256, 0, s>>>(wa.Up, dmem, wa.st, pG, per);
       J.launches += 8;
       cur_off = off2;
       cur_row = row2;
+      U.off = off2;
+      U.row = row2;
       next_buf ^= 1;
+    }
+    if (J.hook) {
+      // every member went out through the hook
+      CU(cudaEventRecord(E.tev[5], s));
+      CU(cudaEventRecord(E.tev[6], s));
+      CU(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+      J.err = hc.err;
+      return status_from_flags(hc.err);
     }
     CU(cudaEventRecord(E.tev[5], s));
     // -- finalize (Kernel E) --
@@ -1043,13 +1128,15 @@ Layout make_kcore_layout(uint64_t N, uint64_t W, size_t out_bytes) {
   L.stage0 = take(kStageBytes);
   L.stage1 = take(kStageBytes);
   L.cnt = take(sizeof(Counters));
-  L.tiles = take(64);     // scan counters: count, next count, smallest degree left, remaining
+  L.tiles = take(256);    // the level loop's state (KcState)
   L.total = p;
   return L;
 }
 
-// Level loop of the k-core peel (liu_et_al.rs:295-420): the host reads the
-// frontier size after each scan and sub-level.
+// Level loop of the k-core peel (liu_et_al.rs:295-420) on the device: a CUDA
+// graph whose WHILE node runs k_kcore_wave four times per iteration (the last
+// block of each wave plans the next and sets the condition), or host-launched
+// waves with SPARX_LOOP_HOST.
 int run_kcore(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   const Layout& L = J.L;
   const uint32_t N = (uint32_t)J.N;
@@ -1060,63 +1147,81 @@ int run_kcore(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaStreamSynchronize(s));
     if (*herr) { J.err = *herr; return status_from_flags(*herr); }
   }
+  static_assert(sizeof(KcState) <= 256, "KcState fits its slot");
   uint32_t* deg = at<uint32_t>(E, L.dplus);
   uint32_t* alive = at<uint32_t>(E, L.act0);
   uint32_t* core = at<uint32_t>(E, L.opos);
   uint32_t* qa = at<uint32_t>(E, L.q0);
   uint32_t* qb = at<uint32_t>(E, L.q1);
-  uint32_t* sc = at<uint32_t>(E, L.tiles);  // [0] count, [1] next count, [2] smallest degree left
-  unsigned long long* remaining_d = (unsigned long long*)(sc + 4);
+  KcState* kst = at<KcState>(E, L.tiles);
   const int u8 = O.support_mode == SPARX_SUPPORT_U8;
   const int vgrid = grid_for(N, 256, E.sm_count * 16);
-  CU(cudaMemsetAsync(remaining_d, 0, 8, s));
+  CU(cudaMemsetAsync(kst, 0, sizeof(KcState), s));
   CU(cudaEventRecord(E.tev[1], s));
-  k_kcore_init<<<vgrid, 256, 0, s>>>(J.off, N, u8, deg, alive, core, remaining_d);
-  J.launches += 1;
-  uint32_t* h = (uint32_t*)E.pinned_small;
-  unsigned long long remaining = 0;
-  CU(cudaMemcpyAsync(h, remaining_d, 8, cudaMemcpyDeviceToHost, s));
-  CU(cudaStreamSynchronize(s));
-  std::memcpy(&remaining, h, 8);
+  k_kcore_init<<<vgrid, 256, 0, s>>>(J.off, N, u8, deg, alive, core, &kst->remaining);
+  // every wave is a scan or a sub-level that peels >= 1 vertex; scans per level <= 2
+  k_kcore_start<<<1, 1, 0, s>>>(kst, 3ull * N + 2 * J.W + 64, O.timeout_ms * 1000000ull);
+  J.launches += 2;
   CU(cudaEventRecord(E.tev[4], s));
-  uint64_t k = 1;
-  const auto t_start = std::chrono::steady_clock::now();
-  while (remaining > 0) {
-    if (O.timeout_ms && std::chrono::steady_clock::now() - t_start > std::chrono::milliseconds(O.timeout_ms)) {
-      set_error("k-core peel exceeded the time budget");
-      return SPARX_E_TIMEOUT;
+  const int wgrid = E.sm_count * 8;
+  if (O.loop == SPARX_LOOP_GRAPH) {
+    cudaGraph_t g;
+    CU(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    CU(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CU(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CU(cudaStreamBeginCaptureToGraph(E.capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    for (int i = 0; i < 4; ++i)
+      k_kcore_wave<<<wgrid, 256, 0, E.capture>>>(J.off, J.nbr, N, deg, alive, core, qa, qb, kst, h, 1);
+    cudaGraph_t captured;
+    CU(cudaStreamEndCapture(E.capture, &captured));
+    cudaGraphExec_t ex;
+    cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(g);
+      set_error(std::string("k-core graph: ") + cudaGetErrorString(ie));
+      return SPARX_E_CUDA;
     }
-    CU(cudaMemsetAsync(sc, 0, 8, s));
-    CU(cudaMemsetAsync(sc + 2, 0xFF, 4, s));
-    k_kcore_scan<<<vgrid, 256, 0, s>>>(deg, alive, N, (uint32_t)k, qa, sc, sc + 2);
-    J.launches += 1;
-    CU(cudaMemcpyAsync(h, sc, 12, cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
-    uint32_t count = h[0];
-    const uint32_t min_left = h[2];
-    if (count == 0) {
-      // no live vertex at this level: go to the smallest degree left
-      if (min_left == 0xFFFFFFFFu) { set_error("k-core: live vertices but none found"); return SPARX_E_CUDA; }
-      k = std::max<uint64_t>(k + 1, min_left);
-      continue;
+    const cudaError_t le = cudaGraphLaunch(ex, s);
+    const cudaError_t se = cudaStreamSynchronize(s);
+    cudaGraphExecDestroy(ex);
+    cudaGraphDestroy(g);
+    if (le != cudaSuccess || se != cudaSuccess) {
+      set_error(std::string("k-core loop: ") + cudaGetErrorString(le != cudaSuccess ? le : se));
+      return SPARX_E_CUDA;
     }
-    J.kc_levels += 1;
-    J.kc_max = (uint32_t)k;
-    while (count > 0) {
-      remaining -= std::min<unsigned long long>(remaining, count);
-      CU(cudaMemsetAsync(sc + 1, 0, 4, s));
-      const int pgrid = grid_for(32ull * count, 256, E.sm_count * 16);
-      k_kcore_peel<<<pgrid, 256, 0, s>>>(J.off, J.nbr, qa, count, (uint32_t)k, deg, alive, core, qb, sc + 1);
-      J.launches += 1;
-      J.kc_waves += 1;
-      CU(cudaMemcpyAsync(h + 1, sc + 1, 4, cudaMemcpyDeviceToHost, s));
+  } else {
+    KcState* h = (KcState*)E.pinned_small;
+    for (;;) {
+      for (int i = 0; i < 16; ++i)
+        k_kcore_wave<<<wgrid, 256, 0, s>>>(J.off, J.nbr, N, deg, alive, core, qa, qb, kst,
+                                           cudaGraphConditionalHandle{}, 0);
+      J.launches += 16;
+      CU(cudaMemcpyAsync(h, kst, sizeof(KcState), cudaMemcpyDeviceToHost, s));
       CU(cudaStreamSynchronize(s));
-      count = h[1];
-      std::swap(qa, qb);
+      if (h->phase == 2) break;
     }
-    k += 1;
   }
   CU(cudaEventRecord(E.tev[5], s));
+  KcState hs;
+  CU(cudaMemcpyAsync(&hs, kst, sizeof(KcState), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (O.loop == SPARX_LOOP_GRAPH) J.launches += (uint32_t)hs.waves_run;
+  if (hs.err) {
+    J.err = hs.err;
+    set_error("k-core level loop stopped: " + std::string(hs.err & kErrTimeout ? "time budget" : "wave bound"));
+    return status_from_flags(hs.err);
+  }
+  J.kc_levels = hs.levels;
+  J.kc_waves = hs.subs;
+  J.kc_max = hs.kmax;
   if (O.out_bits == 8 && J.kc_max > 255) {
     // the reference's u8 level counter overflows (liu_et_al.rs:335-343)
     set_error("a core number exceeds 255 with 8-bit output");
@@ -1467,20 +1572,25 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
 
 // ---------------------------------------------------------------------------
 // Serving: continuous batching over execution lanes.  Each lane is a private
-// engine (stream, workspace, staging, cached peel graph).  An idle lane takes
-// every queued request that fits its share of the HBM budget (FIFO), packs
-// them into one union and runs it; requests that arrive while other lanes are
-// busy start on the next free lane at once, so their work overlaps on the
-// device with the unions already running.
+// engine (stream, workspace, staging, cached peel graph) running one served
+// union at a time: an idle lane packs the queued requests that fit its share
+// of the HBM budget into a union with room to spare; while its peel runs,
+// requests that arrive are admitted into it at the next wave boundary (the
+// lane's planner stops when the host sets the lane's admission word; the
+// newcomers are prepared -- narrowed, oriented, supported -- on the lane's
+// second engine and joined behind the running members), and each member's
+// truss numbers go back as soon as its own peel ends, not when the union's
+// does.  Lanes run on separate streams, so their work overlaps on the GPU.
 
-constexpr int kServerLanes = 4;
-constexpr size_t kServerMaxMembers = 4096;
+constexpr int kServerLanes = 4;                // default; SPARX_SERVE_LANES (1..16) overrides
+constexpr uint32_t kServeMaxMembers = 4096;   // members per served union, joined ones included
 
 struct ServerReq {
   uint64_t ticket = 0;
   HostMember h;
   int status = SPARX_OK;
   bool running = false, done = false, cancelled = false;
+  bool fresh_only = false;  // joining failed on the device: run in a fresh (unserved) union
   sparx_pkt_stats st{};
   std::chrono::steady_clock::time_point t_submit, t_start, t_done;
 };
@@ -1509,8 +1619,11 @@ void engine_release(Engine* E) {
 struct sparx_server {
   int device = 0;
   Opts O;
-  uint64_t lane_budget = 0;
-  std::vector<Engine*> lanes;
+  std::vector<uint64_t> lane_budget;  // lane 0: half the budget (large graphs), the others a sixth
+  std::vector<Engine*> lanes;         // runs the lane's unions
+  std::vector<Engine*> prep;          // prepares the requests that join the lane's running union
+  uint32_t* admit_host = nullptr;     // one mapped word per lane: requests wait to join
+  uint32_t* admit_dev = nullptr;
   std::vector<std::thread> workers;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -1518,6 +1631,8 @@ struct sparx_server {
   std::unordered_map<uint64_t, ServerReq*> reqs;
   uint64_t next_ticket = 1;
   bool stop = false;
+  int nlanes = kServerLanes;
+  std::atomic<uint64_t> unions{0}, joined{0};  // served unions started; requests that joined one running
 };
 
 namespace {
@@ -1531,12 +1646,292 @@ void server_finish(sparx_server* S, ServerReq* r, int status) {
   (void)S;
 }
 
+uint64_t prep_budget(uint64_t lane_budget) { return lane_budget / 5; }
+
+bool layout_fits(uint64_t N, uint64_t W, uint32_t G, size_t esz, uint64_t max_n, uint64_t budget) {
+  return N < 0xFFFFFFFFull && W < 0xFFFFFFFFull && make_layout(N, W, G, true, esz * W, max_n).total <= budget;
+}
+
+// The lane's hook: delivers members as they finish and joins waiting requests.
+struct LaneHook : ServeHook {
+  sparx_server* S = nullptr;
+  int lane = 0;
+  Engine* P = nullptr;              // prepares joining requests
+  std::vector<ServerReq*> reqs;     // per member of the union
+  std::vector<char> delivered;
+  uint64_t N_cap = 0, W_cap = 0;    // the union's room
+  uint64_t max_n0 = 0;              // largest initial member (the hub pool was sized for it)
+
+  int deliver(Engine& E, UnionJob& J, uint32_t G, cudaStream_t s) {
+    const Layout& L = J.L;
+    std::vector<MemberState> st(G);
+    std::vector<unsigned long long> tri(G);
+    std::vector<uint32_t> mx(G);
+    CU(cudaMemcpyAsync(st.data(), at<MemberState>(E, L.st), sizeof(MemberState) * G, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(tri.data(), at<unsigned long long>(E, L.mem_tri), 8ull * G, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(mx.data(), at<uint32_t>(E, L.mem_maxsup), 4ull * G, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const size_t esz = S->O.out_bits / 8;
+    const int u8 = S->O.support_mode == SPARX_SUPPORT_U8;
+    Counters* cnt = at<Counters>(E, L.cnt);
+    const unsigned long long* row0 = at<unsigned long long>(E, L.row0);
+    const int2* es = at<int2>(E, L.es);
+    for (uint32_t g = 0; g < G; ++g) {
+      if (delivered[g] || st[g].phase != kPhaseDone) continue;
+      const Member& M = J.members[g];
+      uint32_t* ferr = &cnt->fin_err;
+      CU(cudaMemsetAsync(ferr, 0, 4, s));
+      char* out = (char*)J.out + (size_t)M.sb * esz;
+      if (M.w) {
+        // a deduplicated (multigraph) union maps the member's caller slots through smap
+        const int fg = grid_for(M.w, 256, E.sm_count * 16);
+        const unsigned long long* r0 = J.smap ? row0 : row0 + M.sb;
+        const uint32_t* sm = J.smap ? J.smap + M.sb : nullptr;
+        if (esz == 1)
+          k_finalize<uint8_t><<<fg, 256, 0, s>>>(r0, es, M.w, (uint8_t*)out, u8, 1, &cnt->kmax, ferr, sm);
+        else
+          k_finalize<uint32_t><<<fg, 256, 0, s>>>(r0, es, M.w, (uint32_t*)out, u8, 0, &cnt->kmax, ferr, sm);
+      }
+      uint32_t* hferr = (uint32_t*)E.pinned_small;
+      CU(cudaMemcpyAsync(hferr, ferr, 4, cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+      const int status = status_from_flags(*hferr);
+      ServerReq* r = reqs[g];
+      if (!status && M.w) {
+        int rc = download(E, r->h.out, out, (size_t)M.w * esz, s);
+        if (rc) return rc;
+        CU(cudaStreamSynchronize(s));
+      }
+      sparx_pkt_stats ps{};
+      ps.n = M.n;
+      ps.width = M.w;
+      ps.m = M.m;
+      ps.self_loops = M.w - 2ull * M.m;
+      ps.triangles = tri[g] / 3;
+      ps.max_support = mx[g];
+      ps.k_max = M.w ? st[g].max_level + 2 : 0;
+      ps.levels = st[g].levels;
+      ps.waves = st[g].waves;
+      delivered[g] = 1;
+      {
+        std::lock_guard<std::mutex> lk(S->mu);
+        r->st = ps;
+        server_finish(S, r, status);
+      }
+      S->cv_done.notify_all();
+    }
+    return SPARX_OK;
+  }
+
+  // Join the queued requests that fit; returns the number joined.
+  int admit(Engine& E, UnionJob& J, PeelCtx& ctx, cudaStream_t s, uint32_t* joined) {
+    *joined = 0;
+    S->admit_host[lane] = 0;
+    if (J.multi) return SPARX_OK;  // a deduplicated union has no room for more rows: wait for a lane
+    std::vector<ServerReq*> take;
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      uint64_t N = ctx.N, W = ctx.Ws, pn = 0, pw = 0, pmax = 0;
+      uint32_t G = ctx.G;
+      for (auto it = S->queue.begin(); it != S->queue.end();) {
+        ServerReq* r = *it;
+        const uint64_t n2 = N + r->h.n, w2 = W + r->h.w;
+        const bool fits = !r->fresh_only && G + 1 <= kServeMaxMembers && n2 <= N_cap && w2 <= W_cap &&
+                          layout_fits(pn + r->h.n, pw + r->h.w, (uint32_t)take.size() + 1, 4,
+                                      std::max<uint64_t>(pmax, r->h.n), prep_budget(S->lane_budget[lane]));
+        if (!fits) { ++it; continue; }
+        it = S->queue.erase(it);
+        r->running = true;
+        r->t_start = std::chrono::steady_clock::now();
+        take.push_back(r);
+        N = n2;
+        W = w2;
+        pn += r->h.n;
+        pw += r->h.w;
+        pmax = std::max<uint64_t>(pmax, r->h.n);
+        ++G;
+      }
+    }
+    if (take.empty()) return SPARX_OK;
+    // host checks, then one prepared union of the valid newcomers
+    std::vector<HostMember> hm;
+    std::vector<ServerReq*> ok;
+    for (ServerReq* r : take) {
+      int st = host_validate(r->h);
+      if (st == SPARX_OK && r->h.w / 2 > kEidMask) st = SPARX_E_TOO_LARGE;
+      if (st) {
+        std::lock_guard<std::mutex> lk(S->mu);
+        server_finish(S, r, st);
+        continue;
+      }
+      HostMember h = r->h;
+      h.index = hm.size();
+      hm.push_back(h);
+      ok.push_back(r);
+    }
+    S->cv_done.notify_all();
+    if (hm.empty()) return SPARX_OK;
+    UnionJob PJ;
+    uint64_t Np = 0, Wp = 0, maxn = 0;
+    for (const HostMember& h : hm) {
+      PJ.members.push_back(Member{(uint32_t)Np, (uint32_t)h.n, (uint32_t)Wp, (uint32_t)h.w, 0, 0});
+      Np += h.n;
+      Wp += h.w;
+      maxn = std::max<uint64_t>(maxn, h.n);
+    }
+    PJ.N = Np;
+    PJ.W = Wp;
+    PJ.prep_only = true;
+    PJ.L = make_layout(Np, Wp, (uint32_t)hm.size(), true, 4 * Wp, maxn);
+    PJ.L.hub_cap = 0;  // joining members get no hub maps
+    int rc = ensure_ws(*P, PJ.L.total, false);
+    int prc = rc;
+    if (!rc) {
+      cudaStream_t ps = P->stream;
+      PJ.off = at<uint32_t>(*P, PJ.L.off);
+      PJ.nbr = at<uint32_t>(*P, PJ.L.nbr);
+      CU(cudaMemsetAsync(at<Counters>(*P, PJ.L.cnt), 0, sizeof(Counters), ps));
+      prc = upload_union(*P, hm, PJ.members, Np, Wp, PJ.off, (uint32_t*)PJ.nbr, ps);
+      if (!prc) prc = run_union(*P, PJ, S->O, ps);
+    }
+    if (prc) {
+      // an input defect, a multigraph or no room: these requests run in a fresh union
+      std::lock_guard<std::mutex> lk(S->mu);
+      for (auto it = ok.rbegin(); it != ok.rend(); ++it) {
+        (*it)->running = false;
+        (*it)->fresh_only = true;
+        S->queue.push_front(*it);
+      }
+      S->cv_work.notify_all();
+      return SPARX_OK;
+    }
+    // join: the prepared arrays go behind the union's, ids shifted
+    const Layout& L = J.L;
+    const uint32_t N0 = ctx.N, G0 = ctx.G;
+    const uint64_t W0 = ctx.Ws, m0 = ctx.m, mp = PJ.prep_m;
+    const int gridW = grid_for(std::max<uint64_t>(Wp, 1), 256, E.sm_count * 16);
+    const int gridN = grid_for(Np + 1, 256, E.sm_count * 16);
+    const int gridM = grid_for(std::max<uint64_t>(mp, 1), 256, E.sm_count * 16);
+    uint32_t* off = J.off;
+    unsigned long long* row0 = at<unsigned long long>(E, L.row0);
+    k_shift_u32<<<gridN, 256, 0, s>>>(off + N0, at<uint32_t>(*P, PJ.L.off), Np + 1, (uint32_t)W0);
+    if (Wp) k_shift_pairs<<<gridW, 256, 0, s>>>(row0 + W0, at<unsigned long long>(*P, PJ.L.row0), Wp, N0,
+                                                (uint32_t)m0);
+    if (ctx.cur_row != row0) {  // compacted working rows: the new rows go behind their live entries
+      k_shift_u32<<<gridN, 256, 0, s>>>((uint32_t*)ctx.cur_off + N0, at<uint32_t>(*P, PJ.L.off), Np + 1,
+                                        (uint32_t)ctx.csr_slots);
+      if (Wp)
+        k_shift_pairs<<<gridW, 256, 0, s>>>((unsigned long long*)ctx.cur_row + ctx.csr_slots,
+                                            at<unsigned long long>(*P, PJ.L.row0), Wp, N0, (uint32_t)m0);
+    }
+    k_shift_u32<<<gridN, 256, 0, s>>>(at<uint32_t>(E, L.opos) + N0, at<uint32_t>(*P, PJ.L.opos), Np + 1,
+                                      (uint32_t)m0);
+    if (mp) {
+      k_shift_u32<<<gridM, 256, 0, s>>>(at<uint32_t>(E, L.ocol) + m0, at<uint32_t>(*P, PJ.L.ocol), mp, N0);
+      k_shift_u32<<<gridM, 256, 0, s>>>(at<uint32_t>(E, L.osrc) + m0, at<uint32_t>(*P, PJ.L.osrc), mp, N0);
+      CU(cudaMemcpyAsync(at<int2>(E, L.es) + m0, at<int2>(*P, PJ.L.es), 8 * mp, cudaMemcpyDeviceToDevice, s));
+    }
+    if (ctx.U.hub_slot && Np) CU(cudaMemsetAsync(at<uint32_t>(E, L.hub_slot) + N0, 0xFF, 4 * Np, s));
+    Counters* cnt = at<Counters>(E, L.cnt);
+    if (Np) k_big_rows_range<<<grid_for(Np, 256, E.sm_count * 8), 256, 0, s>>>(off, N0, N0 + (uint32_t)Np,
+                                                                                 at<uint32_t>(E, L.big),
+                                                                                 &cnt->big_count);
+    std::vector<Member> nm;
+    for (const Member& M : PJ.members)
+      nm.push_back(Member{M.vb + N0, M.n, M.sb + (uint32_t)W0, M.w, M.eb + (uint32_t)m0, M.m});
+    Member* dmem = at<Member>(E, L.mem);
+    CU(cudaMemcpyAsync(dmem + G0, nm.data(), sizeof(Member) * nm.size(), cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(at<unsigned long long>(E, L.mem_tri) + G0, 0, 8 * nm.size(), s));
+    CU(cudaMemsetAsync(at<uint32_t>(E, L.mem_maxsup) + G0, 0, 4 * nm.size(), s));
+    const uint32_t G1 = G0 + (uint32_t)nm.size();
+    k_member_init<<<1, 256, 0, s>>>(dmem, at<MemberState>(E, L.st), G0, G1);
+    ctx.U.n = N0 + (uint32_t)Np;
+    ctx.U.m = (uint32_t)(m0 + mp);
+    ctx.U.width = (uint32_t)(W0 + Wp);
+    ctx.U.G = G1;
+    CU(cudaMemcpyAsync(at<Union>(E, L.uni), &ctx.U, sizeof(Union), cudaMemcpyHostToDevice, s));
+    if (mp)
+      k_peel_setup<<<grid_for(mp, 256, E.sm_count * 8), 256, 0, s>>>(
+          at<Union>(E, L.uni), dmem, S->O.support_mode == SPARX_SUPPORT_U8, at<unsigned long long>(E, L.mem_tri),
+          at<uint32_t>(E, L.mem_maxsup), nullptr, &cnt->err, (uint32_t)m0);
+    k_ctl_join<<<1, 1, 0, s>>>(at<Control>(E, L.ctl), G1, 3ull * mp + 64, Wp);
+    CU(cudaStreamSynchronize(s));
+    for (const Member& M : nm) {
+      J.members.push_back(M);
+      (void)M;
+    }
+    for (ServerReq* r : ok) reqs.push_back(r);
+    delivered.resize(reqs.size(), 0);
+    ctx.N = N0 + (uint32_t)Np;
+    ctx.G = G1;
+    ctx.m = m0 + mp;
+    ctx.Ws = W0 + Wp;
+    ctx.csr_slots += Wp;
+    *joined = (uint32_t)nm.size();
+    S->joined += nm.size();
+    return SPARX_OK;
+  }
+
+  int at_stop(Engine& E, UnionJob& J, PeelCtx& ctx, uint32_t reason, cudaStream_t s) override {
+    int rc = deliver(E, J, ctx.G, s);
+    if (rc) return rc;
+    uint32_t joined = 0;
+    bool stopping;
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      stopping = S->stop;
+    }
+    if (!stopping && reason != kExitDone) {
+      rc = admit(E, J, ctx, s, &joined);
+      if (rc) return rc;
+    }
+    bool live = false;
+    for (size_t g = 0; g < delivered.size(); ++g) live |= !delivered[g];
+    ctx.resume = live;
+    return SPARX_OK;
+  }
+};
+
+// Requests that could not join (an input defect or a multigraph): the batch
+// path, which attributes a device error to the member that caused it.
+void run_fresh(sparx_server* S, Engine& E, std::vector<ServerReq*>& batch) {
+  std::vector<HostMember> hm;
+  std::vector<size_t> which;
+  std::vector<int> status(batch.size(), SPARX_OK);
+  for (size_t i = 0; i < batch.size(); ++i) {
+    HostMember h = batch[i]->h;
+    status[i] = host_validate(h);
+    if (status[i] == SPARX_OK && h.w / 2 > kEidMask) status[i] = SPARX_E_TOO_LARGE;
+    if (status[i] == SPARX_OK) {
+      h.index = hm.size();
+      hm.push_back(h);
+      which.push_back(i);
+    }
+  }
+  std::vector<int> st2(hm.size(), SPARX_OK);
+  std::vector<sparx_pkt_stats> stats(hm.size());
+  int first_fail = SPARX_OK;
+  if (!hm.empty()) run_batch_union(E, hm, S->O, st2.data(), stats.data(), &first_fail);
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (size_t k = 0; k < which.size(); ++k) {
+      status[which[k]] = st2[k];
+      batch[which[k]]->st = stats[k];
+    }
+    for (size_t i = 0; i < batch.size(); ++i) server_finish(S, batch[i], status[i]);
+  }
+  S->cv_done.notify_all();
+}
+
 void server_worker(sparx_server* S, int lane) {
   Engine& E = *S->lanes[lane];
   cudaSetDevice(S->device);
   const size_t esz = S->O.out_bits / 8;
+  const uint64_t budget = S->lane_budget[lane];
+  const uint64_t main_budget = budget - prep_budget(budget);
   for (;;) {
     std::vector<ServerReq*> batch;
+    bool fresh = false;
     {
       std::unique_lock<std::mutex> lk(S->mu);
       S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
@@ -1544,58 +1939,115 @@ void server_worker(sparx_server* S, int lane) {
         if (S->stop) return;
         continue;
       }
-      uint64_t N = 0, W = 0, max_n = 0;
-      while (!S->queue.empty() && batch.size() < kServerMaxMembers) {
-        ServerReq* r = S->queue.front();
-        const uint64_t N2 = N + r->h.n, W2 = W + r->h.w, mx2 = std::max<uint64_t>(max_n, r->h.n);
-        const size_t bytes = make_layout(N2, W2, (uint32_t)batch.size() + 1, true, esz * W2, mx2).total;
-        const bool fits = bytes <= S->lane_budget && N2 < 0xFFFFFFFFull && W2 < 0xFFFFFFFFull;
-        if (!fits) {
-          if (batch.empty()) {  // never fits a lane on its own
-            S->queue.pop_front();
+      // FIFO; a request too large for this lane is left for a larger one
+      uint64_t N = 0, W = 0, mx = 0;
+      for (auto it = S->queue.begin(); it != S->queue.end() && batch.size() < kServeMaxMembers;) {
+        ServerReq* r = *it;
+        if (!batch.empty() && r->fresh_only != fresh) { ++it; continue; }
+        const uint64_t N2 = N + r->h.n, W2 = W + r->h.w, mx2 = std::max<uint64_t>(mx, r->h.n);
+        if (!layout_fits(N2, W2, kServeMaxMembers, esz, mx2, main_budget)) {
+          bool fits_any = false;
+          for (uint64_t b : S->lane_budget)
+            fits_any |= layout_fits(r->h.n, r->h.w, kServeMaxMembers, esz, r->h.n, b - prep_budget(b));
+          if (!fits_any) {  // no lane can ever hold it
+            it = S->queue.erase(it);
             server_finish(S, r, SPARX_E_OOM);
             S->cv_done.notify_all();
             continue;
           }
-          break;
+          ++it;
+          continue;
         }
-        S->queue.pop_front();
+        if (batch.empty()) fresh = r->fresh_only;
+        it = S->queue.erase(it);
         r->running = true;
         r->t_start = std::chrono::steady_clock::now();
         batch.push_back(r);
         N = N2;
         W = W2;
-        max_n = mx2;
+        mx = mx2;
+      }
+      if (batch.empty()) {
+        // nothing fits this lane now: wait for a change
+        S->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+        continue;
       }
     }
-    if (batch.empty()) continue;
-    // host checks, then one union for the valid requests
+    if (fresh) {
+      run_fresh(S, E, batch);
+      continue;
+    }
+    // a served union: the batch, with room for requests that join while it runs
     std::vector<HostMember> hm;
-    std::vector<size_t> which;
-    std::vector<int> status(batch.size(), SPARX_OK);
-    for (size_t i = 0; i < batch.size(); ++i) {
-      HostMember h = batch[i]->h;
-      status[i] = host_validate(h);
-      if (status[i] == SPARX_OK && h.w / 2 > kEidMask) status[i] = SPARX_E_TOO_LARGE;
-      if (status[i] == SPARX_OK) {
-        h.index = hm.size();
-        hm.push_back(h);
-        which.push_back(i);
+    LaneHook hook;
+    hook.S = S;
+    hook.lane = lane;
+    hook.P = S->prep[lane];
+    hook.admit_dev = S->admit_dev + lane;
+    for (ServerReq* r : batch) {
+      int st = host_validate(r->h);
+      if (st == SPARX_OK && r->h.w / 2 > kEidMask) st = SPARX_E_TOO_LARGE;
+      if (st) {
+        std::lock_guard<std::mutex> lk(S->mu);
+        server_finish(S, r, st);
+        continue;
       }
-    }
-    std::vector<int> st2(hm.size(), SPARX_OK);
-    std::vector<sparx_pkt_stats> stats(hm.size());
-    int first_fail = SPARX_OK;
-    if (!hm.empty()) run_batch_union(E, hm, S->O, st2.data(), stats.data(), &first_fail);
-    {
-      std::lock_guard<std::mutex> lk(S->mu);
-      for (size_t k = 0; k < which.size(); ++k) {
-        status[which[k]] = st2[k];
-        batch[which[k]]->st = stats[k];
-      }
-      for (size_t i = 0; i < batch.size(); ++i) server_finish(S, batch[i], status[i]);
+      HostMember h = r->h;
+      h.index = hm.size();
+      hm.push_back(h);
+      hook.reqs.push_back(r);
     }
     S->cv_done.notify_all();
+    if (hm.empty()) continue;
+    UnionJob J;
+    uint64_t N = 0, W = 0, mx = 0;
+    for (const HostMember& h : hm) {
+      J.members.push_back(Member{(uint32_t)N, (uint32_t)h.n, (uint32_t)W, (uint32_t)h.w, 0, 0});
+      N += h.n;
+      W += h.w;
+      mx = std::max<uint64_t>(mx, h.n);
+    }
+    // room: the largest extra (slots e, vertices e / 2) the lane's budget holds
+    uint64_t extra = 0;
+    for (uint64_t step = 1ull << 40; step; step >>= 1) {
+      const uint64_t e2 = extra + step;
+      if (W + e2 < (1ull << 31) && layout_fits(N + e2 / 2, W + e2, kServeMaxMembers, esz, mx, main_budget))
+        extra = e2;
+    }
+    hook.N_cap = N + extra / 2;
+    hook.W_cap = W + extra;
+    hook.max_n0 = mx;
+    hook.delivered.assign(hook.reqs.size(), 0);
+    J.N = N;
+    J.W = W;
+    J.hook = &hook;
+    S->unions += 1;
+    J.L = make_layout(hook.N_cap, hook.W_cap, kServeMaxMembers, true, esz * hook.W_cap, mx);
+    int rc = ensure_ws(E, J.L.total, false);
+    if (!rc) {
+      cudaStream_t s = E.stream;
+      J.off = at<uint32_t>(E, J.L.off);
+      J.nbr = at<uint32_t>(E, J.L.nbr);
+      J.out = at<void>(E, J.L.out);
+      cudaMemsetAsync(at<Counters>(E, J.L.cnt), 0, sizeof(Counters), s);
+      cudaEventRecord(E.tev[0], s);
+      rc = upload_union(E, hm, J.members, N, W, J.off, (uint32_t*)J.nbr, s);
+      if (!rc) rc = run_union(E, J, S->O, s);
+    }
+    if (rc) {
+      // members not delivered: run them again through the batch path (which
+      // names the member an input defect belongs to)
+      std::vector<ServerReq*> rest;
+      for (size_t g = 0; g < hook.reqs.size(); ++g)
+        if (!hook.delivered[g]) rest.push_back(hook.reqs[g]);
+      cudaStreamSynchronize(E.stream);
+      cudaGetLastError();
+      if (!rest.empty()) run_fresh(S, E, rest);
+    }
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->admit_host[lane] = 0;
+    }
   }
 }
 
@@ -1874,19 +2326,37 @@ int sparx_server_create(sparx_server** out, uint64_t hbm_budget_bytes, const spa
   auto* S = new sparx_server();
   S->device = device;
   S->O = O;
-  S->lane_budget = budget / kServerLanes;
-  for (int i = 0; i < kServerLanes; ++i) {
+  if (const char* env = std::getenv("SPARX_SERVE_LANES")) {
+    const int k = std::atoi(env);
+    if (k >= 1 && k <= 16) S->nlanes = k;
+  }
+  const int nl = S->nlanes;
+  // lane 0 takes half the budget (a large graph fits there, with room for
+  // requests that join it); the other lanes share the rest
+  for (int i = 0; i < nl; ++i)
+    S->lane_budget.push_back(nl == 1 ? budget : i == 0 ? budget / 2 : budget / 2 / (nl - 1));
+  auto fail = [&](int code) {
+    for (Engine* L : S->lanes) engine_release(L);
+    for (Engine* L : S->prep) engine_release(L);
+    if (S->admit_host) cudaFreeHost(S->admit_host);
+    delete S;
+    return code;
+  };
+  cudaError_t e = cudaHostAlloc(&S->admit_host, 4 * nl, cudaHostAllocMapped);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); S->admit_host = nullptr; return fail(SPARX_E_CUDA); }
+  std::memset(S->admit_host, 0, 4 * nl);
+  e = cudaHostGetDevicePointer((void**)&S->admit_dev, S->admit_host, 0);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return fail(SPARX_E_CUDA); }
+  for (int i = 0; i < 2 * nl; ++i) {
     Engine* E = new Engine();
     rc = engine_init(*E, device);
     if (rc) {
       engine_release(E);
-      for (Engine* L : S->lanes) engine_release(L);
-      delete S;
-      return rc;
+      return fail(rc);
     }
-    S->lanes.push_back(E);
+    (i < nl ? S->lanes : S->prep).push_back(E);
   }
-  for (int i = 0; i < kServerLanes; ++i) S->workers.emplace_back(server_worker, S, i);
+  for (int i = 0; i < nl; ++i) S->workers.emplace_back(server_worker, S, i);
   *out = S;
   return SPARX_OK;
 }
@@ -1915,6 +2385,8 @@ int sparx_server_submit(sparx_server* S, const sparx_graph_view* v, uint64_t* ti
     r->ticket = S->next_ticket++;
     S->reqs[r->ticket] = r;
     S->queue.push_back(r);
+    // running unions stop at their next wave to see whether it can join
+    for (int i = 0; i < S->nlanes; ++i) ((volatile uint32_t*)S->admit_host)[i] = 1;
   }
   S->cv_work.notify_one();
   *ticket = r->ticket;
@@ -1961,6 +2433,13 @@ int sparx_server_cancel(sparx_server* S, uint64_t ticket) {
   return SPARX_OK;
 }
 
+int sparx_server_info(sparx_server* S, uint64_t* unions, uint64_t* joined) {
+  if (!S) return SPARX_E_ARG;
+  if (unions) *unions = S->unions.load();
+  if (joined) *joined = S->joined.load();
+  return SPARX_OK;
+}
+
 int sparx_server_destroy(sparx_server* S) {
   if (!S) return SPARX_E_ARG;
   {
@@ -1970,6 +2449,8 @@ int sparx_server_destroy(sparx_server* S) {
   S->cv_work.notify_all();
   for (auto& t : S->workers) t.join();
   for (Engine* E : S->lanes) engine_release(E);
+  for (Engine* E : S->prep) engine_release(E);
+  if (S->admit_host) cudaFreeHost(S->admit_host);
   for (auto& kv : S->reqs) delete kv.second;
   delete S;
   return SPARX_OK;

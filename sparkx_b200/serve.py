@@ -1,11 +1,12 @@
 """Continuous-batching PKT service (``sparx_server_*``).
 
 Requests are decompositions of independent graphs submitted at any time.  The
-engine runs them on four execution lanes: an idle lane takes every queued
-request that fits its share of the HBM budget, packs them into one
-concatenated CSR and runs the whole pipeline; requests that arrive while other
-lanes are busy start on the next free lane, so their GPU work overlaps.  Each
-request's result is the same as a solo decomposition of its graph.
+engine runs them on execution lanes (4; SPARX_SERVE_LANES overrides), each on
+its own stream: an idle lane packs the queued requests that fit its share of
+the HBM budget into one concatenated CSR with room to spare and runs it;
+requests that arrive while it runs join it at the next wave boundary, and every
+member's result is returned as soon as its own peel ends.  Each request's
+result is the same as a solo decomposition of its graph.
 """
 from __future__ import annotations
 
@@ -34,6 +35,8 @@ def _lib():
         L.sparx_server_cancel.argtypes = [vp, u64]
         L.sparx_server_destroy.restype = i32
         L.sparx_server_destroy.argtypes = [vp]
+        L.sparx_server_info.restype = i32
+        L.sparx_server_info.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L._sparx_server_typed = True
     return L
 
@@ -92,6 +95,12 @@ class PktServer:
         status, st = ctypes.c_int(), P._Stats()
         P._check(_lib().sparx_server_wait(self._h, ticket, timeout_ms, ctypes.byref(status), ctypes.byref(st)))
         return self._result(ticket, status.value, st)
+
+    def info(self) -> dict:
+        """Served unions started, and requests that joined a union already running."""
+        u, j = ctypes.c_uint64(), ctypes.c_uint64()
+        P._check(_lib().sparx_server_info(self._h, ctypes.byref(u), ctypes.byref(j)))
+        return {"unions": u.value, "joined": j.value}
 
     def cancel(self, ticket: int) -> bool:
         rc = _lib().sparx_server_cancel(self._h, ticket)

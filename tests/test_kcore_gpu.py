@@ -62,3 +62,18 @@ def test_algoliu_api(tmp_path, monkeypatch):
     assert np.array_equal(again.k_cores(), a.k_cores())
     a.drop_cache()
     assert np.array_equal(gm.k_core_lea().k_cores(), a.k_cores())
+
+
+def test_kcore_level_loop_on_device_and_host_agree():
+    """The device-resident level loop (CUDA-graph WHILE node, the default) and host-launched
+    waves (SPARX_LOOP_HOST) give the oracle's core numbers, on graphs with many levels and
+    multigraph rows (a parallel edge counts once per copy in the reference's degree)."""
+    rng = np.random.default_rng(37)
+    graphs = [gen.rmat(15, 16, seed=9), gen.with_parallel_edges(gen.rmat(11, 16, seed=3), 0.3, seed=3)]
+    graphs += [random_graph(rng) for _ in range(5)]
+    for g in graphs:
+        want = O.kcore(g.offsets, g.neighbours)
+        for loop in (P.LOOP_GRAPH, P.LOOP_HOST):
+            cores, st = P.run_kcore(g.offsets, g.neighbours, P.PktOptions(out_bits=32, loop=loop))
+            assert np.array_equal(cores.astype(np.int64), want), loop
+            assert st.k_max == (int(want.max()) if want.size else 0)

@@ -73,3 +73,59 @@ def test_errors_cancel_and_budget():
         big = gen.rmat(20, 16, seed=1)  # needs more than a quarter of a 1 GiB budget
         r = srv.wait(srv.submit(big.offsets, big.neighbours), timeout_ms=60_000)
         assert r.status == P.E_OOM
+
+
+def _one_lane_server(budget):
+    import os
+    old = os.environ.get("SPARX_SERVE_LANES")
+    os.environ["SPARX_SERVE_LANES"] = "1"
+    try:
+        return PktServer(budget)
+    finally:
+        if old is None:
+            del os.environ["SPARX_SERVE_LANES"]
+        else:
+            os.environ["SPARX_SERVE_LANES"] = old
+
+
+def test_requests_join_a_running_union_mid_peel():
+    """One lane: a long request starts a union; requests submitted while its peel runs join
+    it at a wave boundary (the server counts them), finish before it, and every result
+    equals the solo decomposition and the oracle."""
+    big = gen.rmat(20, 16, seed=7)  # ~0.1 s of peel: the others arrive while it runs
+    rng = np.random.default_rng(29)
+    small = [random_graph(rng, n_max=60) for _ in range(10)]
+    small += [gen.mix_graph(gen.mix_member(i)) for i in range(8) if gen.mix_member(i).n < 20_000]
+    small.append(gen.with_parallel_edges(gen.rmat(9, 8, seed=2), 0.3, seed=2))  # a multigraph: not joined
+    with _one_lane_server(16 << 30) as srv:
+        tb = srv.submit(big.offsets, big.neighbours)
+        time.sleep(0.02)  # the big request's union is running
+        ts = [srv.submit(g.offsets, g.neighbours) for g in small]
+        rs = [srv.wait(t, timeout_ms=120_000) for t in ts]
+        rb = srv.wait(tb, timeout_ms=120_000)
+        info = srv.info()
+    assert rb.status == P.OK
+    assert np.array_equal(rb.truss, P.run_pkt(big.offsets, big.neighbours, P.PktOptions(out_bits=32))[0])
+    for g, r in zip(small, rs):
+        assert r.status == P.OK
+        assert np.array_equal(r.truss, O.pkt(g.offsets, g.neighbours, threads=2))
+    assert info["joined"] >= 1, info
+    # joined members leave as soon as they finish: the small ones do not wait for the big one
+    assert min(r.latency_ms for r in rs) < rb.latency_ms
+
+
+def test_invalid_request_is_isolated_from_a_running_union():
+    good = gen.rmat(12, 16, seed=5)
+    bad = (np.array([0, 1, 3, 4, 4], np.uint64), np.array([1, 0, 2, 3], np.uint32))
+    big = gen.rmat(19, 16, seed=8)
+    with _one_lane_server(8 << 30) as srv:
+        tb = srv.submit(big.offsets, big.neighbours)
+        time.sleep(0.01)
+        tx = srv.submit(*bad)
+        tg = [srv.submit(good.offsets, good.neighbours) for _ in range(5)]
+        assert srv.wait(tx, timeout_ms=60_000).status == P.E_INVALID_CSR
+        want = O.pkt(good.offsets, good.neighbours)
+        for t in tg:
+            r = srv.wait(t, timeout_ms=60_000)
+            assert r.status == P.OK and np.array_equal(r.truss, want)
+        assert srv.wait(tb, timeout_ms=60_000).status == P.OK
