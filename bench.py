@@ -192,6 +192,12 @@ def run_mix(args, rank=0, world=1, local=0):
         sample = [gen.mix_graph(members[i]) for i in mine[: min(24, len(mine))]]
         tuned = autotune_batch([(g.offsets, g.neighbours) for g in sample], opts, repeats=2)
         log(f"rank {rank}: autotuned {tuned}")
+    from concurrent.futures import ThreadPoolExecutor
+
+    def make_member(m):
+        gen.set_threads(1)
+        return gen.mix_graph(m)
+    gen_pool = ThreadPoolExecutor(max_workers=host_threads())
     warm = gen.mix_graph(members[mine[0]])
     run_batch([(warm.offsets, warm.neighbours)], opts)
     run_pkt(warm.offsets, warm.neighbours, opts)
@@ -202,18 +208,18 @@ def run_mix(args, rank=0, world=1, local=0):
     step = args.mix_chunk * world
     for c0 in range(0, len(members), step):
         chunk = list(range(c0, min(c0 + step, len(members))))
-        loaded = {}
+        # this rank's graphs of the chunk (the placement run_sharded_batch makes), generated in
+        # parallel, one generator thread per graph: small graphs are dominated by per-graph setup
+        mine_j = shard.assign_lpt([works[i] for i in chunk], world)[rank]
+        t1 = time.perf_counter()
+        loaded = dict(zip(mine_j, gen_pool.map(make_member, [members[chunk[j]] for j in mine_j])))
+        t_gen += time.perf_counter() - t1
 
         def load(j):  # j indexes the chunk; each rank builds only the graphs placed on it
-            t1 = time.perf_counter()
-            g = gen.mix_graph(members[chunk[j]])
-            loaded[j] = g
-            nonlocal_t[0] += time.perf_counter() - t1
+            g = loaded[j]
             return g.offsets, g.neighbours
 
-        nonlocal_t = [0.0]
         out = shard.run_sharded_batch([works[i] for i in chunk], load, opts=opts, gather=False)
-        t_gen += nonlocal_t[0]
         t_batch += out.seconds  # slowest rank's time for this chunk
         res = out.local
         assert all(r[2] == 0 for r in res.values()), [r[2] for r in res.values() if r[2]]

@@ -1395,26 +1395,88 @@ int upload_union(Engine& E, const std::vector<HostMember>& hm, const std::vector
       auto lo_of = [&](const Member& M) -> uint64_t { return pass == 0 ? M.vb : M.sb; };
       auto len_of = [&](const Member& M) -> uint64_t { return pass == 0 ? M.n : M.w; };
       while (g0 < mem.size() && lo_of(mem[g0]) + len_of(mem[g0]) <= a) ++g0;
-      size_t g1 = g0;
-      while (g1 < mem.size() && lo_of(mem[g1]) < b) ++g1;
+      // fixed-size pieces of the chunk, whatever members they cross: a large
+      // member is narrowed by all threads, not by one
+      constexpr uint64_t kPiece = 1ull << 18;
+      const long long pieces = (long long)((b - a + kPiece - 1) / kPiece);
 #pragma omp parallel for schedule(dynamic, 1)
-      for (long long gi = (long long)g0; gi < (long long)g1; ++gi) {
-        const Member& M = mem[gi];
-        const HostMember& H = hm[gi];
-        const uint64_t lo = std::max<uint64_t>(a, lo_of(M)), hi = std::min<uint64_t>(b, lo_of(M) + len_of(M));
-        if (pass == 0) {
-          for (uint64_t x = lo; x < hi; ++x) buf[x - a] = (uint32_t)(H.off[x - M.vb] + M.sb);
-        } else if (H.bits == 64) {
-          const uint64_t* src = (const uint64_t*)H.nbr;
-          for (uint64_t x = lo; x < hi; ++x) buf[x - a] = (uint32_t)src[x - M.sb] + M.vb;
-        } else {
-          const uint32_t* src = (const uint32_t*)H.nbr;
-          for (uint64_t x = lo; x < hi; ++x) buf[x - a] = src[x - M.sb] + M.vb;
+      for (long long pi = 0; pi < pieces; ++pi) {
+        const uint64_t lo = a + (uint64_t)pi * kPiece, hi = std::min<uint64_t>(b, lo + kPiece);
+        // first member whose range reaches past lo
+        size_t g = g0, gh = mem.size();
+        while (g < gh) {
+          const size_t mid = (g + gh) / 2;
+          if (lo_of(mem[mid]) + len_of(mem[mid]) <= lo) g = mid + 1; else gh = mid;
+        }
+        for (uint64_t x = lo; x < hi;) {
+          while (g < mem.size() && lo_of(mem[g]) + len_of(mem[g]) <= x) ++g;
+          if (g >= mem.size()) break;
+          const Member& M = mem[g];
+          const HostMember& H = hm[g];
+          const uint64_t end = std::min<uint64_t>(hi, lo_of(M) + len_of(M));
+          if (pass == 0) {
+            for (; x < end; ++x) buf[x - a] = (uint32_t)(H.off[x - M.vb] + M.sb);
+          } else if (H.bits == 64) {
+            const uint64_t* src = (const uint64_t*)H.nbr;
+            for (; x < end; ++x) buf[x - a] = (uint32_t)src[x - M.sb] + M.vb;
+          } else {
+            const uint32_t* src = (const uint32_t*)H.nbr;
+            for (; x < end; ++x) buf[x - a] = src[x - M.sb] + M.vb;
+          }
         }
       }
       if (pass == 0 && b == total) buf[total - 1 - a] = (uint32_t)W;  // the closing offset
       CU(cudaMemcpyAsync(dst + a, buf, (b - a) * 4, cudaMemcpyHostToDevice, s));
       CU(cudaEventRecord(E.pin_ev[slot], s));
+    }
+  }
+  return SPARX_OK;
+}
+
+// The union's per-slot results to each member's host buffer: pinned chunks
+// (double-buffered against the copies), split into fixed pieces that all
+// threads copy out, whatever members they cross.
+int download_union(Engine& E, const std::vector<HostMember>& hm, const std::vector<Member>& mem, const void* dev,
+                   size_t esz, cudaStream_t s) {
+  uint64_t W = 0;
+  for (const Member& M : mem) W = std::max<uint64_t>(W, (uint64_t)M.sb + M.w);
+  if (!W) return SPARX_OK;
+  const uint64_t chunk = kStageBytes / esz;
+  const uint64_t nchunks = (W + chunk - 1) / chunk;
+  auto issue = [&](uint64_t c) -> int {
+    const int slot = (int)(c & 1);
+    const uint64_t a = c * chunk, k = std::min<uint64_t>(chunk, W - a);
+    CU(cudaMemcpyAsync(E.pinned[slot], (const char*)dev + a * esz, k * esz, cudaMemcpyDeviceToHost, s));
+    CU(cudaEventRecord(E.pin_ev[slot], s));
+    return SPARX_OK;
+  };
+  CU(cudaEventSynchronize(E.pin_ev[0]));
+  CU(cudaEventSynchronize(E.pin_ev[1]));
+  int rc = issue(0);
+  if (rc) return rc;
+  for (uint64_t c = 0; c < nchunks; ++c) {
+    const int slot = (int)(c & 1);
+    if (c + 1 < nchunks && (rc = issue(c + 1))) return rc;
+    CU(cudaEventSynchronize(E.pin_ev[slot]));
+    const uint64_t a = c * chunk, b = std::min<uint64_t>(W, a + chunk);
+    const char* buf = (const char*)E.pinned[slot];
+    constexpr uint64_t kPiece = 1ull << 18;
+    const long long pieces = (long long)((b - a + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long pi = 0; pi < pieces; ++pi) {
+      const uint64_t lo = a + (uint64_t)pi * kPiece, hi = std::min<uint64_t>(b, lo + kPiece);
+      size_t g = 0, gh = mem.size();
+      while (g < gh) {
+        const size_t mid = (g + gh) / 2;
+        if ((uint64_t)mem[mid].sb + mem[mid].w <= lo) g = mid + 1; else gh = mid;
+      }
+      for (uint64_t x = lo; x < hi && g < mem.size(); ++g) {
+        const Member& M = mem[g];
+        if ((uint64_t)M.sb + M.w <= x) continue;
+        const uint64_t end = std::min<uint64_t>(hi, (uint64_t)M.sb + M.w);
+        std::memcpy((char*)hm[g].out + (x - M.sb) * esz, buf + (x - a) * esz, (end - x) * esz);
+        x = end;
+      }
     }
   }
   return SPARX_OK;
@@ -1474,19 +1536,10 @@ int run_batch_union(Engine& E, std::vector<HostMember>& hm, const Opts& O, int* 
   }
   if (rc) { fail_all(rc); return rc; }
   const size_t esz = O.out_bits / 8;
-  // download the union's truss numbers, then hand each member its slot range
-  std::vector<uint8_t> host_out;
-  void* dst_all = nullptr;
-  if (G == 1) dst_all = hm[0].out;
-  else { host_out.resize(out_bytes); dst_all = host_out.data(); }
-  rc = download(E, dst_all, J.out, out_bytes, s);
+  // download the union's truss numbers straight into the members' buffers
+  rc = G == 1 ? download(E, hm[0].out, J.out, out_bytes, s) : download_union(E, hm, J.members, J.out, esz, s);
   if (rc) { fail_all(rc); return rc; }
   CU(cudaStreamSynchronize(s));
-  if (G > 1) {
-#pragma omp parallel for schedule(dynamic, 1)
-    for (long long g = 0; g < (long long)G; ++g)
-      std::memcpy(hm[g].out, host_out.data() + (size_t)J.members[g].sb * esz, (size_t)J.members[g].w * esz);
-  }
   auto t1 = std::chrono::steady_clock::now();
   const double total_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   for (size_t g = 0; g < G; ++g) {
