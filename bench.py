@@ -44,7 +44,10 @@ WORKLOADS = {
     "rmat20": dict(kind="rmat", scale=20, ef=16, seed=2, desc="R-MAT scale 20, edge factor 16, seed 2"),
     "rmat21": dict(kind="rmat", scale=21, ef=16, seed=2, desc="R-MAT scale 21, edge factor 16, seed 2"),
     "er1": dict(kind="er", n=100_000, m=1_000_000, seed=1,
-                desc="Erdos-Renyi n=100,000, m=1,000,000 distinct pairs, seed 1"),
+                desc="Erdos-Renyi n=100,000, m=1,000,000 distinct pairs, seed 1 (config 1)"),
+    "dbg": dict(kind="dbg", seq_len=20_000_000, k=21, copies=1000, seg_len=10_000, mut_rate=0.05, seed=3,
+                desc="de Bruijn 21-mer graph of a 20,000,000-base seeded sequence plus 1,000 mutated 10 kb "
+                     "segment copies, seed 3 (config 3)"),
 }
 CPU_SAMPLE_SCALE = 16
 
@@ -59,6 +62,9 @@ def make_graph(spec):
         return gen.rmat(spec["scale"], spec["ef"], seed=spec["seed"])
     if spec["kind"] == "er":
         return gen.erdos_renyi(spec["n"], spec["m"], spec["seed"])
+    if spec["kind"] == "dbg":
+        return gen.debruijn(spec["seq_len"], spec["k"], spec["copies"], spec["seg_len"], spec["mut_rate"],
+                            spec["seed"])
     raise ValueError(spec)
 
 

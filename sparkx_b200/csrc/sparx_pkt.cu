@@ -1824,6 +1824,37 @@ struct LaneHook : ServeHook {
     }
     S->cv_done.notify_all();
     if (hm.empty()) return SPARX_OK;
+    int rc = join_group(E, J, ctx, s, hm, ok, joined);
+    if (rc == SPARX_E_CUDA) return rc;
+    if (rc) {
+      // one of them could not be prepared (an input defect, parallel edges, no
+      // room): try them one by one, so the others still join
+      std::vector<ServerReq*> back;
+      for (size_t i = 0; i < hm.size(); ++i) {
+        std::vector<HostMember> one{hm[i]};
+        one[0].index = 0;
+        std::vector<ServerReq*> r1{ok[i]};
+        const int r = join_group(E, J, ctx, s, one, r1, joined);
+        if (r == SPARX_E_CUDA) return r;
+        if (r) back.push_back(ok[i]);
+      }
+      // the rest run in a fresh union, through the batch path that names the error
+      std::lock_guard<std::mutex> lk(S->mu);
+      for (auto it = back.rbegin(); it != back.rend(); ++it) {
+        (*it)->running = false;
+        (*it)->fresh_only = true;
+        S->queue.push_front(*it);
+      }
+      S->cv_work.notify_all();
+    }
+    return SPARX_OK;
+  }
+
+  // Prepare a group of newcomers on the second engine and join them behind
+  // the running members; nonzero: the group could not be prepared (nothing
+  // joined), SPARX_E_CUDA: the device failed.
+  int join_group(Engine& E, UnionJob& J, PeelCtx& ctx, cudaStream_t s, std::vector<HostMember>& hm,
+                 std::vector<ServerReq*>& ok, uint32_t* joined) {
     UnionJob PJ;
     uint64_t Np = 0, Wp = 0, maxn = 0;
     for (const HostMember& h : hm) {
@@ -1848,15 +1879,9 @@ struct LaneHook : ServeHook {
       if (!prc) prc = run_union(*P, PJ, S->O, ps);
     }
     if (prc) {
-      // an input defect, a multigraph or no room: these requests run in a fresh union
-      std::lock_guard<std::mutex> lk(S->mu);
-      for (auto it = ok.rbegin(); it != ok.rend(); ++it) {
-        (*it)->running = false;
-        (*it)->fresh_only = true;
-        S->queue.push_front(*it);
-      }
-      S->cv_work.notify_all();
-      return SPARX_OK;
+      cudaStreamSynchronize(P->stream);
+      cudaGetLastError();
+      return prc == SPARX_E_CUDA ? SPARX_E_CUDA : prc;
     }
     // join: the prepared arrays go behind the union's, ids shifted
     const Layout& L = J.L;
@@ -1920,7 +1945,7 @@ struct LaneHook : ServeHook {
     ctx.m = m0 + mp;
     ctx.Ws = W0 + Wp;
     ctx.csr_slots += Wp;
-    *joined = (uint32_t)nm.size();
+    *joined += (uint32_t)nm.size();
     S->joined += nm.size();
     return SPARX_OK;
   }
