@@ -1637,6 +1637,10 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
 
 constexpr int kServerLanes = 4;                // default; SPARX_SERVE_LANES (1..16) overrides
 constexpr uint32_t kServeMaxMembers = 4096;   // members per served union, joined ones included
+// a union holding a member with more slots than this takes no joins: every
+// member advances one step per wave, and such a member's waves would set the
+// pace of small newcomers (R-MAT-24's waves take milliseconds)
+constexpr uint64_t kJoinMaxMemberSlots = 1ull << 26;
 
 struct ServerReq {
   uint64_t ticket = 0;
@@ -1685,6 +1689,7 @@ struct sparx_server {
   uint64_t next_ticket = 1;
   bool stop = false;
   int nlanes = kServerLanes;
+  int idle = 0;  // lanes waiting for work (a newcomer goes to one of them rather than joining)
   std::atomic<uint64_t> unions{0}, joined{0};  // served unions started; requests that joined one running
 };
 
@@ -1714,6 +1719,7 @@ struct LaneHook : ServeHook {
   std::vector<char> delivered;
   uint64_t N_cap = 0, W_cap = 0;    // the union's room
   uint64_t max_n0 = 0;              // largest initial member (the hub pool was sized for it)
+  uint64_t max_member_w = 0;        // slots of the union's largest member
 
   int deliver(Engine& E, UnionJob& J, uint32_t G, cudaStream_t s) {
     const Layout& L = J.L;
@@ -1781,9 +1787,19 @@ struct LaneHook : ServeHook {
     *joined = 0;
     S->admit_host[lane] = 0;
     if (J.multi) return SPARX_OK;  // a deduplicated union has no room for more rows: wait for a lane
+    if (max_member_w > kJoinMaxMemberSlots) return SPARX_OK;
     std::vector<ServerReq*> take;
     {
       std::lock_guard<std::mutex> lk(S->mu);
+      if (S->idle > 0) return SPARX_OK;  // an idle lane starts them at once, at their own pace
+      // the largest lane drains (takes no joins) while a request only it can hold is waiting
+      uint64_t other = 0;
+      for (size_t i = 0; i < S->lane_budget.size(); ++i)
+        if ((int)i != lane) other = std::max<uint64_t>(other, S->lane_budget[i] - prep_budget(S->lane_budget[i]));
+      const uint64_t mine = S->lane_budget[lane] - prep_budget(S->lane_budget[lane]);
+      if (mine > other)
+        for (const ServerReq* r : S->queue)
+          if (!layout_fits(r->h.n, r->h.w, kServeMaxMembers, 4, r->h.n, other)) return SPARX_OK;
       uint64_t N = ctx.N, W = ctx.Ws, pn = 0, pw = 0, pmax = 0;
       uint32_t G = ctx.G;
       for (auto it = S->queue.begin(); it != S->queue.end();) {
@@ -1938,7 +1954,10 @@ struct LaneHook : ServeHook {
       J.members.push_back(M);
       (void)M;
     }
-    for (ServerReq* r : ok) reqs.push_back(r);
+    for (ServerReq* r : ok) {
+      reqs.push_back(r);
+      max_member_w = std::max<uint64_t>(max_member_w, r->h.w);
+    }
     delivered.resize(reqs.size(), 0);
     ctx.N = N0 + (uint32_t)Np;
     ctx.G = G1;
@@ -2012,7 +2031,9 @@ void server_worker(sparx_server* S, int lane) {
     bool fresh = false;
     {
       std::unique_lock<std::mutex> lk(S->mu);
+      S->idle += 1;
       S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
+      S->idle -= 1;
       if (S->queue.empty()) {
         if (S->stop) return;
         continue;
@@ -2095,6 +2116,7 @@ void server_worker(sparx_server* S, int lane) {
     hook.N_cap = N + extra / 2;
     hook.W_cap = W + extra;
     hook.max_n0 = mx;
+    for (const HostMember& h : hm) hook.max_member_w = std::max<uint64_t>(hook.max_member_w, h.w);
     hook.delivered.assign(hook.reqs.size(), 0);
     J.N = N;
     J.W = W;
