@@ -245,6 +245,8 @@ typedef struct sparx_tuning {
   uint32_t support_kernel;  /* 1 balanced edge form, 2 vertex form (1) */
   uint32_t compact_pct;     /* peel: rebuild the working rows once live entries fill at most
                                this percentage of them (85) */
+  uint32_t hash_min_degree; /* peel: rows of at least this degree (>= 8) get a hash table that the
+                               per-lane search probes instead of a binary search; 0 = none (0) */
 } sparx_tuning;
 
 int sparx_tuning_default(sparx_tuning* t);
@@ -263,7 +265,7 @@ int sparx_tuning_load(const char* path);
  * Autotune on one sample graph (host, the reference's layout): coordinate
  * descent from the defaults over the support form and sampling threshold
  * (timed by the support pass), then the hub floor, merge ratio and compaction
- * fill (timed by orientation + peel); `repeats` decompositions per candidate
+ * fill and row hash floor (timed by orientation + peel); `repeats` decompositions per candidate
  * (median).  Stores the winner under the sample's key and returns it.
  */
 int sparx_autotune(const uint64_t* offsets, uint64_t n_plus_1, const uint64_t* neighbours, uint64_t width,

@@ -72,6 +72,10 @@ struct Union {  // the prepared concatenated graph, as the peel sees it
   const uint32_t* hub_map;         // map pool: hub k's neighbour id w -> hub_map[hub_base[k] + w]
   const uint32_t* hub_base;        // per hub: its map's start in the pool minus its member's first
                                    // vertex id (u32 arithmetic, so base + w wraps into the map)
+  const unsigned long long* hpool; // row hash tables (nullptr = none): vertex v's at 4 * off0[v]
+  const uint32_t* off0;            // the rows' original offsets (hash table positions)
+  uint2* qh[2];                    // per queue entry: {hash table position, log2 capacity} or 0
+  uint32_t hash_min;               // rows of at least this degree have a hash table (0: none)
   uint32_t n;
   uint32_t m;
   uint32_t width;
@@ -96,8 +100,14 @@ struct PeelArrays {
   const uint32_t* hub_map;
   const uint32_t* hub_base;
   const uint32_t* mu;    // multigraphs: multiplicity per edge id (nullptr: simple graph)
+  const unsigned long long* hpool;
+  const uint32_t* off0;
+  uint2* qh0;
+  uint2* qh1;
   uint32_t n;
   uint32_t merge_ratio;  // merge the rows when the longer is at most this many times the shorter
+  uint32_t hash_min;
+  uint32_t pad;
 };
 
 // Field-by-field copy of a device-resident Union into registers (a struct
@@ -118,18 +128,32 @@ struct UnionRegs {
   const uint32_t* __restrict__ hub_map;
   const uint32_t* __restrict__ hub_base;
   const uint32_t* __restrict__ mu;
+  const unsigned long long* __restrict__ hpool;
+  const uint32_t* __restrict__ off0;
+  uint2* qh0;
+  uint2* qh1;
   uint32_t n;
+  uint32_t hash_min;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
       : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]),
         qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), hub_base(p->hub_base),
-        mu(nullptr), n(p->n) {}
+        mu(nullptr), hpool(p->hpool), off0(p->off0), qh0(p->qh[0]), qh1(p->qh[1]), n(p->n),
+        hash_min(p->hash_min) {}
   __device__ __forceinline__ UnionRegs(const Union* p, const PeelArrays& a)
       : off(p->off), row(p->row), ocol(a.ocol), osrc(a.osrc), es(a.es),
         act0(a.act0), act1(a.act1), q0(a.q0), q1(a.q1),
         qd0(a.qd0), qd1(a.qd1), hub_slot(a.hub_slot), hub_map(a.hub_map), hub_base(a.hub_base), mu(a.mu),
-        n(a.n) {}
+        hpool(a.hpool), off0(a.off0), qh0(a.qh0), qh1(a.qh1), n(a.n), hash_min(a.hash_min) {}
 };
+
+// Row hash tables: vertex v of original degree d >= hash_min (and no hub map)
+// has an open-addressed table of its (neighbour id | edge id << 32) pairs with
+// 2^(1 + ceil(log2 d)) entries (at most 4d, so at 4 * off0[v] the tables of
+// consecutive vertices never overlap), probed linearly from a multiplicative
+// hash of the id; an empty entry is all ones.
+__device__ __forceinline__ uint32_t hash_log2cap(uint32_t d) { return 1u + (d > 1 ? 32u - __clz(d - 1) : 0u); }
+__device__ __forceinline__ uint32_t hash_first(uint32_t w, uint32_t lg) { return (w * 0x9E3779B1u) >> (32 - lg); }
 
 // A queue-entry descriptor whose longer row belongs to a hub carries kHubDesc
 // in place of the longer row's begin and the hub's map base in place of its
@@ -1237,17 +1261,24 @@ struct WaveArgs {
 // Rows of frontier edge x in the working CSR: {shorter row start, its length,
 // longer row begin, longer row end}, or {.., .., kHubDesc, hub map base} when
 // the longer row's vertex has a hub map.  The length is the edge's work.
-__device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x) {
+// *hq: the longer row's hash table {position, log2 capacity}, or {0, 0}.
+__device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x, uint2* hq) {
   const uint32_t u = __ldg(U.osrc + x), v = __ldg(U.ocol + x);
   const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
   const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
   const bool u_short = ue - ub <= ve - vb;
+  *hq = make_uint2(0, 0);
   if (U.hub_slot) {
     const uint32_t hs = __ldg(U.hub_slot + (u_short ? v : u));
     if (hs != kInvalid) {
       const uint32_t base = __ldg(U.hub_base + hs);
       return u_short ? make_uint4(ub, ue - ub, kHubDesc, base) : make_uint4(vb, ve - vb, kHubDesc, base);
     }
+  }
+  if (U.hash_min) {
+    const uint32_t lv = u_short ? v : u;
+    const uint32_t b0 = __ldg(U.off0 + lv), d0 = __ldg(U.off0 + lv + 1) - b0;
+    if (d0 >= U.hash_min) *hq = make_uint2(4 * b0, hash_log2cap(d0));
   }
   return u_short ? make_uint4(ub, ue - ub, vb, ve) : make_uint4(vb, ve - vb, ub, ue);
 }
@@ -1363,13 +1394,15 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, co
   // the queue being built (q_sel names the one being processed)
   unsigned long long* qnext = q_sel ? U.q0 : U.q1;
   uint4* qdnext = q_sel ? U.qd0 : U.qd1;
+  uint2* qhnext = q_sel ? U.qh0 : U.qh1;
   __syncwarp();
   const uint32_t n = ps.n;
   if (n == 0) return;
   const uint32_t lane = lane_id();
   const uint32_t x0 = lane < n ? ps.eid[lane] : 0u, x1 = lane + 32 < n ? ps.eid[lane + 32] : 0u;
-  const uint4 d0 = lane < n ? edge_desc(U, x0) : make_uint4(0, 0, 0, 0);
-  const uint4 d1 = lane + 32 < n ? edge_desc(U, x1) : make_uint4(0, 0, 0, 0);
+  uint2 h0 = make_uint2(0, 0), h1 = make_uint2(0, 0);
+  const uint4 d0 = lane < n ? edge_desc(U, x0, &h0) : make_uint4(0, 0, 0, 0);
+  const uint4 d1 = lane + 32 < n ? edge_desc(U, x1, &h1) : make_uint4(0, 0, 0, 0);
   const unsigned long long p0 = warp_incl_scan(d0.y), p1 = warp_incl_scan(d1.y);
   const unsigned long long t0 = __shfl_sync(kFull, p0, 31), t1 = __shfl_sync(kFull, p1, 31);
   unsigned long long old = 0;
@@ -1383,6 +1416,7 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, co
     if (pos + lane < M.m) {
       qnext[M.eb + pos + lane] = ((ws + p0 - d0.y) << kEidBits) | (x0 - M.eb);
       qdnext[M.eb + pos + lane] = d0;
+      if (U.hash_min) qhnext[M.eb + pos + lane] = h0;
     } else {
       atomicOr(err, kErrCapacity);
     }
@@ -1391,6 +1425,7 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, co
     if (pos + 32 + lane < M.m) {
       qnext[M.eb + pos + 32 + lane] = ((ws + t0 + p1 - d1.y) << kEidBits) | (x1 - M.eb);
       qdnext[M.eb + pos + 32 + lane] = d1;
+      if (U.hash_min) qhnext[M.eb + pos + 32 + lane] = h1;
     } else {
       atomicOr(err, kErrCapacity);
     }
@@ -1741,10 +1776,24 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
             if (lane == 0) s_cnt[2][wib]++;
             m_e = kInvalid;
             if (look) {
+              const uint2 hq = U.hash_min ? (q_sel ? U.qh1 : U.qh0)[M.eb + x] : make_uint2(0, 0);
               if (hubs && (lb & kHubDesc)) {
                 // the longer row's vertex has a hub map: one lookup
                 h = __ldg(U.hub_map + (uint32_t)(le + w));
                 p = h != kInvalid ? 0u : kInvalid;
+              } else if (hq.y) {
+                // the longer row has a hash table: probe from the id's hash
+                const unsigned long long* tb = U.hpool + hq.x;
+                const uint32_t mask = (1u << hq.y) - 1;
+                uint32_t at = hash_first(w, hq.y);
+#pragma unroll 1
+                for (uint32_t it = 0; it <= mask; ++it) {
+                  const unsigned long long en = __ldg(tb + at);
+                  const uint32_t id = (uint32_t)en;
+                  if (id == w) { h = (uint32_t)(en >> 32); p = 0; break; }
+                  if (id == kInvalid) break;
+                  at = (at + 1) & mask;
+                }
               } else {
                 p = find_in_row(U.row, lb, le, w);
                 if (p != kInvalid) h = (uint32_t)(__ldg(U.row + p) >> 32);
@@ -2128,8 +2177,12 @@ __global__ void __launch_bounds__(256) k_refresh_desc(const Union* __restrict__ 
   const Member M = mem[g];
   const unsigned long long* q = (s.q_sel ? U.q1 : U.q0) + M.eb;
   uint4* qd = (s.q_sel ? U.qd1 : U.qd0) + M.eb;
-  for (uint32_t x = part * blockDim.x + threadIdx.x; x < cnt; x += per * blockDim.x)
-    qd[x] = edge_desc(U, M.eb + (uint32_t)(q[x] & kEidMask));
+  uint2* qh = U.hash_min ? (s.q_sel ? U.qh1 : U.qh0) + M.eb : nullptr;
+  for (uint32_t x = part * blockDim.x + threadIdx.x; x < cnt; x += per * blockDim.x) {
+    uint2 hq;
+    qd[x] = edge_desc(U, M.eb + (uint32_t)(q[x] & kEidMask), &hq);
+    if (qh) qh[x] = hq;
+  }
 }
 
 // Publish the compacted rows and resume the loop.
@@ -2673,6 +2726,32 @@ __global__ void k_replan(const Member* __restrict__ mem, const MemberState* __re
     ctl->t_start = globaltimer();
     ctl->done = 0;
     ctl->exit_reason = kExitNone;
+  }
+}
+
+// Row hash tables (see hash_log2cap): a warp per row of degree >= hash_min
+// without a hub map; pairs go in by 64-bit compare-and-swap on empty entries.
+__global__ void __launch_bounds__(256) k_hash_fill(const uint32_t* __restrict__ off0,
+                                                   const unsigned long long* __restrict__ row0, uint32_t n,
+                                                   uint32_t hash_min, const uint32_t* __restrict__ hub_slot,
+                                                   unsigned long long* __restrict__ pool) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(off0 + u), d = __ldg(off0 + u + 1) - b;
+    if (d < hash_min || (hub_slot && __ldg(hub_slot + u) != kInvalid)) continue;
+    const uint32_t lg = hash_log2cap(d), mask = (1u << lg) - 1;
+    unsigned long long* tb = pool + 4ull * b;
+    for (uint32_t s = b + lane; s < b + d; s += 32) {
+      const unsigned long long pr = __ldg(row0 + s);
+      if ((uint32_t)(pr >> 32) == kInvalid) continue;  // a self-loop: no edge
+      uint32_t at = hash_first((uint32_t)pr, lg);
+      for (uint32_t it = 0; it <= mask; ++it) {
+        if (atomicCAS(tb + at, ~0ull, pr) == ~0ull) break;
+        at = (at + 1) & mask;
+      }
+    }
   }
 }
 

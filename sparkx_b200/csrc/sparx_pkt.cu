@@ -71,6 +71,7 @@ struct Tuning {
   uint32_t sample_min = 64;        // support: longer out-lists from this length go through 64 samples
   uint32_t support_kernel = 1;     // 1 balanced edge form, 2 vertex form
   uint32_t compact_pct = 85;       // rebuild the peel's rows when live entries fill <= this % of them
+  uint32_t hash_min_degree = 0;    // rows of at least this degree get a hash table for the per-lane search (0: none)
 };
 
 // Degree-distribution signature: log2 of the slot count, log2 bucket of the
@@ -106,16 +107,16 @@ thread_local TuneKey g_tune_last_key;
 bool valid_tuning(const Tuning& t) {
   return t.merge_ratio >= 1 && t.merge_ratio <= 1024 && (t.hub_min_degree == 0 || t.hub_min_degree >= 256) &&
          t.sample_min >= 2 && (t.support_kernel == 1 || t.support_kernel == 2) && t.compact_pct >= 10 &&
-         t.compact_pct <= 100;
+         t.compact_pct <= 100 && (t.hash_min_degree == 0 || t.hash_min_degree >= 8);
 }
 
-// Text cache: one line per key, "log_w log_dmax skew8 merge hub sample kernel compact".
+// Text cache: one line per key, "log_w log_dmax skew8 merge hub sample kernel compact hash".
 int tune_load_locked(const char* path) {
   FILE* f = std::fopen(path, "r");
   if (!f) return SPARX_E_NOT_FOUND;
-  unsigned a, b, c, d, e, g, h, i;
-  while (std::fscanf(f, "%u %u %u %u %u %u %u %u", &a, &b, &c, &d, &e, &g, &h, &i) == 8) {
-    Tuning t{d, e, g, h, i};
+  unsigned a, b, c, d, e, g, h, i, j;
+  while (std::fscanf(f, "%u %u %u %u %u %u %u %u %u", &a, &b, &c, &d, &e, &g, &h, &i, &j) == 9) {
+    Tuning t{d, e, g, h, i, j};
     if (valid_tuning(t)) g_tune[TuneKey{a, b, c}] = t;
   }
   std::fclose(f);
@@ -126,9 +127,9 @@ int tune_save_locked(const char* path) {
   FILE* f = std::fopen(path, "w");
   if (!f) return SPARX_E_ARG;
   for (const auto& kv : g_tune)
-    std::fprintf(f, "%u %u %u %u %u %u %u %u\n", kv.first.log_w, kv.first.log_dmax, kv.first.skew8,
+    std::fprintf(f, "%u %u %u %u %u %u %u %u %u\n", kv.first.log_w, kv.first.log_dmax, kv.first.skew8,
                  kv.second.merge_ratio, kv.second.hub_min_degree, kv.second.sample_min, kv.second.support_kernel,
-                 kv.second.compact_pct);
+                 kv.second.compact_pct, kv.second.hash_min_degree);
   std::fclose(f);
   return SPARX_OK;
 }
@@ -279,6 +280,8 @@ struct Engine {
   int wave_blocks_multi = 0;  // k_wave<true> grid (multigraphs)
   char* ws2 = nullptr;        // multigraph rows, multiplicities and slot map (allocated on first use)
   size_t ws2_cap = 0;
+  char* ws3 = nullptr;        // row hash tables and their queue descriptors (allocated on first use)
+  size_t ws3_cap = 0;
   ulonglong4* trace = nullptr;  // wave trace records (SPARX_TRACE_FILE set)
   std::mutex mu;
 };
@@ -350,6 +353,20 @@ int ensure_ws(Engine& E, size_t bytes, bool slack = true) {
     }
   }
   E.ws_cap = cap;
+  return SPARX_OK;
+}
+
+int ensure_ws3(Engine& E, size_t bytes) {
+  if (E.ws3_cap >= bytes) return SPARX_OK;
+  if (E.ws3) { CU(cudaStreamSynchronize(E.stream)); CU(cudaFree(E.ws3)); E.ws3 = nullptr; E.ws3_cap = 0; }
+  cudaError_t e = cudaMalloc(&E.ws3, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("hash table workspace of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+    E.ws3 = nullptr;
+    return SPARX_E_OOM;
+  }
+  E.ws3_cap = bytes;
   return SPARX_OK;
 }
 
@@ -593,8 +610,14 @@ PeelArrays peel_arrays(const Union& U) {
   a.hub_map = U.hub_map;
   a.hub_base = U.hub_base;
   a.mu = nullptr;
+  a.hpool = U.hpool;
+  a.off0 = U.off0;
+  a.qh0 = U.qh[0];
+  a.qh1 = U.qh[1];
   a.n = U.n;
   a.merge_ratio = Tuning{}.merge_ratio;
+  a.hash_min = U.hash_min;
+  a.pad = 0;
   return a;
 }
 
@@ -811,6 +834,26 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     d_hub_base = hbase;
   }
   J.hubs = hubs;
+  // row hash tables for the peel's per-lane search (tuned; not in served unions,
+  // whose joining rows would have none)
+  unsigned long long* hpool = nullptr;
+  uint2* qh0 = nullptr;
+  uint2* qh1 = nullptr;
+  uint32_t hash_min = 0;
+  if (T.hash_min_degree && !J.support_only && !J.prep_only && !J.hook && Ws < (1ull << 30) && Ws) {
+    const uint64_t Mx = std::max<uint64_t>(W / 2, 1);
+    const size_t pool_b = align_up(32ull * Ws), qh_b = align_up(8ull * Mx);
+    int rc = ensure_ws3(E, pool_b + 2 * qh_b);
+    if (rc) return rc;
+    hpool = (unsigned long long*)E.ws3;
+    qh0 = (uint2*)(E.ws3 + pool_b);
+    qh1 = (uint2*)(E.ws3 + pool_b + qh_b);
+    hash_min = T.hash_min_degree;
+    CU(cudaMemsetAsync(hpool, 0xFF, 32ull * Ws, s));
+    k_hash_fill<<<grid_for(32ull * N, 256, E.sm_count * 16), 256, 0, s>>>(J.off, row0, N, hash_min, d_hub_slot,
+                                                                            hpool);
+    J.launches += 1;
+  }
   CU(cudaEventRecord(E.tev[2], s));
 
   // -- support (Kernel C) --
@@ -860,6 +903,11 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     U.hub_slot = d_hub_slot;
     U.hub_map = d_hub_map;
     U.hub_base = d_hub_base;
+    U.hpool = hpool;
+    U.off0 = J.off;
+    U.qh[0] = qh0;
+    U.qh[1] = qh1;
+    U.hash_min = hash_min;
     U.n = N;
     U.m = (uint32_t)m;
     U.width = (uint32_t)W;
@@ -1659,6 +1707,7 @@ void engine_release(Engine* E) {
   if (E->peel.exec) { cudaGraphExecDestroy(E->peel.exec); cudaGraphDestroy(E->peel.graph); }
   if (E->ws) cudaFree(E->ws);
   if (E->ws2) cudaFree(E->ws2);
+  if (E->ws3) cudaFree(E->ws3);
   if (E->trace) cudaFree(E->trace);
   for (int i = 0; i < 2; ++i) {
     if (E->pinned[i]) cudaFreeHost(E->pinned[i]);
@@ -2568,6 +2617,7 @@ int sparx_tuning_default(sparx_tuning* t) {
   t->sample_min = d.sample_min;
   t->support_kernel = d.support_kernel;
   t->compact_pct = d.compact_pct;
+  t->hash_min_degree = d.hash_min_degree;
   return SPARX_OK;
 }
 
@@ -2591,7 +2641,8 @@ int sparx_tuning_signature(const uint64_t* offsets, uint64_t n_plus_1, uint32_t 
 
 namespace {
 Tuning from_c(const sparx_tuning* t) {
-  return Tuning{t->merge_ratio, t->hub_min_degree, t->sample_min, t->support_kernel, t->compact_pct};
+  return Tuning{t->merge_ratio, t->hub_min_degree, t->sample_min, t->support_kernel, t->compact_pct,
+                t->hash_min_degree};
 }
 void to_c(const Tuning& t, sparx_tuning* o) {
   o->struct_size = sizeof(sparx_tuning);
@@ -2600,6 +2651,7 @@ void to_c(const Tuning& t, sparx_tuning* o) {
   o->sample_min = t.sample_min;
   o->support_kernel = t.support_kernel;
   o->compact_pct = t.compact_pct;
+  o->hash_min_degree = t.hash_min_degree;
 }
 }  // namespace
 
@@ -2719,6 +2771,9 @@ int autotune_core(RunF run, uint32_t repeats, Tuning* best_out, TuneKey* key_out
   std::vector<Tuning> c4;
   for (uint32_t cp : {75u, 95u}) { Tuning t = cur; t.compact_pct = cp; c4.push_back(t); }
   if ((rc = try_group(c4, false))) return rc;
+  std::vector<Tuning> c5;
+  for (uint32_t hm : {32u, 128u, 512u}) { Tuning t = cur; t.hash_min_degree = hm; c5.push_back(t); }
+  if ((rc = try_group(c5, false))) return rc;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = cur;

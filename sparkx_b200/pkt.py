@@ -88,7 +88,8 @@ class _GraphView(ctypes.Structure):
 
 class _Tuning(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint32) for name in
-                ("struct_size", "merge_ratio", "hub_min_degree", "sample_min", "support_kernel", "compact_pct")]
+                ("struct_size", "merge_ratio", "hub_min_degree", "sample_min", "support_kernel", "compact_pct",
+                 "hash_min_degree")]
 
 
 EXPORTS = [
@@ -546,6 +547,7 @@ class PktTuning:
     sample_min: int = 64
     support_kernel: int = 1
     compact_pct: int = 85
+    hash_min_degree: int = 0
 
     def c(self) -> _Tuning:
         t = _Tuning()

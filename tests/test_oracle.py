@@ -322,3 +322,20 @@ def test_multigraph_larger_graphs_pkt_equals_fast_peel():
         want = O.fast_truss(g.offsets, g.neighbours)[0]
         assert np.array_equal(O.pkt(g.offsets, g.neighbours, threads=4), want)
         assert O.verify(g.offsets, g.neighbours, want, threads=4) == -1
+
+
+def test_every_pinned_truss_is_certified_by_the_verifier():
+    """Each fixture's mode-0 truss carries two independent oracles or a verifier pass; the two
+    largest (R-MAT-22 and the R-MAT-24 tail, pinned by the independent peel alone) carry a pass
+    of the corrected verifier (symmetry, support >= k - 2 inside the k-truss, local
+    maximality), recorded by tests/golden/make_golden.py."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "fixtures.json")) as f:
+        fx = json.load(f)
+    for name, entry in fx.items():
+        m0 = entry["modes"]["0"]
+        assert m0.get("verified") is True or len(m0["oracles"]) >= 2, name
+    for name in ("cfg2_rmat22", "cfg5_rmat24_tail", "rmat20"):
+        assert fx[name]["modes"]["0"].get("verified") is True, name
+    assert set(fx["rmat20"]["modes"]["0"]["oracles"]) == {"pkt", "fast"}

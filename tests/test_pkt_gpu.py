@@ -294,3 +294,15 @@ def test_sharded_batch_single_rank_uses_the_engine():
     assert out.parts == [[0, 1, 2, 3]]
     for g, (t, st, status) in zip(gs, out.results):
         assert status == 0 and np.array_equal(t, O.pkt(g.offsets, g.neighbours))
+
+
+def test_gpu_truss_passes_the_verifier_on_rmat18():
+    """The corrected verifier (the definition, no peel involved) accepts the GPU's R-MAT-18
+    decomposition and rejects it with one slot changed."""
+    g = gen.rmat(18, 16, seed=2)
+    t, _ = run_pkt(g.offsets, g.neighbours, O32)
+    assert O.verify(g.offsets, g.neighbours, t, threads=os.cpu_count() or 1) == -1
+    bad = t.copy()
+    s = int(np.argmax(t))
+    bad[s] += 1
+    assert O.verify(g.offsets, g.neighbours, bad, threads=os.cpu_count() or 1) >= 0

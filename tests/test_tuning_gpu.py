@@ -14,8 +14,10 @@ import sparkx_b200.pkt as P
 pytestmark = pytest.mark.gpu
 O32 = P.PktOptions(out_bits=32, timeout_ms=120_000)
 
-CANDIDATES = [P.PktTuning(merge_ratio=mr, hub_min_degree=h, sample_min=smp, support_kernel=sk, compact_pct=cp)
-              for mr, h, smp, sk, cp in itertools.product((4, 16), (0, 256, 4096), (32, 256), (1, 2), (75, 95))]
+CANDIDATES = [P.PktTuning(merge_ratio=mr, hub_min_degree=h, sample_min=smp, support_kernel=sk, compact_pct=cp,
+                          hash_min_degree=hm)
+              for mr, h, smp, sk, cp, hm in itertools.product((4, 16), (0, 256, 4096), (32, 256), (1, 2), (75, 95),
+                                                              (0, 8, 64))]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -47,7 +49,7 @@ def test_every_candidate_gives_the_same_truss():
     # R-MAT-16 has rows past 1024 and 4096 entries (hub maps) and is big enough to compact
     g = gen.rmat(16, 16, seed=2)
     want = O.fast_truss(g.offsets, g.neighbours)[0]
-    for t in CANDIDATES[::3]:
+    for t in CANDIDATES[::5]:
         got, st = _with_tuning(t, lambda: P.run_pkt(g.offsets, g.neighbours, O32))
         assert np.array_equal(got, want), t
         assert (st.hub_maps > 0) == (t.hub_min_degree in (256, 4096)), (t, st.hub_maps)
@@ -59,7 +61,7 @@ def test_batched_unions_get_member_hub_maps():
     want = [O.fast_truss(m.offsets, m.neighbours)[0] for m in members]
     pairs = [(m.offsets, m.neighbours) for m in members]
     for t in (P.PktTuning(hub_min_degree=256), P.PktTuning(hub_min_degree=256, merge_ratio=4, compact_pct=95),
-              P.PktTuning(hub_min_degree=0)):
+              P.PktTuning(hub_min_degree=0), P.PktTuning(hub_min_degree=1024, hash_min_degree=16)):
         res = _with_tuning(t, lambda: P.run_batch(pairs, O32))
         for w, (truss, st, status) in zip(want, res):
             assert status == 0 and np.array_equal(truss, w), t
