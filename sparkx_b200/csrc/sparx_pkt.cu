@@ -401,23 +401,50 @@ inline int grid_for(unsigned long long items, int threads, int cap_blocks) {
   return (int)std::max<unsigned long long>(1, std::min<unsigned long long>(b, (unsigned long long)cap_blocks));
 }
 
-// host ids (u64 or u32) -> device u32 (+ base), chunked through pinned staging
+// host ids (u64 or u32) -> device u32 (+ base), chunked through pinned staging:
+// host threads narrow each chunk to u32 and check id < n while copying it into
+// the pinned buffer (so 4 bytes per slot cross PCIe, not 8), and the chunk goes
+// straight to its place in HBM.  A bad id sets kErrRange in *d_err's host twin.
 int upload_ids(Engine& E, const void* host, int bits, uint64_t count, uint32_t* dst, uint64_t n_limit,
                uint32_t base, cudaStream_t s, char* stage[2], uint32_t* d_err) {
-  const size_t esz = bits == 64 ? 8 : 4;
-  const uint64_t chunk = kStageBytes / esz;
+  (void)stage;
+  const uint64_t chunk = kStageBytes / 4;
+  bool bad = false;
   for (uint64_t c = 0, at = 0; at < count; ++c, at += chunk) {
     const int slot = (int)(c & 1);
     const uint64_t k = std::min<uint64_t>(chunk, count - at);
     CU(cudaEventSynchronize(E.pin_ev[slot]));
-    parallel_copy(E.pinned[slot], (const char*)host + at * esz, k * esz);
-    CU(cudaMemcpyAsync(stage[slot], E.pinned[slot], k * esz, cudaMemcpyHostToDevice, s));
-    const int grid = grid_for(k, 256, E.sm_count * 16);
-    if (bits == 64)
-      k_narrow_ids<<<grid, 256, 0, s>>>((const unsigned long long*)stage[slot], dst + at, k, n_limit, base, d_err);
-    else
-      k_range_ids<<<grid, 256, 0, s>>>((const uint32_t*)stage[slot], dst + at, k, (uint32_t)n_limit, base, d_err);
+    uint32_t* buf = (uint32_t*)E.pinned[slot];
+    const long long pieces = (long long)((k + (1u << 18) - 1) >> 18);
+    bool chunk_bad = false;
+#pragma omp parallel for schedule(static) reduction(|| : chunk_bad) num_threads(std::min<int>(omp_get_max_threads(), 16))
+    for (long long pi = 0; pi < pieces; ++pi) {
+      const uint64_t lo = (uint64_t)pi << 18, hi = std::min<uint64_t>(k, lo + (1u << 18));
+      bool b = false;
+      if (bits == 64) {
+        const uint64_t* src = (const uint64_t*)host + at;
+        for (uint64_t i = lo; i < hi; ++i) {
+          const uint64_t x = src[i];
+          b |= x >= n_limit;
+          buf[i] = (uint32_t)x + base;
+        }
+      } else {
+        const uint32_t* src = (const uint32_t*)host + at;
+        for (uint64_t i = lo; i < hi; ++i) {
+          const uint32_t x = src[i];
+          b |= x >= n_limit;
+          buf[i] = x + base;
+        }
+      }
+      chunk_bad = chunk_bad || b;
+    }
+    bad = bad || chunk_bad;
+    CU(cudaMemcpyAsync(dst + at, buf, k * 4, cudaMemcpyHostToDevice, s));
     CU(cudaEventRecord(E.pin_ev[slot], s));
+  }
+  if (bad) {
+    const uint32_t flag = kErrRange;
+    CU(cudaMemcpyAsync(d_err, &flag, 4, cudaMemcpyHostToDevice, s));  // pageable: copied before return
   }
   return SPARX_OK;
 }
@@ -1361,10 +1388,8 @@ int run_host(const uint64_t* offsets, uint64_t n_plus_1, const void* nbrs, int b
   if (bad_host) { set_error("offsets: first must be 0, last must equal width, non-decreasing"); return SPARX_E_INVALID_CSR; }
   rc = upload_ids(E, nbrs, bits, width, (uint32_t*)J.nbr, n, 0, s, stage, &cnt->err);
   if (rc) return rc;
-  J.launches += (uint32_t)((n_plus_1 + kStageBytes / 8 - 1) / (kStageBytes / 8)) +
-                (uint32_t)((width + kStageBytes / (bits / 8) - 1) / (kStageBytes / (bits / 8)));
-  auto t_up_host = std::chrono::steady_clock::now();
-  (void)t_up_host;
+  // one narrowing kernel per offsets chunk (the ids are narrowed by the host)
+  J.launches += (uint32_t)((n_plus_1 + kStageBytes / 8 - 1) / (kStageBytes / 8));
   rc = kcore ? run_kcore(E, J, O, s) : run_union(E, J, O, s);
   if (rc) {
     fill_stats(J, 0, stats);
