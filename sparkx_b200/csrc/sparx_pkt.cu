@@ -1871,9 +1871,11 @@ struct LaneHook : ServeHook {
       for (size_t i = 0; i < S->lane_budget.size(); ++i)
         if ((int)i != lane) other = std::max<uint64_t>(other, S->lane_budget[i] - prep_budget(S->lane_budget[i]));
       const uint64_t mine = S->lane_budget[lane] - prep_budget(S->lane_budget[lane]);
-      if (mine > other)
+      if (other > 0 && mine > other)
         for (const ServerReq* r : S->queue)
-          if (!layout_fits(r->h.n, r->h.w, kServeMaxMembers, 4, r->h.n, other)) return SPARX_OK;
+          if (!layout_fits(r->h.n, r->h.w, kServeMaxMembers, 4, r->h.n, other) &&
+              layout_fits(r->h.n, r->h.w, kServeMaxMembers, 4, r->h.n, mine))
+            return SPARX_OK;
       uint64_t N = ctx.N, W = ctx.Ws, pn = 0, pw = 0, pmax = 0;
       uint32_t G = ctx.G;
       for (auto it = S->queue.begin(); it != S->queue.end();) {
