@@ -247,6 +247,8 @@ typedef struct sparx_tuning {
                                this percentage of them (85) */
   uint32_t hash_min_degree; /* peel: rows of at least this degree (>= 8) get a hash table that the
                                per-lane search probes instead of a binary search; 0 = none (0) */
+  uint32_t sup_hash_min;    /* support: oriented out-lists of at least this length (>= 4) get a hash
+                               table probed instead of the sampled search; 0 = none (0) */
 } sparx_tuning;
 
 int sparx_tuning_default(sparx_tuning* t);

@@ -788,12 +788,33 @@ __device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i,
 // (e, f, h) stands for mu_e * mu_f * mu_h triangles of copies, so a copy of e
 // is credited mu_f * mu_h (each hit lane adds its own product; the one-atomic
 // run credit of the simple form is for unit weights only).
-template <bool kMulti>
+//
+// kHash: out-lists of at least hash_min entries have an open-addressed table
+// of (id | position << 32) at 4 * their start in `hpool` (k_sup_hash_fill,
+// same layout rule as the row tables), probed instead of searched.
+__device__ __forceinline__ uint32_t probe_list(const unsigned long long* __restrict__ hpool, uint32_t lb,
+                                               uint32_t len, uint32_t c) {
+  const uint32_t lg = hash_log2cap(len), mask = (1u << lg) - 1;
+  const unsigned long long* tb = hpool + 4ull * lb;
+  uint32_t at = hash_first(c, lg);
+#pragma unroll 1
+  for (uint32_t it = 0; it <= mask; ++it) {
+    const unsigned long long en = __ldg(tb + at);
+    const uint32_t id = (uint32_t)en;
+    if (id == c) return (uint32_t)(en >> 32);
+    if (id == kInvalid) return kInvalid;
+    at = (at + 1) & mask;
+  }
+  return kInvalid;
+}
+
+template <bool kMulti, bool kHash>
 __global__ void __launch_bounds__(256, 8) k_support_balanced(
     const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
     const uint32_t* __restrict__ osrc, const unsigned long long* __restrict__ spref, uint32_t m,
     int2* __restrict__ es, unsigned long long* __restrict__ tri_total, uint32_t* __restrict__ err,
-    const uint32_t* __restrict__ mu, uint32_t sample_min) {
+    const uint32_t* __restrict__ mu, uint32_t sample_min, const unsigned long long* __restrict__ hpool,
+    uint32_t hash_min) {
   const uint32_t lane = lane_id();
   const unsigned long long total = spref[m];
   const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -823,8 +844,12 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
       uint32_t p = kInvalid;  // position of c in the longer list
       if (valid) {
         const uint32_t c = __ldg(ocol + sb + o);
-        const uint32_t q = lower_bound_u32(ocol, lb, le, c);
-        if (q < le && __ldg(ocol + q) == c) p = q;
+        if (kHash && le - lb >= hash_min) {
+          p = probe_list(hpool, lb, le - lb, c);
+        } else {
+          const uint32_t q = lower_bound_u32(ocol, lb, le, c);
+          if (q < le && __ldg(ocol + q) == c) p = q;
+        }
       }
       const bool hit = valid && p != kInvalid;
       if (kMulti) {
@@ -866,7 +891,8 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
         // per lane (gathered once per edge, then shuffles), leaving ~1/64 of it
         // to search
         const uint32_t flen = fle - flb;
-        const bool sampled = flen >= sample_min;
+        const bool hashed = kHash && flen >= hash_min;
+        const bool sampled = !hashed && flen >= sample_min;
         const uint32_t smp = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane) * flen) >> 6)) : 0u;
         const uint32_t smp1 = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane + 1) * flen) >> 6)) : 0u;
         do {
@@ -874,6 +900,28 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
           const uint32_t fo = (uint32_t)(kb + lane - e_start);
           const uint32_t c = __ldg(ocol + fsb + fo);
           uint32_t lo = flb, hi = fle;
+          if (hashed) {
+            const uint32_t q = probe_list(hpool, flb, flen, c);
+            const bool fh = q != kInvalid;
+            if (kMulti) {
+              if (fh) {
+                const uint32_t me = __ldg(mu + i), mf = __ldg(mu + fsb + fo), mh = __ldg(mu + q);
+                atomicAdd(&es[fsb + fo].x, (int)(me * mh));
+                atomicAdd(&es[q].x, (int)(me * mf));
+                atomicAdd(&es[i].x, (int)(mf * mh));
+                found_total += (unsigned long long)me * mf * mh;
+              }
+            } else {
+              if (fh) {
+                atomicAdd(&es[fsb + fo].x, 1);
+                atomicAdd(&es[q].x, 1);
+                found_total++;
+              }
+              const int cnt = __popc(__ballot_sync(kFull, fh));
+              if (lane == 0 && cnt) atomicAdd(&es[i].x, cnt);
+            }
+            continue;
+          }
           if (sampled) {
             uint32_t t = 0;
 #pragma unroll
@@ -2726,6 +2774,31 @@ __global__ void k_replan(const Member* __restrict__ mem, const MemberState* __re
     ctl->t_start = globaltimer();
     ctl->done = 0;
     ctl->exit_reason = kExitNone;
+  }
+}
+
+// Out-list hash tables for the support pass: a warp per vertex whose oriented
+// out-list has at least hash_min entries; entry = (id | position << 32).
+__global__ void __launch_bounds__(256) k_sup_hash_fill(const uint32_t* __restrict__ opos,
+                                                       const uint32_t* __restrict__ ocol, uint32_t n,
+                                                       uint32_t hash_min, unsigned long long* __restrict__ pool) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t b = __ldg(opos + u), d = __ldg(opos + u + 1) - b;
+    if (d < hash_min) continue;
+    const uint32_t lg = hash_log2cap(d), mask = (1u << lg) - 1;
+    unsigned long long* tb = pool + 4ull * b;
+    for (uint32_t j = b + lane; j < b + d; j += 32) {
+      const uint32_t c = __ldg(ocol + j);
+      const unsigned long long en = (unsigned long long)c | ((unsigned long long)j << 32);
+      uint32_t at = hash_first(c, lg);
+      for (uint32_t it = 0; it <= mask; ++it) {
+        if (atomicCAS(tb + at, ~0ull, en) == ~0ull) break;
+        at = (at + 1) & mask;
+      }
+    }
   }
 }
 

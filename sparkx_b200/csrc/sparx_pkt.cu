@@ -72,6 +72,7 @@ struct Tuning {
   uint32_t support_kernel = 1;     // 1 balanced edge form, 2 vertex form
   uint32_t compact_pct = 85;       // rebuild the peel's rows when live entries fill <= this % of them
   uint32_t hash_min_degree = 0;    // rows of at least this degree get a hash table for the per-lane search (0: none)
+  uint32_t sup_hash_min = 0;       // support: out-lists of at least this length are probed in a hash table (0: none)
 };
 
 // Degree-distribution signature: log2 of the slot count, log2 bucket of the
@@ -107,16 +108,18 @@ thread_local TuneKey g_tune_last_key;
 bool valid_tuning(const Tuning& t) {
   return t.merge_ratio >= 1 && t.merge_ratio <= 1024 && (t.hub_min_degree == 0 || t.hub_min_degree >= 256) &&
          t.sample_min >= 2 && (t.support_kernel == 1 || t.support_kernel == 2) && t.compact_pct >= 10 &&
-         t.compact_pct <= 100 && (t.hash_min_degree == 0 || t.hash_min_degree >= 8);
+         t.compact_pct <= 100 && (t.hash_min_degree == 0 || t.hash_min_degree >= 8) &&
+         (t.sup_hash_min == 0 || t.sup_hash_min >= 4);
 }
 
-// Text cache: one line per key, "log_w log_dmax skew8 merge hub sample kernel compact hash".
+// Text cache: one line per key,
+// "log_w log_dmax skew8 merge hub sample kernel compact hash sup_hash".
 int tune_load_locked(const char* path) {
   FILE* f = std::fopen(path, "r");
   if (!f) return SPARX_E_NOT_FOUND;
-  unsigned a, b, c, d, e, g, h, i, j;
-  while (std::fscanf(f, "%u %u %u %u %u %u %u %u %u", &a, &b, &c, &d, &e, &g, &h, &i, &j) == 9) {
-    Tuning t{d, e, g, h, i, j};
+  unsigned a, b, c, d, e, g, h, i, j, k;
+  while (std::fscanf(f, "%u %u %u %u %u %u %u %u %u %u", &a, &b, &c, &d, &e, &g, &h, &i, &j, &k) == 10) {
+    Tuning t{d, e, g, h, i, j, k};
     if (valid_tuning(t)) g_tune[TuneKey{a, b, c}] = t;
   }
   std::fclose(f);
@@ -127,9 +130,9 @@ int tune_save_locked(const char* path) {
   FILE* f = std::fopen(path, "w");
   if (!f) return SPARX_E_ARG;
   for (const auto& kv : g_tune)
-    std::fprintf(f, "%u %u %u %u %u %u %u %u %u\n", kv.first.log_w, kv.first.log_dmax, kv.first.skew8,
+    std::fprintf(f, "%u %u %u %u %u %u %u %u %u %u\n", kv.first.log_w, kv.first.log_dmax, kv.first.skew8,
                  kv.second.merge_ratio, kv.second.hub_min_degree, kv.second.sample_min, kv.second.support_kernel,
-                 kv.second.compact_pct, kv.second.hash_min_degree);
+                 kv.second.compact_pct, kv.second.hash_min_degree, kv.second.sup_hash_min);
   std::fclose(f);
   return SPARX_OK;
 }
@@ -495,7 +498,8 @@ int launch_support(int sm_count, uint32_t support_kernel, uint32_t n, uint64_t m
                    const uint32_t* opos, const uint32_t* ocol, const uint32_t* osrc, int2* es,
                    unsigned long long* spref, unsigned long long* tiles, Counters* cnt, uint32_t* heavy_list,
                    cudaStream_t s, uint32_t* launches, unsigned long long* support_elements,
-                   const uint32_t* mu = nullptr, uint32_t sample_min = Tuning{}.sample_min) {
+                   const uint32_t* mu = nullptr, uint32_t sample_min = Tuning{}.sample_min,
+                   const unsigned long long* hpool = nullptr, uint32_t hash_min = 0) {
   if (m == 0) return SPARX_OK;
   uint32_t slots = 8;
   while (slots < 2 * max_dplus) slots <<= 1;
@@ -514,12 +518,22 @@ int launch_support(int sm_count, uint32_t support_kernel, uint32_t n, uint64_t m
     return SPARX_OK;
   }
   exclusive_scan<unsigned long long>(SupportWork{opos, osrc, ocol}, m, spref, tiles, &cnt->grand, s);
-  if (mu)
-    k_support_balanced<true><<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri,
-                                                          &cnt->err, mu, sample_min);
-  else
-    k_support_balanced<false><<<sm_count * 8, 256, 0, s>>>(opos, ocol, osrc, spref, (uint32_t)m, es, &cnt->tri,
-                                                           &cnt->err, nullptr, sample_min);
+  const int g = sm_count * 8;
+  const uint32_t mm = (uint32_t)m;
+  if (hpool && hash_min) {
+    if (mu)
+      k_support_balanced<true, true><<<g, 256, 0, s>>>(opos, ocol, osrc, spref, mm, es, &cnt->tri, &cnt->err, mu,
+                                                       sample_min, hpool, hash_min);
+    else
+      k_support_balanced<false, true><<<g, 256, 0, s>>>(opos, ocol, osrc, spref, mm, es, &cnt->tri, &cnt->err,
+                                                        nullptr, sample_min, hpool, hash_min);
+  } else if (mu) {
+    k_support_balanced<true, false><<<g, 256, 0, s>>>(opos, ocol, osrc, spref, mm, es, &cnt->tri, &cnt->err, mu,
+                                                      sample_min, nullptr, 0);
+  } else {
+    k_support_balanced<false, false><<<g, 256, 0, s>>>(opos, ocol, osrc, spref, mm, es, &cnt->tri, &cnt->err,
+                                                       nullptr, sample_min, nullptr, 0);
+  }
   *launches += 4;
   CU(cudaMemcpyAsync(support_elements, spref + m, 8, cudaMemcpyDeviceToHost, s));
   return SPARX_OK;
@@ -863,23 +877,40 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   J.hubs = hubs;
   // row hash tables for the peel's per-lane search (tuned; not in served unions,
   // whose joining rows would have none)
+  // and out-list hash tables for the support pass (tuned)
   unsigned long long* hpool = nullptr;
+  unsigned long long* spool = nullptr;
   uint2* qh0 = nullptr;
   uint2* qh1 = nullptr;
-  uint32_t hash_min = 0;
-  if (T.hash_min_degree && !J.support_only && !J.prep_only && !J.hook && Ws < (1ull << 30) && Ws) {
+  uint32_t hash_min = 0, sup_hash_min = 0;
+  {
+    const bool peel_hash = T.hash_min_degree && !J.support_only && !J.prep_only && !J.hook &&
+                           Ws < (1ull << 30) && Ws;
+    const bool sup_hash = T.sup_hash_min && m > 0 && m < (1ull << 28);
     const uint64_t Mx = std::max<uint64_t>(W / 2, 1);
-    const size_t pool_b = align_up(32ull * Ws), qh_b = align_up(8ull * Mx);
-    int rc = ensure_ws3(E, pool_b + 2 * qh_b);
-    if (rc) return rc;
-    hpool = (unsigned long long*)E.ws3;
-    qh0 = (uint2*)(E.ws3 + pool_b);
-    qh1 = (uint2*)(E.ws3 + pool_b + qh_b);
-    hash_min = T.hash_min_degree;
-    CU(cudaMemsetAsync(hpool, 0xFF, 32ull * Ws, s));
-    k_hash_fill<<<grid_for(32ull * N, 256, E.sm_count * 16), 256, 0, s>>>(J.off, row0, N, hash_min, d_hub_slot,
-                                                                            hpool);
-    J.launches += 1;
+    const size_t pool_b = peel_hash ? align_up(32ull * Ws) : 0, qh_b = peel_hash ? align_up(8ull * Mx) : 0;
+    const size_t spool_b = sup_hash ? align_up(32ull * m) : 0;
+    if (peel_hash || sup_hash) {
+      int rc = ensure_ws3(E, pool_b + 2 * qh_b + spool_b);
+      if (rc) return rc;
+    }
+    if (peel_hash) {
+      hpool = (unsigned long long*)E.ws3;
+      qh0 = (uint2*)(E.ws3 + pool_b);
+      qh1 = (uint2*)(E.ws3 + pool_b + qh_b);
+      hash_min = T.hash_min_degree;
+      CU(cudaMemsetAsync(hpool, 0xFF, 32ull * Ws, s));
+      k_hash_fill<<<grid_for(32ull * N, 256, E.sm_count * 16), 256, 0, s>>>(J.off, row0, N, hash_min, d_hub_slot,
+                                                                              hpool);
+      J.launches += 1;
+    }
+    if (sup_hash) {
+      spool = (unsigned long long*)(E.ws3 + pool_b + 2 * qh_b);
+      sup_hash_min = T.sup_hash_min;
+      CU(cudaMemsetAsync(spool, 0xFF, 32ull * m, s));
+      k_sup_hash_fill<<<grid_for(32ull * N, 256, E.sm_count * 16), 256, 0, s>>>(opos, ocol, N, sup_hash_min, spool);
+      J.launches += 1;
+    }
   }
   CU(cudaEventRecord(E.tev[2], s));
 
@@ -889,7 +920,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     int rc = launch_support(E.sm_count, O.support_kernel ? O.support_kernel : T.support_kernel, N, m,
                             hc.max_dplus, opos, ocol, osrc, es, at<unsigned long long>(E, L.q0),
                             at<unsigned long long>(E, L.tiles), cnt, at<uint32_t>(E, L.act0), s, &J.launches,
-                            &J.support_elements, mu, T.sample_min);
+                            &J.support_elements, mu, T.sample_min, spool, sup_hash_min);
     if (rc) return rc;
   }
   CU(cudaEventRecord(E.tev[3], s));
@@ -2645,6 +2676,7 @@ int sparx_tuning_default(sparx_tuning* t) {
   t->support_kernel = d.support_kernel;
   t->compact_pct = d.compact_pct;
   t->hash_min_degree = d.hash_min_degree;
+  t->sup_hash_min = d.sup_hash_min;
   return SPARX_OK;
 }
 
@@ -2669,7 +2701,7 @@ int sparx_tuning_signature(const uint64_t* offsets, uint64_t n_plus_1, uint32_t 
 namespace {
 Tuning from_c(const sparx_tuning* t) {
   return Tuning{t->merge_ratio, t->hub_min_degree, t->sample_min, t->support_kernel, t->compact_pct,
-                t->hash_min_degree};
+                t->hash_min_degree, t->sup_hash_min};
 }
 void to_c(const Tuning& t, sparx_tuning* o) {
   o->struct_size = sizeof(sparx_tuning);
@@ -2679,6 +2711,7 @@ void to_c(const Tuning& t, sparx_tuning* o) {
   o->support_kernel = t.support_kernel;
   o->compact_pct = t.compact_pct;
   o->hash_min_degree = t.hash_min_degree;
+  o->sup_hash_min = t.sup_hash_min;
 }
 }  // namespace
 
@@ -2788,6 +2821,7 @@ int autotune_core(RunF run, uint32_t repeats, Tuning* best_out, TuneKey* key_out
   std::vector<Tuning> c1;
   for (uint32_t smp : {32u, 128u, 256u}) { Tuning t = cur; t.sample_min = smp; c1.push_back(t); }
   { Tuning t = cur; t.support_kernel = 2; c1.push_back(t); }
+  for (uint32_t sh : {16u, 64u}) { Tuning t = cur; t.sup_hash_min = sh; c1.push_back(t); }
   if ((rc = try_group(c1, true))) return rc;
   std::vector<Tuning> c2;
   for (uint32_t h : {0u, 512u, 4096u}) { Tuning t = cur; t.hub_min_degree = h; c2.push_back(t); }

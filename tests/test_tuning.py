@@ -37,7 +37,8 @@ def test_store_lookup_save_load(tmp_path):
     key = (20, 12, 3)
     t, found = P.tuning_lookup(key)
     assert not found and t == P.PktTuning()
-    mine = P.PktTuning(merge_ratio=4, hub_min_degree=512, sample_min=128, support_kernel=2, compact_pct=75)
+    mine = P.PktTuning(merge_ratio=4, hub_min_degree=512, sample_min=128, support_kernel=2, compact_pct=75,
+                       hash_min_degree=32, sup_hash_min=16)
     P.tuning_store(key, mine)
     assert P.tuning_lookup(key) == (mine, True)
     path = str(tmp_path / "tune.txt")
@@ -50,4 +51,6 @@ def test_store_lookup_save_load(tmp_path):
         P.tuning_store(key, P.PktTuning(compact_pct=5))   # out of range
     with pytest.raises(P.PktError):
         P.tuning_store(key, P.PktTuning(hub_min_degree=100))
+    with pytest.raises(P.PktError):
+        P.tuning_store(key, P.PktTuning(sup_hash_min=2))
     P.tuning_clear()

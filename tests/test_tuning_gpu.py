@@ -15,9 +15,9 @@ pytestmark = pytest.mark.gpu
 O32 = P.PktOptions(out_bits=32, timeout_ms=120_000)
 
 CANDIDATES = [P.PktTuning(merge_ratio=mr, hub_min_degree=h, sample_min=smp, support_kernel=sk, compact_pct=cp,
-                          hash_min_degree=hm)
-              for mr, h, smp, sk, cp, hm in itertools.product((4, 16), (0, 256, 4096), (32, 256), (1, 2), (75, 95),
-                                                              (0, 8, 64))]
+                          hash_min_degree=hm, sup_hash_min=sh)
+              for mr, h, smp, sk, cp, hm, sh in itertools.product((4, 16), (0, 256, 4096), (32, 256), (1, 2),
+                                                                  (75, 95), (0, 8, 64), (0, 4, 64))]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -49,7 +49,7 @@ def test_every_candidate_gives_the_same_truss():
     # R-MAT-16 has rows past 1024 and 4096 entries (hub maps) and is big enough to compact
     g = gen.rmat(16, 16, seed=2)
     want = O.fast_truss(g.offsets, g.neighbours)[0]
-    for t in CANDIDATES[::5]:
+    for t in CANDIDATES[::13]:
         got, st = _with_tuning(t, lambda: P.run_pkt(g.offsets, g.neighbours, O32))
         assert np.array_equal(got, want), t
         assert (st.hub_maps > 0) == (t.hub_min_degree in (256, 4096)), (t, st.hub_maps)
@@ -61,10 +61,26 @@ def test_batched_unions_get_member_hub_maps():
     want = [O.fast_truss(m.offsets, m.neighbours)[0] for m in members]
     pairs = [(m.offsets, m.neighbours) for m in members]
     for t in (P.PktTuning(hub_min_degree=256), P.PktTuning(hub_min_degree=256, merge_ratio=4, compact_pct=95),
-              P.PktTuning(hub_min_degree=0), P.PktTuning(hub_min_degree=1024, hash_min_degree=16)):
+              P.PktTuning(hub_min_degree=0), P.PktTuning(hub_min_degree=1024, hash_min_degree=16),
+              P.PktTuning(sup_hash_min=4), P.PktTuning(sup_hash_min=32, support_kernel=2)):
         res = _with_tuning(t, lambda: P.run_batch(pairs, O32))
         for w, (truss, st, status) in zip(want, res):
             assert status == 0 and np.array_equal(truss, w), t
+
+
+def test_support_hash_on_multigraphs_and_support_only():
+    """The hashed out-list probe finds every copy's run the same way the
+    search does: weighted supports and the peel over them are unchanged."""
+    g = gen.with_parallel_edges(gen.rmat(12, 16, seed=6), 0.25, seed=6)
+    want = O.pkt(g.offsets, g.neighbours, threads=4)
+    for t in (P.PktTuning(sup_hash_min=4), P.PktTuning(sup_hash_min=16, support_kernel=2)):
+        got, _ = _with_tuning(t, lambda: P.run_pkt(g.offsets, g.neighbours, O32))
+        assert np.array_equal(got, want), t
+    h = gen.rmat(15, 16, seed=8)
+    tri = O.triangles(h.offsets, h.neighbours, threads=4)
+    for t in (P.PktTuning(sup_hash_min=4), P.PktTuning(sup_hash_min=64)):
+        got, _ = _with_tuning(t, lambda: P.run_triangles(h.offsets, h.neighbours))
+        assert np.array_equal(got, tri), t
 
 
 def test_autotune_stores_a_choice_the_next_launch_uses(tmp_path, monkeypatch):
