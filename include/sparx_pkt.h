@@ -246,7 +246,9 @@ typedef struct sparx_tuning {
   uint32_t compact_pct;     /* peel: rebuild the working rows once live entries fill at most
                                this percentage of them (85) */
   uint32_t hash_min_degree; /* peel: rows of at least this degree (>= 8) get a hash table that the
-                               per-lane search probes instead of a binary search; 0 = none (0) */
+                               per-lane search probes instead of a binary search; 0 = none (128).
+                               Skipped, with the same results, when its workspace (32 B per slot
+                               plus 16 B per edge) is over a batch's budget or cannot be allocated */
   uint32_t sup_hash_min;    /* support: oriented out-lists of at least this length (>= 4) get a hash
                                table probed instead of the sampled search; 0 = none (0) */
 } sparx_tuning;

@@ -71,7 +71,7 @@ struct Tuning {
   uint32_t sample_min = 64;        // support: longer out-lists from this length go through 64 samples
   uint32_t support_kernel = 1;     // 1 balanced edge form, 2 vertex form
   uint32_t compact_pct = 85;       // rebuild the peel's rows when live entries fill <= this % of them
-  uint32_t hash_min_degree = 0;    // rows of at least this degree get a hash table for the per-lane search (0: none)
+  uint32_t hash_min_degree = 128;  // rows of at least this degree get a hash table for the per-lane search (0: none)
   uint32_t sup_hash_min = 0;       // support: out-lists of at least this length are probed in a hash table (0: none)
 };
 
@@ -603,6 +603,7 @@ struct UnionJob {
   ServeHook* hook = nullptr;     // served union (members join and leave between graph launches)
   bool prep_only = false;        // stop after the support pass (members about to join a served union)
   const uint32_t* smap = nullptr;  // multigraphs: caller slot -> deduplicated slot (device)
+  uint64_t budget = 0;             // device bytes the launch may hold (batched unions); 0: no bound
   uint64_t prep_m = 0, prep_Ws = 0;  // prep_only: edges and slots prepared
   std::vector<Member> members;  // vb, n, sb, w set; eb, m filled by the pipeline
   Layout L{};
@@ -883,16 +884,19 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   uint2* qh0 = nullptr;
   uint2* qh1 = nullptr;
   uint32_t hash_min = 0, sup_hash_min = 0;
+  // Both are optional: when their workspace does not fit the launch's budget
+  // or cannot be allocated, the launch runs without them (same results).
   {
-    const bool peel_hash = T.hash_min_degree && !J.support_only && !J.prep_only && !J.hook &&
-                           Ws < (1ull << 30) && Ws;
-    const bool sup_hash = T.sup_hash_min && m > 0 && m < (1ull << 28);
+    bool peel_hash = T.hash_min_degree && !J.support_only && !J.prep_only && !J.hook && Ws < (1ull << 30) && Ws;
+    bool sup_hash = T.sup_hash_min && m > 0 && m < (1ull << 28);
     const uint64_t Mx = std::max<uint64_t>(W / 2, 1);
-    const size_t pool_b = peel_hash ? align_up(32ull * Ws) : 0, qh_b = peel_hash ? align_up(8ull * Mx) : 0;
-    const size_t spool_b = sup_hash ? align_up(32ull * m) : 0;
-    if (peel_hash || sup_hash) {
-      int rc = ensure_ws3(E, pool_b + 2 * qh_b + spool_b);
-      if (rc) return rc;
+    size_t pool_b = peel_hash ? align_up(32ull * Ws) : 0, qh_b = peel_hash ? align_up(8ull * Mx) : 0;
+    size_t spool_b = sup_hash ? align_up(32ull * m) : 0;
+    if ((peel_hash || sup_hash) &&
+        ((J.budget && L.total + pool_b + 2 * qh_b + spool_b > J.budget) ||
+         ensure_ws3(E, pool_b + 2 * qh_b + spool_b) != SPARX_OK)) {
+      peel_hash = sup_hash = false;
+      pool_b = qh_b = spool_b = 0;
     }
     if (peel_hash) {
       hpool = (unsigned long long*)E.ws3;
@@ -1589,9 +1593,10 @@ int download_union(Engine& E, const std::vector<HostMember>& hm, const std::vect
 // Decompose one union of validated members; on a device-detected input error
 // the members are re-run one by one to attribute the status.
 int run_batch_union(Engine& E, std::vector<HostMember>& hm, const Opts& O, int* status_out,
-                    sparx_pkt_stats* stats_out, int* first_fail) {
+                    sparx_pkt_stats* stats_out, int* first_fail, uint64_t budget = 0) {
   const size_t G = hm.size();
   UnionJob J;
+  J.budget = budget;
   uint64_t N = 0, Wt = 0, max_n = 0;
   for (const HostMember& h : hm) {
     J.members.push_back(Member{(uint32_t)N, (uint32_t)h.n, (uint32_t)Wt, (uint32_t)h.w, 0, 0});
@@ -1634,7 +1639,7 @@ int run_batch_union(Engine& E, std::vector<HostMember>& hm, const Opts& O, int* 
     // attribute: one member at a time
     for (size_t g = 0; g < G; ++g) {
       std::vector<HostMember> one{hm[g]};
-      run_batch_union(E, one, O, status_out, stats_out, first_fail);
+      run_batch_union(E, one, O, status_out, stats_out, first_fail, budget);
     }
     return SPARX_OK;
   }
@@ -1722,7 +1727,7 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
       max_n = mx2;
       ++at_i;
     }
-    if (!wave.empty()) run_batch_union(E, wave, O, status_out, stats_out, &first_fail);
+    if (!wave.empty()) run_batch_union(E, wave, O, status_out, stats_out, &first_fail, budget);
   }
   return first_fail;
 }
@@ -2833,7 +2838,7 @@ int autotune_core(RunF run, uint32_t repeats, Tuning* best_out, TuneKey* key_out
   for (uint32_t cp : {75u, 95u}) { Tuning t = cur; t.compact_pct = cp; c4.push_back(t); }
   if ((rc = try_group(c4, false))) return rc;
   std::vector<Tuning> c5;
-  for (uint32_t hm : {32u, 128u, 512u}) { Tuning t = cur; t.hash_min_degree = hm; c5.push_back(t); }
+  for (uint32_t hm : {0u, 32u, 512u}) { Tuning t = cur; t.hash_min_degree = hm; c5.push_back(t); }
   if ((rc = try_group(c5, false))) return rc;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -547,7 +547,7 @@ class PktTuning:
     sample_min: int = 64
     support_kernel: int = 1
     compact_pct: int = 85
-    hash_min_degree: int = 0
+    hash_min_degree: int = 128
     sup_hash_min: int = 0
 
     def c(self) -> _Tuning:

@@ -68,6 +68,18 @@ def test_batched_unions_get_member_hub_maps():
             assert status == 0 and np.array_equal(truss, w), t
 
 
+def test_tight_batch_budget_runs_without_the_hash_tables():
+    """Unions packed up to a small budget leave no room for the row hash tables
+    (32 B per slot): they run without them and give the same truss numbers."""
+    members = [gen.rmat(13, 16, seed=s) for s in range(8)]
+    want = [O.fast_truss(m.offsets, m.neighbours)[0] for m in members]
+    pairs = [(m.offsets, m.neighbours) for m in members]
+    for budget in (150 << 20, 200 << 20, 0):  # a union holds 128 MB of staging buffers
+        res = P.run_batch(pairs, O32, hbm_budget_bytes=budget)
+        for w, (truss, st, status) in zip(want, res):
+            assert status == 0 and np.array_equal(truss, w), budget
+
+
 def test_support_hash_on_multigraphs_and_support_only():
     """The hashed out-list probe finds every copy's run the same way the
     search does: weighted supports and the peel over them are unchanged."""
