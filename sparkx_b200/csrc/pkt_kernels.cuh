@@ -790,8 +790,9 @@ __device__ __forceinline__ uint32_t window_find(const StartF& start, uint32_t i,
 // run credit of the simple form is for unit weights only).
 //
 // kHash: out-lists of at least hash_min entries have an open-addressed table
-// of (id | position << 32) at 4 * their start in `hpool` (k_sup_hash_fill,
-// same layout rule as the row tables), probed instead of searched.
+// of (id | position << 32) at 4 * their start in `hpool` (k_table_fill with
+// OutListSource, the same layout as the peel's row tables), probed instead of
+// searched.
 __device__ __forceinline__ uint32_t probe_list(const unsigned long long* __restrict__ hpool, uint32_t lb,
                                                uint32_t len, uint32_t c) {
   const uint32_t lg = hash_log2cap(len), mask = (1u << lg) - 1;
@@ -1437,17 +1438,20 @@ struct PushStage {
   uint32_t n;     // warp-uniform fill
 };
 
-__device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, const Member& M,
-                                           MemberState* st, uint32_t* err, uint32_t q_sel) {
+// Publication of a warp's staged pushes.  Not inlined: it runs once per
+// kPushBuf pushes, and as a call its temporaries (two row descriptors, hash
+// descriptors, scans) stay out of the element loop's register budget.  It
+// reads the union's arrays from the device-resident Union.
+__device__ __noinline__ void push_flush_cold(const uint32_t* eid, uint32_t n, const Union* Up, uint32_t eb,
+                                             uint32_t m, MemberState* st, uint32_t* err, uint32_t q_sel) {
+  const UnionRegs U(Up);
   // the queue being built (q_sel names the one being processed)
   unsigned long long* qnext = q_sel ? U.q0 : U.q1;
   uint4* qdnext = q_sel ? U.qd0 : U.qd1;
   uint2* qhnext = q_sel ? U.qh0 : U.qh1;
-  __syncwarp();
-  const uint32_t n = ps.n;
-  if (n == 0) return;
+  const Member M{0, 0, 0, 0, eb, m};
   const uint32_t lane = lane_id();
-  const uint32_t x0 = lane < n ? ps.eid[lane] : 0u, x1 = lane + 32 < n ? ps.eid[lane + 32] : 0u;
+  const uint32_t x0 = lane < n ? eid[lane] : 0u, x1 = lane + 32 < n ? eid[lane + 32] : 0u;
   uint2 h0 = make_uint2(0, 0), h1 = make_uint2(0, 0);
   const uint4 d0 = lane < n ? edge_desc(U, x0, &h0) : make_uint4(0, 0, 0, 0);
   const uint4 d1 = lane + 32 < n ? edge_desc(U, x1, &h1) : make_uint4(0, 0, 0, 0);
@@ -1478,18 +1482,25 @@ __device__ __forceinline__ void push_flush(PushStage& ps, const UnionRegs& U, co
       atomicOr(err, kErrCapacity);
     }
   }
+}
+
+__device__ __forceinline__ void push_flush(PushStage& ps, const Union* Up, const Member& M, MemberState* st,
+                                           uint32_t* err, uint32_t q_sel) {
+  __syncwarp();
+  if (ps.n == 0) return;
+  push_flush_cold(ps.eid, ps.n, Up, M.eb, M.m, st, err, q_sel);
   ps.n = 0;
   __syncwarp();
 }
 
 // Queue edge x (union eid) for wave W + 1.  All lanes call it.
-__device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, const Member& M, MemberState* st,
-                                          uint32_t* err, uint32_t q_sel, bool want,
+__device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, const Union* Up, const Member& M,
+                                          MemberState* st, uint32_t* err, uint32_t q_sel, bool want,
                                           uint32_t x, uint32_t W) {
   const unsigned bal = __ballot_sync(kFull, want);
   if (!bal) return;
   const uint32_t k = __popc(bal);
-  if (ps.n + k > kPushBuf) push_flush(ps, U, M, st, err, q_sel);
+  if (ps.n + k > kPushBuf) push_flush(ps, Up, M, st, err, q_sel);
   if (want) {
     U.es[x].y = (int)(W + 1);
     ps.eid[ps.n + __popc(bal & ((1u << lane_id()) - 1))] = x;
@@ -1860,8 +1871,8 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           if (hit) es_f = U.es[f];
 #endif
           if (hit) pkt_rule<kMulti>(U, e, f, es_f, h, level, W, pf, ph);
-          push_edge(ps, U, M, st, a.err, q_sel, pf, f, W);
-          push_edge(ps, U, M, st, a.err, q_sel, ph, h, W);
+          push_edge(ps, U, a.Up, M, st, a.err, q_sel, pf, f, W);
+          push_edge(ps, U, a.Up, M, st, a.err, q_sel, ph, h, W);
           i = x_last;
         }
       } else if (phase == kPhaseScan0 || phase == kPhaseScan) {
@@ -1888,7 +1899,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
               else { keep = true; mn = min(mn, (uint32_t)s); }
             }
           }
-          push_edge(ps, U, M, st, a.err, q_sel, queue, e, W);
+          push_edge(ps, U, a.Up, M, st, a.err, q_sel, queue, e, W);
           const unsigned kb_bal = __ballot_sync(kFull, keep);
           if (kb_bal) {
             const uint32_t kc = __popc(kb_bal);
@@ -1921,7 +1932,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
         }
         __syncwarp();
       }
-      push_flush(ps, U, M, st, a.err, q_sel);  // entries belong to this member: publish before moving on
+      push_flush(ps, a.Up, M, st, a.err, q_sel);  // entries belong to this member: publish before moving on
       k = seg_end;
     }
   }
@@ -2777,52 +2788,78 @@ __global__ void k_replan(const Member* __restrict__ mem, const MemberState* __re
   }
 }
 
-// Out-list hash tables for the support pass: a warp per vertex whose oriented
-// out-list has at least hash_min entries; entry = (id | position << 32).
-__global__ void __launch_bounds__(256) k_sup_hash_fill(const uint32_t* __restrict__ opos,
-                                                       const uint32_t* __restrict__ ocol, uint32_t n,
-                                                       uint32_t hash_min, unsigned long long* __restrict__ pool) {
-  const uint32_t lane = lane_id();
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t b = __ldg(opos + u), d = __ldg(opos + u + 1) - b;
-    if (d < hash_min) continue;
-    const uint32_t lg = hash_log2cap(d), mask = (1u << lg) - 1;
-    unsigned long long* tb = pool + 4ull * b;
-    for (uint32_t j = b + lane; j < b + d; j += 32) {
-      const uint32_t c = __ldg(ocol + j);
-      const unsigned long long en = (unsigned long long)c | ((unsigned long long)j << 32);
-      uint32_t at = hash_first(c, lg);
-      for (uint32_t it = 0; it <= mask; ++it) {
-        if (atomicCAS(tb + at, ~0ull, en) == ~0ull) break;
-        at = (at + 1) & mask;
-      }
-    }
-  }
-}
+// Hash tables per row (see hash_log2cap): the rows of at least `min_len`
+// entries (the peel: original rows without a hub map; the support pass:
+// oriented out-lists) get an open-addressed table of 2^(1+ceil(log2 d)) 8-byte
+// entries at 4 * the row's start in `pool`.  A warp reads the lengths of 32
+// consecutive rows at once and builds each qualifying row's table in turn:
+// tables of up to kTableSmem entries in its own slice of shared memory (cleared,
+// filled by compare-and-swap, then stored coalesced), longer ones in place
+// (cleared, then filled).  Every table is written whole, so the pool needs no
+// clearing beforehand; entries outside the tables are never read.
+constexpr uint32_t kTableSmem = 1024;  // entries per warp (8 KB)
+constexpr int kTableWarps = 4;
 
-// Row hash tables (see hash_log2cap): a warp per row of degree >= hash_min
-// without a hub map; pairs go in by 64-bit compare-and-swap on empty entries.
-__global__ void __launch_bounds__(256) k_hash_fill(const uint32_t* __restrict__ off0,
-                                                   const unsigned long long* __restrict__ row0, uint32_t n,
-                                                   uint32_t hash_min, const uint32_t* __restrict__ hub_slot,
-                                                   unsigned long long* __restrict__ pool) {
+// peel: (column id | edge id << 32) from the original rows; self-loop slots
+// (edge id kInvalid) stay out
+struct RowPairSource {
+  const unsigned long long* row0;
+  __device__ __forceinline__ unsigned long long operator()(uint32_t s) const {
+    const unsigned long long pr = __ldg(row0 + s);
+    return (uint32_t)(pr >> 32) == kInvalid ? ~0ull : pr;
+  }
+};
+// support: (column id | position << 32) from the oriented out-lists
+struct OutListSource {
+  const uint32_t* ocol;
+  __device__ __forceinline__ unsigned long long operator()(uint32_t j) const {
+    return (unsigned long long)__ldg(ocol + j) | ((unsigned long long)j << 32);
+  }
+};
+
+template <class Source>
+__global__ void __launch_bounds__(kTableWarps * 32) k_table_fill(const uint32_t* __restrict__ off, uint32_t n,
+                                                                  uint32_t min_len,
+                                                                  const uint32_t* __restrict__ hub_slot,
+                                                                  Source src, unsigned long long* __restrict__ pool) {
+  __shared__ unsigned long long s_tab[kTableWarps][kTableSmem];
   const uint32_t lane = lane_id();
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t b = __ldg(off0 + u), d = __ldg(off0 + u + 1) - b;
-    if (d < hash_min || (hub_slot && __ldg(hub_slot + u) != kInvalid)) continue;
-    const uint32_t lg = hash_log2cap(d), mask = (1u << lg) - 1;
-    unsigned long long* tb = pool + 4ull * b;
-    for (uint32_t s = b + lane; s < b + d; s += 32) {
-      const unsigned long long pr = __ldg(row0 + s);
-      if ((uint32_t)(pr >> 32) == kInvalid) continue;  // a self-loop: no edge
-      uint32_t at = hash_first((uint32_t)pr, lg);
-      for (uint32_t it = 0; it <= mask; ++it) {
-        if (atomicCAS(tb + at, ~0ull, pr) == ~0ull) break;
-        at = (at + 1) & mask;
+  unsigned long long* st = s_tab[threadIdx.x >> 5];
+  const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long u0 = warp * 32; u0 < n; u0 += nwarps * 32) {
+    const unsigned long long u = u0 + lane;
+    uint32_t b = 0, d = 0;
+    bool want = false;
+    if (u < n) {
+      b = __ldg(off + u);
+      d = __ldg(off + u + 1) - b;
+      want = d >= min_len && !(hub_slot && __ldg(hub_slot + u) != kInvalid);
+    }
+    unsigned todo = __ballot_sync(kFull, want);
+    while (todo) {
+      const int r = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t rb = __shfl_sync(kFull, b, r), rd = __shfl_sync(kFull, d, r);
+      const uint32_t lg = hash_log2cap(rd), cap = 1u << lg, mask = cap - 1;
+      unsigned long long* tb = pool + 4ull * rb;
+      const bool local = cap <= kTableSmem;
+      unsigned long long* t = local ? st : tb;
+      for (uint32_t i = lane; i < cap; i += 32) t[i] = ~0ull;
+      __syncwarp();
+      for (uint32_t x = rb + lane; x < rb + rd; x += 32) {
+        const unsigned long long en = src(x);
+        if (en == ~0ull) continue;
+        uint32_t at = hash_first((uint32_t)en, lg);
+        for (uint32_t it = 0; it <= mask; ++it) {
+          if (atomicCAS(t + at, ~0ull, en) == ~0ull) break;
+          at = (at + 1) & mask;
+        }
+      }
+      __syncwarp();
+      if (local) {
+        for (uint32_t i = lane; i < cap; i += 32) tb[i] = st[i];
+        __syncwarp();
       }
     }
   }

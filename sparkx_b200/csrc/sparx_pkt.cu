@@ -903,16 +903,15 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       qh0 = (uint2*)(E.ws3 + pool_b);
       qh1 = (uint2*)(E.ws3 + pool_b + qh_b);
       hash_min = T.hash_min_degree;
-      CU(cudaMemsetAsync(hpool, 0xFF, 32ull * Ws, s));
-      k_hash_fill<<<grid_for(32ull * N, 256, E.sm_count * 16), 256, 0, s>>>(J.off, row0, N, hash_min, d_hub_slot,
-                                                                              hpool);
+      k_table_fill<<<grid_for(N, kTableWarps * 32, E.sm_count * 16), kTableWarps * 32, 0, s>>>(
+          J.off, N, hash_min, d_hub_slot, RowPairSource{row0}, hpool);
       J.launches += 1;
     }
     if (sup_hash) {
       spool = (unsigned long long*)(E.ws3 + pool_b + 2 * qh_b);
       sup_hash_min = T.sup_hash_min;
-      CU(cudaMemsetAsync(spool, 0xFF, 32ull * m, s));
-      k_sup_hash_fill<<<grid_for(32ull * N, 256, E.sm_count * 16), 256, 0, s>>>(opos, ocol, N, sup_hash_min, spool);
+      k_table_fill<<<grid_for(N, kTableWarps * 32, E.sm_count * 16), kTableWarps * 32, 0, s>>>(
+          opos, N, sup_hash_min, nullptr, OutListSource{ocol}, spool);
       J.launches += 1;
     }
   }

@@ -74,7 +74,7 @@ def test_tight_batch_budget_runs_without_the_hash_tables():
     members = [gen.rmat(13, 16, seed=s) for s in range(8)]
     want = [O.fast_truss(m.offsets, m.neighbours)[0] for m in members]
     pairs = [(m.offsets, m.neighbours) for m in members]
-    for budget in (150 << 20, 200 << 20, 0):  # a union holds 128 MB of staging buffers
+    for budget in (200 << 20, 260 << 20, 0):  # a union holds 128 MB of staging buffers and hub maps
         res = P.run_batch(pairs, O32, hbm_budget_bytes=budget)
         for w, (truss, st, status) in zip(want, res):
             assert status == 0 and np.array_equal(truss, w), budget
@@ -108,3 +108,25 @@ def test_autotune_stores_a_choice_the_next_launch_uses(tmp_path, monkeypatch):
     best_b, key_b = P.autotune_batch([(m.offsets, m.neighbours) for m in members], repeats=1)
     assert P.tuning_lookup(key_b) == (best_b, True)
     P.tuning_clear()
+
+
+def test_hash_tables_with_self_loops_and_compaction():
+    """Rows that carry self-loop slots (no edge id: kept out of the tables) and
+    a peel that compacts its rows many times: the row and out-list tables give
+    the oracle's truss numbers at floors from 8 (most rows hashed) upwards."""
+    rng = np.random.default_rng(41)
+    base = gen.rmat(14, 16, seed=11)
+    n = base.n
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(base.offsets.astype(np.int64)))
+    dst = base.neighbours.astype(np.int64)
+    keep = src < dst
+    edges = list(zip(src[keep].tolist(), dst[keep].tolist()))
+    loops = rng.choice(n, size=n // 8, replace=False)
+    edges += [(int(v), int(v)) for v in loops]
+    g = gen.from_edges(n, edges)
+    assert g.self_loops() > 0
+    want = O.pkt(g.offsets, g.neighbours, threads=4)
+    for t in (P.PktTuning(hash_min_degree=8, compact_pct=95), P.PktTuning(hash_min_degree=8, sup_hash_min=4),
+              P.PktTuning(hash_min_degree=64, hub_min_degree=0, sup_hash_min=16)):
+        got, _ = _with_tuning(t, lambda: P.run_pkt(g.offsets, g.neighbours, O32))
+        assert np.array_equal(got, want), t
