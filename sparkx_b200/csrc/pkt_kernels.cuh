@@ -1422,6 +1422,9 @@ constexpr int kWaveThreads = 256;
 #define SPARX_WAVE_MINB 7  // resident 256-thread blocks per SM the register budget targets
 #endif
 constexpr int kWaveWarps = kWaveThreads / 32;
+// slots of the per-warp loop state in shared memory (k_wave)
+enum : int { kCtxJb = 0, kCtxSegEnd = 1, kCtxKend = 2 };
+enum : int { kCtxEb = 0, kCtxM, kCtxLevel, kCtxQsel, kCtxQcount, kCtxSegLen, kCtxG, kCtxW };
 // kept active-list entries staged per warp before one atomic reserves their
 // place: every kept entry of a large scan goes through one counter per member
 constexpr int kKeepBuf = 256;
@@ -1484,23 +1487,23 @@ __device__ __noinline__ void push_flush_cold(const uint32_t* eid, uint32_t n, co
   }
 }
 
-__device__ __forceinline__ void push_flush(PushStage& ps, const Union* Up, const Member& M, MemberState* st,
+__device__ __forceinline__ void push_flush(PushStage& ps, const Union* Up, uint32_t eb, uint32_t m, MemberState* st,
                                            uint32_t* err, uint32_t q_sel) {
   __syncwarp();
   if (ps.n == 0) return;
-  push_flush_cold(ps.eid, ps.n, Up, M.eb, M.m, st, err, q_sel);
+  push_flush_cold(ps.eid, ps.n, Up, eb, m, st, err, q_sel);
   ps.n = 0;
   __syncwarp();
 }
 
 // Queue edge x (union eid) for wave W + 1.  All lanes call it.
-__device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, const Union* Up, const Member& M,
-                                          MemberState* st, uint32_t* err, uint32_t q_sel, bool want,
+__device__ __forceinline__ void push_edge(PushStage& ps, const UnionRegs& U, const Union* Up, uint32_t eb,
+                                          uint32_t m, MemberState* st, uint32_t* err, uint32_t q_sel, bool want,
                                           uint32_t x, uint32_t W) {
   const unsigned bal = __ballot_sync(kFull, want);
   if (!bal) return;
   const uint32_t k = __popc(bal);
-  if (ps.n + k > kPushBuf) push_flush(ps, Up, M, st, err, q_sel);
+  if (ps.n + k > kPushBuf) push_flush(ps, Up, eb, m, st, err, q_sel);
   if (want) {
     U.es[x].y = (int)(W + 1);
     ps.eid[ps.n + __popc(bal & ((1u << lane_id()) - 1))] = x;
@@ -1658,6 +1661,72 @@ __device__ __forceinline__ void plan_wave(const Member* __restrict__ mem, Member
   }
 }
 
+// One member's segment of a level scan (kPhaseScan0 / kPhaseScan): active
+// entry j of the segment is kept (support above the level), queued for this
+// level, or dropped (processed).  Not inlined: its staging state stays out of
+// the frontier loop's register budget.  Publishes its pushes before returning.
+__device__ __noinline__ void wave_scan_segment(const Union* Up, MemberState* st, uint32_t eb, uint32_t m,
+                                               uint32_t phase, uint32_t level, uint32_t act_sel, uint32_t q_sel,
+                                               uint32_t W, uint32_t a0, uint32_t seg_len, uint32_t* keepbuf,
+                                               uint32_t* push_eid, uint32_t* err) {
+  const UnionRegs U(Up);
+  const uint32_t lane = lane_id();
+  PushStage ps{push_eid, 0};
+  const uint32_t* act = act_sel ? U.act1 : U.act0;
+  uint32_t* act_out = act_sel ? U.act0 : U.act1;
+  uint32_t nkeep = 0, nzero = 0, mn = 0xFFFFFFFFu;
+  for (uint32_t r = 0; r < seg_len; r += 32) {
+    const bool valid = r + lane < seg_len;
+    bool keep = false, zero = false, queue = false;
+    uint32_t le = 0, e = 0;
+    if (valid) {
+      le = act[eb + a0 + r + lane];
+      e = eb + le;
+      const int2 st_e = U.es[e];
+      const int32_t s = st_e.x;
+      if (phase == kPhaseScan0) {
+        if (s == 0) { U.es[e].y = 0; zero = true; }
+        else { keep = true; mn = min(mn, (uint32_t)s); }
+      } else if ((uint32_t)st_e.y == kTagActive) {  // processed edges leave the active list
+        if (s <= (int32_t)level) queue = true;
+        else { keep = true; mn = min(mn, (uint32_t)s); }
+      }
+    }
+    push_edge(ps, U, Up, eb, m, st, err, q_sel, queue, e, W);
+    const unsigned kb_bal = __ballot_sync(kFull, keep);
+    if (kb_bal) {
+      const uint32_t kc = __popc(kb_bal);
+      if (nkeep + kc > kKeepBuf) {
+        __syncwarp();
+        uint32_t old = 0;
+        if (lane == 0) old = atomicAdd(&st->kept, nkeep);
+        old = __shfl_sync(kFull, old, 0);
+        for (uint32_t t = lane; t < nkeep; t += 32) act_out[eb + old + t] = keepbuf[t];
+        nkeep = 0;
+        __syncwarp();
+      }
+      if (keep) keepbuf[nkeep + __popc(kb_bal & ((1u << lane) - 1))] = le;
+      nkeep += kc;
+    }
+    nzero += __popc(__ballot_sync(kFull, zero));
+  }
+  __syncwarp();
+  if (nkeep) {
+    uint32_t old = 0;
+    if (lane == 0) old = atomicAdd(&st->kept, nkeep);
+    old = __shfl_sync(kFull, old, 0);
+    for (uint32_t t = lane; t < nkeep; t += 32) act_out[eb + old + t] = keepbuf[t];
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
+  if (lane == 0) {
+    if (mn != 0xFFFFFFFFu) atomicMin(&st->min_kept, mn);
+    if (nzero) atomicAdd(&st->processed, nzero);
+  }
+  __syncwarp();
+  push_flush(ps, Up, eb, m, st, err, q_sel);
+}
+
 // Kernel D: one peel wave.  The wave's work (all members' scan elements and
 // frontier elements, laid out by `wpref`) is cut into warp-sized chunks; a
 // warp walks its chunk member by member, 32 consecutive elements per
@@ -1693,13 +1762,22 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
   if (lane < 4) s_cnt[lane][wib] = 0;
   __syncwarp();
   PushStage ps{s_push_eid[wib], 0};
+  // Warp-uniform state of the frontier loop lives in shared memory and is read
+  // back where it is used: held in registers it was spilled to local memory,
+  // whose lines the loop's random row and state loads evict from L1.
+  __shared__ unsigned long long s_w64[kWaveWarps][3];  // kCtxJb, kCtxSegEnd, kCtxKend
+  __shared__ uint32_t s_w32[kWaveWarps][8];            // kCtxEb .. kCtxW
+  volatile unsigned long long* const w64 = s_w64[wib];
+  volatile uint32_t* const w32 = s_w32[wib];
 
   if (warp * ch < total) {
     const unsigned long long c0 = warp * ch;
-    const unsigned long long kend = min(c0 + ch, total);
+    if (lane == 0) w64[kCtxKend] = min(c0 + ch, total);
+    __syncwarp();
     unsigned long long k = c0;
     uint32_t g = G > 1 ? warp_last_le(PrefKey{a.wpref}, 0, G - 1, k) : 0;
-    while (k < kend) {
+    while (k < w64[kCtxKend]) {
+      const unsigned long long kend = w64[kCtxKend];
       while (g + 1 < G && a.wpref[g + 1] <= k) ++g;
       const unsigned long long mbeg = a.wpref[g];
       // a segment spans < 2^31 elements, so offsets inside it are 32-bit
@@ -1712,23 +1790,38 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
       MemberState* st = a.st + g;
       const uint32_t phase = st->phase, level = st->level, act_sel = st->act_sel, q_sel = st->q_sel;
       if (phase == kPhaseProc) {
-        const unsigned long long* q = (q_sel ? U.q1 : U.q0) + M.eb;
-        const uint4* qd = (q_sel ? U.qd1 : U.qd0) + M.eb;
-        const uint32_t qcount = (uint32_t)(st->curr >> kWorkBits);
-        if (qcount == 0) {
+        const uint32_t qcount0 = (uint32_t)(st->curr >> kWorkBits);
+        if (qcount0 == 0) {
           if (lane == 0) atomicOr(a.err, kErrInternal);
           k = seg_end;
           continue;
         }
-        uint32_t i = warp_last_le(QueueStart{q}, 0, qcount - 1, k - mbeg);
+        const uint32_t i0 =
+            warp_last_le(QueueStart{(q_sel ? U.q1 : U.q0) + M.eb}, 0, qcount0 - 1, k - mbeg);
+        __syncwarp();
+        if (lane == 0) {
+          // element j (member-relative) = jb + r + lane; r counts the segment
+          w64[kCtxJb] = k - mbeg;
+          w64[kCtxSegEnd] = seg_end;
+          w32[kCtxEb] = M.eb;
+          w32[kCtxM] = M.m;
+          w32[kCtxLevel] = level;
+          w32[kCtxQsel] = q_sel;
+          w32[kCtxQcount] = qcount0;
+          w32[kCtxSegLen] = (uint32_t)(seg_end - k);
+          w32[kCtxG] = g;
+          w32[kCtxW] = W;
+        }
+        __syncwarp();
+        uint32_t i = i0;
         // merge cursor carried across iterations that continue the same edge
         uint32_t m_e = kInvalid, m_next_o = 0, m_cur = 0;
-        // element j (member-relative) = jb + r + lane; r counts the segment
-        const unsigned long long jb = k - mbeg;
-        const uint32_t seg_len = (uint32_t)(seg_end - k);
-        for (uint32_t r = 0; r < seg_len; r += 32) {
+        for (uint32_t r = 0; r < w32[kCtxSegLen]; r += 32) {
+          const uint32_t seg_len = w32[kCtxSegLen];
+          const uint32_t qcount = w32[kCtxQcount];
+          const unsigned long long* q = (w32[kCtxQsel] ? U.q1 : U.q0) + w32[kCtxEb];
           const bool valid = r + lane < seg_len;
-          const unsigned long long j = jb + r + lane;
+          const unsigned long long j = w64[kCtxJb] + r + lane;
           // the window's entries, loaded once: each lane picks its own by a
           // shuffle search on the work starts (entries own >= 1 element, so
           // 32 consecutive elements span at most 32 entries)
@@ -1745,9 +1838,9 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           const uint32_t x_last = __shfl_sync(kFull, x, last);
           uint32_t e = 0, o = 0, sb = 0, slen = 0, lb = 0, le = 0;
           if (valid) {
-            e = M.eb + (uint32_t)(ent & kEidMask);
+            e = w32[kCtxEb] + (uint32_t)(ent & kEidMask);
             o = (uint32_t)(j - (ent >> kEidBits));
-            const uint4 dsc = qd[x];
+            const uint4 dsc = ((w32[kCtxQsel] ? U.qd1 : U.qd0) + w32[kCtxEb])[x];
             sb = dsc.x;
             slen = dsc.y;
             lb = dsc.z;
@@ -1765,7 +1858,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           // the other edge of the short row: already processed -> nothing to resolve
           if (look) {
             es_f = U.es[f];
-            look = (uint32_t)es_f.y >= W;
+            look = (uint32_t)es_f.y >= w32[kCtxW];
           }
 #endif
           // lane 0 is always valid: its rows decide, so the branch and the
@@ -1835,7 +1928,7 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
             if (lane == 0) s_cnt[2][wib]++;
             m_e = kInvalid;
             if (look) {
-              const uint2 hq = U.hash_min ? (q_sel ? U.qh1 : U.qh0)[M.eb + x] : make_uint2(0, 0);
+              const uint2 hq = U.hash_min ? (w32[kCtxQsel] ? U.qh1 : U.qh0)[w32[kCtxEb] + x] : make_uint2(0, 0);
               if (hubs && (lb & kHubDesc)) {
                 // the longer row's vertex has a hub map: one lookup
                 h = __ldg(U.hub_map + (uint32_t)(le + w));
@@ -1870,69 +1963,24 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           // that is already processed, which pkt_rule then skips
           if (hit) es_f = U.es[f];
 #endif
-          if (hit) pkt_rule<kMulti>(U, e, f, es_f, h, level, W, pf, ph);
-          push_edge(ps, U, a.Up, M, st, a.err, q_sel, pf, f, W);
-          push_edge(ps, U, a.Up, M, st, a.err, q_sel, ph, h, W);
+          if (hit) pkt_rule<kMulti>(U, e, f, es_f, h, w32[kCtxLevel], w32[kCtxW], pf, ph);
+          push_edge(ps, U, a.Up, w32[kCtxEb], w32[kCtxM], a.st + w32[kCtxG], a.err, w32[kCtxQsel], pf, f,
+                    w32[kCtxW]);
+          push_edge(ps, U, a.Up, w32[kCtxEb], w32[kCtxM], a.st + w32[kCtxG], a.err, w32[kCtxQsel], ph, h,
+                    w32[kCtxW]);
           i = x_last;
         }
+        // entries belong to this member: publish before moving on
+        push_flush(ps, a.Up, w32[kCtxEb], w32[kCtxM], a.st + w32[kCtxG], a.err, w32[kCtxQsel]);
+        k = w64[kCtxSegEnd];
+        g = w32[kCtxG];
+        continue;
       } else if (phase == kPhaseScan0 || phase == kPhaseScan) {
-        const uint32_t* act = act_sel ? U.act1 : U.act0;
-        uint32_t* act_out = act_sel ? U.act0 : U.act1;
-        uint32_t* keepbuf = s_keep[wib];
-        uint32_t nkeep = 0, nzero = 0, mn = 0xFFFFFFFFu;
         // active-list positions are below the member's edge count (< 2^28)
-        const uint32_t a0 = (uint32_t)(k - mbeg), seg_len = (uint32_t)(seg_end - k);
-        for (uint32_t r = 0; r < seg_len; r += 32) {
-          const bool valid = r + lane < seg_len;
-          bool keep = false, zero = false, queue = false;
-          uint32_t le = 0, e = 0;
-          if (valid) {
-            le = act[M.eb + a0 + r + lane];
-            e = M.eb + le;
-            const int2 st_e = U.es[e];
-            const int32_t s = st_e.x;
-            if (phase == kPhaseScan0) {
-              if (s == 0) { U.es[e].y = 0; zero = true; }
-              else { keep = true; mn = min(mn, (uint32_t)s); }
-            } else if ((uint32_t)st_e.y == kTagActive) {  // processed edges leave the active list
-              if (s <= (int32_t)level) queue = true;
-              else { keep = true; mn = min(mn, (uint32_t)s); }
-            }
-          }
-          push_edge(ps, U, a.Up, M, st, a.err, q_sel, queue, e, W);
-          const unsigned kb_bal = __ballot_sync(kFull, keep);
-          if (kb_bal) {
-            const uint32_t kc = __popc(kb_bal);
-            if (nkeep + kc > kKeepBuf) {
-              __syncwarp();
-              uint32_t old = 0;
-              if (lane == 0) old = atomicAdd(&st->kept, nkeep);
-              old = __shfl_sync(kFull, old, 0);
-              for (uint32_t t = lane; t < nkeep; t += 32) act_out[M.eb + old + t] = keepbuf[t];
-              nkeep = 0;
-              __syncwarp();
-            }
-            if (keep) keepbuf[nkeep + __popc(kb_bal & ((1u << lane) - 1))] = le;
-            nkeep += kc;
-          }
-          nzero += __popc(__ballot_sync(kFull, zero));
-        }
-        __syncwarp();
-        if (nkeep) {
-          uint32_t old = 0;
-          if (lane == 0) old = atomicAdd(&st->kept, nkeep);
-          old = __shfl_sync(kFull, old, 0);
-          for (uint32_t t = lane; t < nkeep; t += 32) act_out[M.eb + old + t] = keepbuf[t];
-        }
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) mn = min(mn, __shfl_xor_sync(kFull, mn, d));
-        if (lane == 0) {
-          if (mn != 0xFFFFFFFFu) atomicMin(&st->min_kept, mn);
-          if (nzero) atomicAdd(&st->processed, nzero);
-        }
-        __syncwarp();
+        wave_scan_segment(a.Up, st, M.eb, M.m, phase, level, act_sel, q_sel, W, (uint32_t)(k - mbeg),
+                          (uint32_t)(seg_end - k), s_keep[wib], ps.eid, a.err);
       }
-      push_flush(ps, a.Up, M, st, a.err, q_sel);  // entries belong to this member: publish before moving on
+      push_flush(ps, a.Up, M.eb, M.m, st, a.err, q_sel);  // entries belong to this member: publish before moving on
       k = seg_end;
     }
   }
@@ -2792,11 +2840,14 @@ __global__ void k_replan(const Member* __restrict__ mem, const MemberState* __re
 // entries (the peel: original rows without a hub map; the support pass:
 // oriented out-lists) get an open-addressed table of 2^(1+ceil(log2 d)) 8-byte
 // entries at 4 * the row's start in `pool`.  A warp reads the lengths of 32
-// consecutive rows at once and builds each qualifying row's table in turn:
-// tables of up to kTableSmem entries in its own slice of shared memory (cleared,
-// filled by compare-and-swap, then stored coalesced), longer ones in place
-// (cleared, then filled).  Every table is written whole, so the pool needs no
-// clearing beforehand; entries outside the tables are never read.
+// consecutive rows at once and builds each qualifying row's table in turn in
+// its own slice of shared memory (cleared, filled by compare-and-swap, then
+// stored coalesced).  Rows whose table is larger than the slice are listed
+// for k_table_fill_big, a block per row, which builds them in place: one warp
+// issuing a long row's global compare-and-swaps one round trip at a time took
+// milliseconds on R-MAT's largest non-hub rows.  Every table is written whole,
+// so the pool needs no clearing beforehand; entries outside the tables are
+// never read.
 constexpr uint32_t kTableSmem = 1024;  // entries per warp (8 KB)
 constexpr int kTableWarps = 4;
 
@@ -2821,7 +2872,8 @@ template <class Source>
 __global__ void __launch_bounds__(kTableWarps * 32) k_table_fill(const uint32_t* __restrict__ off, uint32_t n,
                                                                   uint32_t min_len,
                                                                   const uint32_t* __restrict__ hub_slot,
-                                                                  Source src, unsigned long long* __restrict__ pool) {
+                                                                  Source src, unsigned long long* __restrict__ pool,
+                                                                  uint32_t* __restrict__ big, uint32_t* big_count) {
   __shared__ unsigned long long s_tab[kTableWarps][kTableSmem];
   const uint32_t lane = lane_id();
   unsigned long long* st = s_tab[threadIdx.x >> 5];
@@ -2836,32 +2888,58 @@ __global__ void __launch_bounds__(kTableWarps * 32) k_table_fill(const uint32_t*
       d = __ldg(off + u + 1) - b;
       want = d >= min_len && !(hub_slot && __ldg(hub_slot + u) != kInvalid);
     }
-    unsigned todo = __ballot_sync(kFull, want);
+    const bool large = want && hash_log2cap(d) > 31 - __clz(kTableSmem);
+    if (large) big[atomicAdd(big_count, 1u)] = (uint32_t)u;
+    unsigned todo = __ballot_sync(kFull, want && !large);
     while (todo) {
       const int r = __ffs(todo) - 1;
       todo &= todo - 1;
       const uint32_t rb = __shfl_sync(kFull, b, r), rd = __shfl_sync(kFull, d, r);
       const uint32_t lg = hash_log2cap(rd), cap = 1u << lg, mask = cap - 1;
-      unsigned long long* tb = pool + 4ull * rb;
-      const bool local = cap <= kTableSmem;
-      unsigned long long* t = local ? st : tb;
-      for (uint32_t i = lane; i < cap; i += 32) t[i] = ~0ull;
+      for (uint32_t i = lane; i < cap; i += 32) st[i] = ~0ull;
       __syncwarp();
       for (uint32_t x = rb + lane; x < rb + rd; x += 32) {
         const unsigned long long en = src(x);
         if (en == ~0ull) continue;
         uint32_t at = hash_first((uint32_t)en, lg);
         for (uint32_t it = 0; it <= mask; ++it) {
-          if (atomicCAS(t + at, ~0ull, en) == ~0ull) break;
+          if (atomicCAS(st + at, ~0ull, en) == ~0ull) break;
           at = (at + 1) & mask;
         }
       }
       __syncwarp();
-      if (local) {
-        for (uint32_t i = lane; i < cap; i += 32) tb[i] = st[i];
-        __syncwarp();
+      unsigned long long* tb = pool + 4ull * rb;
+      for (uint32_t i = lane; i < cap; i += 32) tb[i] = st[i];
+      __syncwarp();
+    }
+  }
+}
+
+// The listed rows (tables larger than a warp's slice): a block per row, the
+// table cleared and filled in place by all its threads.
+template <class Source>
+__global__ void __launch_bounds__(256) k_table_fill_big(const uint32_t* __restrict__ off,
+                                                        const uint32_t* __restrict__ big,
+                                                        const uint32_t* __restrict__ big_count, Source src,
+                                                        unsigned long long* __restrict__ pool) {
+  const uint32_t nb = *big_count;
+  for (uint32_t i = blockIdx.x; i < nb; i += gridDim.x) {
+    const uint32_t u = big[i];
+    const uint32_t rb = __ldg(off + u), rd = __ldg(off + u + 1) - rb;
+    const uint32_t lg = hash_log2cap(rd), cap = 1u << lg, mask = cap - 1;
+    unsigned long long* tb = pool + 4ull * rb;
+    for (uint32_t j = threadIdx.x; j < cap; j += blockDim.x) tb[j] = ~0ull;
+    __syncthreads();
+    for (uint32_t x = rb + threadIdx.x; x < rb + rd; x += blockDim.x) {
+      const unsigned long long en = src(x);
+      if (en == ~0ull) continue;
+      uint32_t at = hash_first((uint32_t)en, lg);
+      for (uint32_t it = 0; it <= mask; ++it) {
+        if (atomicCAS(tb + at, ~0ull, en) == ~0ull) break;
+        at = (at + 1) & mask;
       }
     }
+    __syncthreads();
   }
 }
 

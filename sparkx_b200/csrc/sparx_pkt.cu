@@ -172,6 +172,7 @@ struct Counters {  // device scalars
   uint32_t hub_count;    // hub maps assigned
   uint32_t big_count;    // rows compacted by a block each
   uint32_t fin_err;      // served unions: error flags of one member's finalize
+  uint32_t table_big;    // hash tables: rows listed for the block-per-row fill
   double cc_possible;    // clustering: sum of d(d - 1)/2 over vertices
   double cc_local;       //             sum of local coefficients
   unsigned long long cc_slots;  //      sum of slot supports
@@ -892,27 +893,36 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     const uint64_t Mx = std::max<uint64_t>(W / 2, 1);
     size_t pool_b = peel_hash ? align_up(32ull * Ws) : 0, qh_b = peel_hash ? align_up(8ull * Mx) : 0;
     size_t spool_b = sup_hash ? align_up(32ull * m) : 0;
+    // rows with tables past a warp's shared slice (more than kTableSmem / 2
+    // entries) are listed for the block-per-row fill: at most W / 512 rows
+    const size_t big_b = align_up(4ull * (W / (kTableSmem / 2) + 2));
     if ((peel_hash || sup_hash) &&
-        ((J.budget && L.total + pool_b + 2 * qh_b + spool_b > J.budget) ||
-         ensure_ws3(E, pool_b + 2 * qh_b + spool_b) != SPARX_OK)) {
+        ((J.budget && L.total + pool_b + 2 * qh_b + spool_b + big_b > J.budget) ||
+         ensure_ws3(E, pool_b + 2 * qh_b + spool_b + big_b) != SPARX_OK)) {
       peel_hash = sup_hash = false;
       pool_b = qh_b = spool_b = 0;
     }
+    uint32_t* big_list = (uint32_t*)(E.ws3 + pool_b + 2 * qh_b + spool_b);
+    uint32_t* big_count = &cnt->table_big;
     if (peel_hash) {
       hpool = (unsigned long long*)E.ws3;
       qh0 = (uint2*)(E.ws3 + pool_b);
       qh1 = (uint2*)(E.ws3 + pool_b + qh_b);
       hash_min = T.hash_min_degree;
+      CU(cudaMemsetAsync(big_count, 0, 4, s));
       k_table_fill<<<grid_for(N, kTableWarps * 32, E.sm_count * 16), kTableWarps * 32, 0, s>>>(
-          J.off, N, hash_min, d_hub_slot, RowPairSource{row0}, hpool);
-      J.launches += 1;
+          J.off, N, hash_min, d_hub_slot, RowPairSource{row0}, hpool, big_list, big_count);
+      k_table_fill_big<<<E.sm_count * 8, 256, 0, s>>>(J.off, big_list, big_count, RowPairSource{row0}, hpool);
+      J.launches += 2;
     }
     if (sup_hash) {
       spool = (unsigned long long*)(E.ws3 + pool_b + 2 * qh_b);
       sup_hash_min = T.sup_hash_min;
+      CU(cudaMemsetAsync(big_count, 0, 4, s));
       k_table_fill<<<grid_for(N, kTableWarps * 32, E.sm_count * 16), kTableWarps * 32, 0, s>>>(
-          opos, N, sup_hash_min, nullptr, OutListSource{ocol}, spool);
-      J.launches += 1;
+          opos, N, sup_hash_min, nullptr, OutListSource{ocol}, spool, big_list, big_count);
+      k_table_fill_big<<<E.sm_count * 8, 256, 0, s>>>(opos, big_list, big_count, OutListSource{ocol}, spool);
+      J.launches += 2;
     }
   }
   CU(cudaEventRecord(E.tev[2], s));
