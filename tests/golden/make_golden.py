@@ -41,7 +41,7 @@ from sparkx_b200 import gen  # noqa: E402
 WORKLOADS = {
     "cfg1_er_100k_1m": dict(fn="er", n=100_000, m=1_000_000, seed=1, oracles=("pkt", "burkhardt", "fast"),
                             modes=(0, 1)),
-    "cfg2_rmat22": dict(fn="rmat", scale=22, ef=16, seed=2, oracles=("fast",), modes=(0,)),
+    "cfg2_rmat22": dict(fn="rmat", scale=22, ef=16, seed=2, oracles=("fast", "pkt"), modes=(0,)),
     # config 5's 1% tail: the first R-MAT-24 request of the served stream
     "cfg5_rmat24_tail": dict(fn="rmat", scale=24, ef=16, seed=100, oracles=("fast",), modes=(0,)),
     "cfg3_debruijn": dict(fn="dbg", seq_len=20_000_000, k=21, copies=1000, seg_len=10_000, mut_rate=0.05,
