@@ -604,7 +604,8 @@ struct UnionJob {
   ServeHook* hook = nullptr;     // served union (members join and leave between graph launches)
   bool prep_only = false;        // stop after the support pass (members about to join a served union)
   const uint32_t* smap = nullptr;  // multigraphs: caller slot -> deduplicated slot (device)
-  uint64_t budget = 0;             // device bytes the launch may hold (batched unions); 0: no bound
+  uint64_t budget = 0;             // device bytes the launch may hold (batched and served unions); 0: no bound
+  bool hook_hash = false;          // served union that takes no joins: row hash tables allowed
   uint64_t prep_m = 0, prep_Ws = 0;  // prep_only: edges and slots prepared
   std::vector<Member> members;  // vb, n, sb, w set; eb, m filled by the pipeline
   Layout L{};
@@ -877,9 +878,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     d_hub_base = hbase;
   }
   J.hubs = hubs;
-  // row hash tables for the peel's per-lane search (tuned; not in served unions,
-  // whose joining rows would have none)
-  // and out-list hash tables for the support pass (tuned)
+  // row hash tables for the peel's per-lane search (tuned; in a served union
+  // only when it takes no joins, since joining rows would have none) and
+  // out-list hash tables for the support pass (tuned)
   unsigned long long* hpool = nullptr;
   unsigned long long* spool = nullptr;
   uint2* qh0 = nullptr;
@@ -888,7 +889,8 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
   // Both are optional: when their workspace does not fit the launch's budget
   // or cannot be allocated, the launch runs without them (same results).
   {
-    bool peel_hash = T.hash_min_degree && !J.support_only && !J.prep_only && !J.hook && Ws < (1ull << 30) && Ws;
+    bool peel_hash = T.hash_min_degree && !J.support_only && !J.prep_only && (!J.hook || J.hook_hash) &&
+                     Ws < (1ull << 30) && Ws;
     bool sup_hash = T.sup_hash_min && m > 0 && m < (1ull << 28);
     const uint64_t Mx = std::max<uint64_t>(W / 2, 1);
     size_t pool_b = peel_hash ? align_up(32ull * Ws) : 0, qh_b = peel_hash ? align_up(8ull * Mx) : 0;
@@ -2227,9 +2229,14 @@ void server_worker(sparx_server* S, int lane) {
       W += h.w;
       mx = std::max<uint64_t>(mx, h.n);
     }
+    for (const HostMember& h : hm) hook.max_member_w = std::max<uint64_t>(hook.max_member_w, h.w);
+    // a union holding a member past kJoinMaxMemberSlots never takes joins: it
+    // gets no room for them, and its rows are final, so the row hash tables
+    // (built once, before the peel) are safe for it within the lane's budget
+    const bool no_joins = hook.max_member_w > kJoinMaxMemberSlots;
     // room: the largest extra (slots e, vertices e / 2) the lane's budget holds
     uint64_t extra = 0;
-    for (uint64_t step = 1ull << 40; step; step >>= 1) {
+    for (uint64_t step = 1ull << 40; step && !no_joins; step >>= 1) {
       const uint64_t e2 = extra + step;
       if (W + e2 < (1ull << 31) && layout_fits(N + e2 / 2, W + e2, kServeMaxMembers, esz, mx, main_budget))
         extra = e2;
@@ -2237,11 +2244,12 @@ void server_worker(sparx_server* S, int lane) {
     hook.N_cap = N + extra / 2;
     hook.W_cap = W + extra;
     hook.max_n0 = mx;
-    for (const HostMember& h : hm) hook.max_member_w = std::max<uint64_t>(hook.max_member_w, h.w);
     hook.delivered.assign(hook.reqs.size(), 0);
     J.N = N;
     J.W = W;
     J.hook = &hook;
+    J.hook_hash = no_joins;
+    J.budget = main_budget;
     S->unions += 1;
     J.L = make_layout(hook.N_cap, hook.W_cap, kServeMaxMembers, true, esz * hook.W_cap, mx);
     int rc = ensure_ws(E, J.L.total, false);

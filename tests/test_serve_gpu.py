@@ -129,3 +129,29 @@ def test_invalid_request_is_isolated_from_a_running_union():
             r = srv.wait(t, timeout_ms=60_000)
             assert r.status == P.OK and np.array_equal(r.truss, want)
         assert srv.wait(tb, timeout_ms=60_000).status == P.OK
+
+
+def test_large_request_runs_with_row_hash_tables():
+    """A request of more than 2^26 slots (R-MAT-22, 128 M) runs in a served union
+    that takes no joins, and so gets the row hash tables: its truss equals the
+    pinned fixture, and requests submitted while it runs are decomposed in the
+    other lanes and equal the oracle's."""
+    import hashlib
+    import json
+    import os
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "fixtures.json")))["cfg2_rmat22"]
+    big = gen.rmat(22, 16, seed=2)
+    rng = np.random.default_rng(31)
+    small = [random_graph(rng, n_max=60) for _ in range(6)] + [gen.rmat(12, 16, seed=9)]
+    with PktServer(48 << 30) as srv:
+        tb = srv.submit(big.offsets, big.neighbours)
+        time.sleep(0.05)
+        ts = [srv.submit(g.offsets, g.neighbours) for g in small]
+        rs = [srv.wait(t, timeout_ms=120_000) for t in ts]
+        rb = srv.wait(tb, timeout_ms=300_000)
+    assert rb.status == P.OK
+    sha = hashlib.sha256(np.ascontiguousarray(rb.truss, dtype="<u4").tobytes()).hexdigest()
+    assert sha == fx["modes"]["0"]["truss_sha256"]
+    for g, r in zip(small, rs):
+        assert r.status == P.OK
+        assert np.array_equal(r.truss, O.pkt(g.offsets, g.neighbours, threads=2))
