@@ -1672,6 +1672,17 @@ int run_batch_union(Engine& E, std::vector<HostMember>& hm, const Opts& O, int* 
   return SPARX_OK;
 }
 
+// workspace of the peel's row hash tables for W slots (run_union's pool, the
+// two queue descriptor arrays and the list of rows built a block each)
+size_t table_bytes(uint64_t W) {
+  return align_up(32ull * W) + 2 * align_up(8ull * std::max<uint64_t>(W / 2, 1)) +
+         align_up(4ull * (W / (kTableSmem / 2) + 2));
+}
+#ifndef SPARX_BATCH_FOR_TABLES
+#define SPARX_BATCH_FOR_TABLES 1  // size batched unions so the row hash tables fit
+#endif
+constexpr bool kBatchForTables = SPARX_BATCH_FOR_TABLES;
+
 int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, const sparx_pkt_opts* opts,
               int* status_out, sparx_pkt_stats* stats_out) {
   g_last_error.clear();
@@ -1725,7 +1736,12 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
       const size_t bytes =
           make_layout(N2, W2, (uint32_t)wave.size() + 1, true, (O.out_bits / 8) * W2, mx2).total;
       const bool fits = N2 < 0xFFFFFFFFull && W2 < 0xFFFFFFFFull && bytes <= budget && wave.size() < 65536;
-      if (!fits && !wave.empty()) break;
+      // a union grows only while its row hash tables fit as well (below 2^30
+      // slots, and within the budget with them): on the mix the tables take
+      // more off the peel than the extra unions' waves cost.  A graph too large
+      // for that still runs, alone, without them.
+      const bool fits_tables = fits && (!kBatchForTables || (W2 < (1ull << 30) && bytes + table_bytes(W2) <= budget));
+      if (!fits_tables && !wave.empty()) break;
       if (!fits) {  // a single graph over the budget
         if (status_out) status_out[h.index] = SPARX_E_OOM;
         if (!first_fail) first_fail = SPARX_E_OOM;
