@@ -242,7 +242,9 @@ typedef struct sparx_tuning {
                                >= 256, or 0 for none (1024) */
   uint32_t sample_min;      /* support: longer out-lists of at least this length are narrowed
                                through 64 samples before the search (64) */
-  uint32_t support_kernel;  /* 1 balanced edge form, 2 vertex form (1) */
+  uint32_t support_kernel;  /* 1 balanced edge form, 2 vertex form (1; 2 for keys with no
+                               slots in rows of degree >= 256 and a largest degree of 64..255,
+                               which is what sparx_tuning_lookup reports for such a key) */
   uint32_t compact_pct;     /* peel: rebuild the working rows once live entries fill at most
                                this percentage of them (85) */
   uint32_t hash_min_degree; /* peel: rows of at least this degree (>= 8) get a hash table that the

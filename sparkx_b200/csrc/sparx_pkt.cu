@@ -98,6 +98,18 @@ TuneKey tune_key(const uint32_t* hist_cnt, const unsigned long long* hist_slots,
   return k;
 }
 
+// The knobs a key gets without a cached choice: the defaults, with the vertex
+// form of the support pass for unskewed graphs whose largest degree is 64..255
+// (no slots in rows of degree >= 256).  Measured on one B200 with both forms:
+// ER n = 4.2 M, m = 67 M support 5.4 vs 7.8 ms, mix members of that class
+// 0.86-1.56 vs 1.09-2.56 ms; smaller largest degrees (de Bruijn graphs, sparse
+// ER) and skewed graphs (R-MAT) are faster with the edge form.
+Tuning default_tuning(const TuneKey& k) {
+  Tuning t;
+  if (k.skew8 == 0 && k.log_dmax >= 7 && k.log_dmax <= 8) t.support_kernel = 2;
+  return t;
+}
+
 std::mutex g_tune_mu;
 std::map<TuneKey, Tuning> g_tune;
 bool g_tune_loaded = false;
@@ -139,9 +151,9 @@ int tune_save_locked(const char* path) {
 
 // The tuning a launch uses: the autotuner's candidate, else the cached choice
 // for the key (the file named by SPARX_TUNE_FILE is read on first use), else
-// the defaults.
+// the key's defaults.
 Tuning resolve_tuning(const TuneKey& key) {
-  Tuning t;
+  Tuning t = default_tuning(key);
   if (g_tune_force) {
     t = *g_tune_force;
   } else {
@@ -2756,9 +2768,10 @@ void to_c(const Tuning& t, sparx_tuning* o) {
 int sparx_tuning_lookup(const uint32_t key[3], sparx_tuning* out, int* found) {
   if (!key || !out) return SPARX_E_ARG;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  auto it = g_tune.find(TuneKey{key[0], key[1], key[2]});
+  const TuneKey k{key[0], key[1], key[2]};
+  auto it = g_tune.find(k);
   if (found) *found = it != g_tune.end();
-  to_c(it != g_tune.end() ? it->second : Tuning{}, out);
+  to_c(it != g_tune.end() ? it->second : default_tuning(k), out);
   return SPARX_OK;
 }
 
@@ -2835,11 +2848,12 @@ int autotune_core(RunF run, uint32_t repeats, Tuning* best_out, TuneKey* key_out
   };
   Tuning cur;
   double sup = 0, rest = 0;
-  int rc = measure(cur, &sup, &rest);  // also warms the engine for this size
-  if (rc) return rc;
-  rc = measure(cur, &sup, &rest);
+  int rc = measure(cur, &sup, &rest);  // also warms the engine for this size and finds the key
   if (rc) return rc;
   const TuneKey key = g_tune_last_key;
+  cur = default_tuning(key);  // descent starts from the key's defaults
+  rc = measure(cur, &sup, &rest);
+  if (rc) return rc;
   auto try_group = [&](std::vector<Tuning> cands, bool support_time) -> int {
     double best = support_time ? sup : rest;
     for (const Tuning& c : cands) {
@@ -2858,7 +2872,7 @@ int autotune_core(RunF run, uint32_t repeats, Tuning* best_out, TuneKey* key_out
   };
   std::vector<Tuning> c1;
   for (uint32_t smp : {32u, 128u, 256u}) { Tuning t = cur; t.sample_min = smp; c1.push_back(t); }
-  { Tuning t = cur; t.support_kernel = 2; c1.push_back(t); }
+  { Tuning t = cur; t.support_kernel = cur.support_kernel == 1 ? 2 : 1; c1.push_back(t); }
   for (uint32_t sh : {16u, 64u}) { Tuning t = cur; t.sup_hash_min = sh; c1.push_back(t); }
   if ((rc = try_group(c1, true))) return rc;
   std::vector<Tuning> c2;

@@ -54,3 +54,13 @@ def test_store_lookup_save_load(tmp_path):
     with pytest.raises(P.PktError):
         P.tuning_store(key, P.PktTuning(sup_hash_min=2))
     P.tuning_clear()
+
+
+def test_defaults_depend_on_the_key():
+    """Unskewed keys with a largest degree of 64..255 default to the vertex form
+    of the support pass; other keys keep the edge form."""
+    P.tuning_clear()
+    assert P.tuning_lookup((24, 7, 0)) == (P.PktTuning(support_kernel=2), False)
+    assert P.tuning_lookup((27, 8, 0)) == (P.PktTuning(support_kernel=2), False)
+    for key in ((24, 6, 0), (24, 9, 0), (24, 7, 1), (25, 3, 0), (27, 20, 4)):
+        assert P.tuning_lookup(key) == (P.PktTuning(), False), key
