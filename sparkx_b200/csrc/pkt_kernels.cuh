@@ -809,6 +809,13 @@ __device__ __forceinline__ uint32_t probe_list(const unsigned long long* __restr
   return kInvalid;
 }
 
+#ifndef SPARX_SUP_SAMPLES
+#define SPARX_SUP_SAMPLES 2  // samples of a long out-list per lane in the support fast path (2 or 4)
+#endif
+constexpr int kSupSamples = SPARX_SUP_SAMPLES;
+static_assert(kSupSamples == 2 || kSupSamples == 4, "2 or 4 samples per lane");
+constexpr int kSupSampleShift = kSupSamples == 4 ? 7 : 6;  // log2 of the sample count
+
 template <bool kMulti, bool kHash>
 __global__ void __launch_bounds__(256, 8) k_support_balanced(
     const uint32_t* __restrict__ opos, const uint32_t* __restrict__ ocol,
@@ -888,14 +895,18 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
         const bool a_short = ae - ab <= be - bb;
         const uint32_t fsb = a_short ? ab : bb, flb = a_short ? bb : ab, fle = a_short ? be : ae;
         const unsigned long long stop = min(kend, e_end);
-        // a long list is narrowed first through 64 evenly spaced samples, two
-        // per lane (gathered once per edge, then shuffles), leaving ~1/64 of it
-        // to search
+        // a long list is narrowed first through 32 * kSupSamples evenly spaced
+        // samples, kSupSamples per lane (gathered once per edge, then
+        // shuffles), leaving that fraction of it to search
         const uint32_t flen = fle - flb;
         const bool hashed = kHash && flen >= hash_min;
         const bool sampled = !hashed && flen >= sample_min;
-        const uint32_t smp = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane) * flen) >> 6)) : 0u;
-        const uint32_t smp1 = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(2 * lane + 1) * flen) >> 6)) : 0u;
+        uint32_t smp[kSupSamples];
+#pragma unroll
+        for (int x = 0; x < kSupSamples; ++x)
+          smp[x] = sampled ? __ldg(ocol + flb + (uint32_t)(((unsigned long long)(kSupSamples * lane + x) * flen) >>
+                                                          kSupSampleShift))
+                           : 0u;
         do {
           kb += 32;
           const uint32_t fo = (uint32_t)(kb + lane - e_start);
@@ -927,13 +938,18 @@ __global__ void __launch_bounds__(256, 8) k_support_balanced(
             uint32_t t = 0;
 #pragma unroll
             for (int d = 16; d > 0; d >>= 1) {
-              const uint32_t cand = __shfl_sync(kFull, smp, t + d);
+              const uint32_t cand = __shfl_sync(kFull, smp[0], t + d);
               if (cand <= c) t += d;
             }
-            // sample 2t is the last even one <= c; its odd neighbour decides
-            const uint32_t kk = 2 * t + (__shfl_sync(kFull, smp1, t) <= c ? 1u : 0u);
-            lo = flb + (uint32_t)(((unsigned long long)kk * flen) >> 6);
-            hi = kk == 63 ? fle : flb + (uint32_t)(((unsigned long long)(kk + 1) * flen) >> 6);
+            // lane t's first sample is the last lane-first one <= c; its
+            // other samples (ascending) decide how far past it c lies
+            uint32_t kk = kSupSamples * t;
+#pragma unroll
+            for (int x = 1; x < kSupSamples; ++x) kk += __shfl_sync(kFull, smp[x], t) <= c ? 1u : 0u;
+            lo = flb + (uint32_t)(((unsigned long long)kk * flen) >> kSupSampleShift);
+            hi = kk == 32 * kSupSamples - 1
+                     ? fle
+                     : flb + (uint32_t)(((unsigned long long)(kk + 1) * flen) >> kSupSampleShift);
           }
           const uint32_t q = lower_bound_u32(ocol, lo, hi, c);
           const bool fh = q < hi && __ldg(ocol + q) == c;
