@@ -2291,6 +2291,14 @@ void server_worker(sparx_server* S, int lane) {
       rc = upload_union(E, hm, J.members, N, W, J.off, (uint32_t*)J.nbr, s);
       if (!rc) rc = run_union(E, J, S->O, s);
     }
+    if (E.ws3) {
+      // the hash tables of a union without join room leave with it, so the
+      // lane holds no more than its share while its next union runs
+      cudaStreamSynchronize(E.stream);
+      cudaFree(E.ws3);
+      E.ws3 = nullptr;
+      E.ws3_cap = 0;
+    }
     if (rc) {
       // members not delivered: run them again through the batch path (which
       // names the member an input defect belongs to)
