@@ -1837,25 +1837,32 @@ __global__ void __launch_bounds__(kWaveThreads, SPARX_WAVE_MINB) k_wave(WaveArgs
           const uint32_t qcount = w32[kCtxQcount];
           const unsigned long long* q = (w32[kCtxQsel] ? U.q1 : U.q0) + w32[kCtxEb];
           const bool valid = r + lane < seg_len;
-          const unsigned long long j = w64[kCtxJb] + r + lane;
           // the window's entries, loaded once: each lane picks its own by a
           // shuffle search on the work starts (entries own >= 1 element, so
-          // 32 consecutive elements span at most 32 entries)
+          // 32 consecutive elements span at most 32 entries).  The search runs
+          // on 32-bit distances from the iteration's first element jr: the
+          // window's first entry owns element jr - 1 or jr and an entry's work
+          // is below 2^31, so every distance lies in (-2^31, 2^31); entries
+          // past the queue's end clamp to the most negative.  Lane l's
+          // element jr + l lies in entry x iff jr - start(x) >= -l.
+          const unsigned long long jr = w64[kCtxJb] + r;
           const unsigned long long qv = (i + lane < qcount) ? q[i + lane] : ~0ull;
+          const int32_t dq = (int32_t)max((long long)(jr - (qv >> kEidBits)), (long long)INT32_MIN);
           uint32_t t = 0;
 #pragma unroll
           for (int d = 16; d > 0; d >>= 1) {
-            const unsigned long long cand = __shfl_sync(kFull, qv, t + d) >> kEidBits;
-            if (cand <= j) t += d;
+            const int32_t cand = __shfl_sync(kFull, dq, t + d);
+            if (cand >= -(int32_t)lane) t += d;
           }
-          const unsigned long long ent = __shfl_sync(kFull, qv, t);
+          const int32_t dt = __shfl_sync(kFull, dq, t);
+          const uint32_t eid_t = __shfl_sync(kFull, (uint32_t)qv & kEidMask, t);
           const uint32_t x = i + t;
           const uint32_t last = min(31u, seg_len - 1 - r);
           const uint32_t x_last = __shfl_sync(kFull, x, last);
           uint32_t e = 0, o = 0, sb = 0, slen = 0, lb = 0, le = 0;
           if (valid) {
-            e = w32[kCtxEb] + (uint32_t)(ent & kEidMask);
-            o = (uint32_t)(j - (ent >> kEidBits));
+            e = w32[kCtxEb] + eid_t;
+            o = (uint32_t)(dt + (int32_t)lane);
             const uint4 dsc = ((w32[kCtxQsel] ? U.qd1 : U.qd0) + w32[kCtxEb])[x];
             sb = dsc.x;
             slen = dsc.y;
