@@ -600,6 +600,7 @@ struct PeelCtx {
   uint64_t m;                     // edges in the union
   uint64_t Ws;                    // slots in the union
   uint32_t N, G;
+  uint64_t waves_run = 0;         // waves the union's loop has run so far
   bool resume = false;            // the hook added members or some are still running
 };
 // Served unions: called at every stop of the peel loop (a member finished,
@@ -1061,6 +1062,7 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
       ctx.Ws = pWs;
       ctx.N = pN;
       ctx.G = pG;
+      ctx.waves_run = hctl->waves_run;
       int rc = J.hook->at_stop(E, J, ctx, reason, s);
       if (rc) return rc;
       U = ctx.U;
@@ -1789,6 +1791,10 @@ constexpr uint32_t kServeMaxMembers = 4096;   // members per served union, joine
 // member advances one step per wave, and such a member's waves would set the
 // pace of small newcomers (R-MAT-24's waves take milliseconds)
 constexpr uint64_t kJoinMaxMemberSlots = 1ull << 26;
+// nor does a union whose waves, measured between its last two stops, take
+// longer than this on average (a large member sets every member's pace; a
+// union of small graphs runs at the ~15-25 us floor of a wave)
+constexpr double kJoinMaxWaveUs = 60.0;
 
 struct ServerReq {
   uint64_t ticket = 0;
@@ -1869,6 +1875,11 @@ struct LaneHook : ServeHook {
   uint64_t N_cap = 0, W_cap = 0;    // the union's room
   uint64_t max_n0 = 0;              // largest initial member (the hub pool was sized for it)
   uint64_t max_member_w = 0;        // slots of the union's largest member
+  // the union's wave pace, measured between stops (host work at a stop excluded)
+  std::chrono::steady_clock::time_point t_mark{};
+  uint64_t w_mark = 0;
+  bool marked = false;
+  double wave_us = 0;
 
   int deliver(Engine& E, UnionJob& J, uint32_t G, cudaStream_t s) {
     const Layout& L = J.L;
@@ -1937,6 +1948,7 @@ struct LaneHook : ServeHook {
     S->admit_host[lane] = 0;
     if (J.multi) return SPARX_OK;  // a deduplicated union has no room for more rows: wait for a lane
     if (max_member_w > kJoinMaxMemberSlots) return SPARX_OK;
+    if (wave_us > kJoinMaxWaveUs) return SPARX_OK;  // its waves would set a newcomer's pace
     std::vector<ServerReq*> take;
     {
       std::lock_guard<std::mutex> lk(S->mu);
@@ -2121,6 +2133,9 @@ struct LaneHook : ServeHook {
   }
 
   int at_stop(Engine& E, UnionJob& J, PeelCtx& ctx, uint32_t reason, cudaStream_t s) override {
+    if (marked && ctx.waves_run >= w_mark + 16)
+      wave_us = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t_mark).count() /
+                (double)(ctx.waves_run - w_mark);
     int rc = deliver(E, J, ctx.G, s);
     if (rc) return rc;
     uint32_t joined = 0;
@@ -2136,6 +2151,9 @@ struct LaneHook : ServeHook {
     bool live = false;
     for (size_t g = 0; g < delivered.size(); ++g) live |= !delivered[g];
     ctx.resume = live;
+    t_mark = std::chrono::steady_clock::now();
+    w_mark = ctx.waves_run;
+    marked = true;
     return SPARX_OK;
   }
 };
