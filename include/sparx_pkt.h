@@ -320,8 +320,11 @@ typedef struct sparx_server sparx_server;
  * join it.  An idle lane packs the queued requests that fit into a union sized
  * to its share; while that union's peel runs, a submitted request stops it at
  * its next wave, and the requests that fit join the union there (prepared on
- * the lane's second engine and placed behind the running members); every
- * member's result goes back as soon as its own peel ends.  A request needing
+ * the lane's second engine and placed behind the running members).  A union
+ * takes no joins while it holds a graph of more than 2^26 slots or while its
+ * waves average more than 60 us (newcomers then wait for a lane), and a union
+ * without join room gets the row hash tables.  Every member's result goes back
+ * as soon as its own peel ends.  A request needing
  * more than any lane holds completes with SPARX_E_OOM.  Requests stay
  * addressable by ticket until sparx_server_destroy. */
 int sparx_server_create(sparx_server** out, uint64_t hbm_budget_bytes, const sparx_pkt_opts* opts);
