@@ -163,10 +163,14 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const unsigned lon
   hist[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
 }
 
+// kPay: a u32 payload travels with each key (pin -> pout), in the same order.
+template <bool kPay>
 __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const unsigned long long* __restrict__ in,
                                                                  unsigned long long* __restrict__ out,
                                                                  unsigned long long count, int shift,
-                                                                 const uint32_t* __restrict__ start) {
+                                                                 const uint32_t* __restrict__ start,
+                                                                 const uint32_t* __restrict__ pin,
+                                                                 uint32_t* __restrict__ pout) {
   __shared__ uint32_t warp_cnt[kRadixWarps][256];
   __shared__ uint32_t run[256];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -180,6 +184,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const unsigned 
     const unsigned long long i = r + threadIdx.x;
     const bool valid = i < b1;
     const unsigned long long k = valid ? in[i] : 0ull;
+    const uint32_t pl = kPay && valid ? pin[i] : 0u;
     const uint32_t d = valid ? (uint32_t)((k >> shift) & 0xFF) : 256u;
     const unsigned same = __match_any_sync(0xFFFFFFFFu, d);
     const uint32_t in_warp = __popc(same & ((1u << lane) - 1));
@@ -189,6 +194,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const unsigned 
       uint32_t before = 0;
       for (uint32_t w = 0; w < wid; ++w) before += warp_cnt[w][d];
       out[run[d] + before + in_warp] = k;
+      if (kPay) pout[run[d] + before + in_warp] = pl;
     }
     __syncthreads();
     // advance the digit's running start, clear the counts for the next round

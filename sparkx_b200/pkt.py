@@ -89,7 +89,7 @@ class _GraphView(ctypes.Structure):
 class _Tuning(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint32) for name in
                 ("struct_size", "merge_ratio", "hub_min_degree", "sample_min", "support_kernel", "compact_pct",
-                 "hash_min_degree", "sup_hash_min")]
+                 "hash_min_degree", "sup_hash_min", "relabel")]
 
 
 EXPORTS = [
@@ -549,6 +549,7 @@ class PktTuning:
     compact_pct: int = 85
     hash_min_degree: int = 128
     sup_hash_min: int = 0
+    relabel: int = 0
 
     def c(self) -> _Tuning:
         t = _Tuning()

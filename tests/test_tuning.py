@@ -34,7 +34,7 @@ def test_signature_matches_the_degree_histogram():
 
 def test_store_lookup_save_load(tmp_path):
     P.tuning_clear()
-    key = (20, 12, 3)
+    key = (20, 12, 1)
     t, found = P.tuning_lookup(key)
     assert not found and t == P.PktTuning()
     mine = P.PktTuning(merge_ratio=4, hub_min_degree=512, sample_min=128, support_kernel=2, compact_pct=75,
@@ -58,9 +58,14 @@ def test_store_lookup_save_load(tmp_path):
 
 def test_defaults_depend_on_the_key():
     """Unskewed keys with a largest degree of 64..255 default to the vertex form
-    of the support pass; other keys keep the edge form."""
+    of the support pass; other keys keep the edge form; large skewed keys relabel."""
     P.tuning_clear()
     assert P.tuning_lookup((24, 7, 0)) == (P.PktTuning(support_kernel=2), False)
     assert P.tuning_lookup((27, 8, 0)) == (P.PktTuning(support_kernel=2), False)
-    for key in ((24, 6, 0), (24, 9, 0), (24, 7, 1), (25, 3, 0), (27, 20, 4)):
+    for key in ((24, 6, 0), (24, 9, 0), (24, 7, 1), (25, 3, 0), (27, 20, 1)):
+        assert P.tuning_lookup(key) == (P.PktTuning(), False), key
+    # large skewed keys (2^26 slots or more, a quarter of them in rows of degree >= 256) relabel
+    for key in ((27, 20, 4), (26, 18, 5), (28, 19, 2)):
+        assert P.tuning_lookup(key) == (P.PktTuning(relabel=1), False), key
+    for key in ((25, 17, 4), (22, 12, 2), (20, 15, 7)):
         assert P.tuning_lookup(key) == (P.PktTuning(), False), key
