@@ -887,8 +887,10 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     if (pass == 0) J.slot_self_loops = hc.self_loops;
     if (pass == 0 && hc.err == 0 && G == 1 && N > 1 && W > 0 && !J.support_only && !J.prep_only && !J.hook &&
         resolve_tuning(tune_key(hist, hist_slots, W)).relabel) {
-      // a sound simple graph: orient its degree-ordered copy instead
+      // a sound simple graph: orient its degree-ordered copy instead (when the
+      // device has no room for the copy, the caller's ids are used as they are)
       int rc = relabel_graph(E, J, N, W, big, &cnt->big_count, s);
+      if (rc == SPARX_E_OOM) break;
       if (rc) return rc;
       smap = const_cast<uint32_t*>(J.smap);
       // the next pass counts them again
