@@ -400,7 +400,8 @@ int ensure_ws2(Engine& E, size_t bytes) {
   cudaError_t e = cudaMalloc(&E.ws2, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    set_error(std::string("multigraph workspace of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+    set_error(std::string("second workspace (deduplicated or relabelled rows) of ") + std::to_string(bytes) + " bytes: " +
+              cudaGetErrorString(e));
     E.ws2 = nullptr;
     return SPARX_E_OOM;
   }
