@@ -6,7 +6,9 @@
 // needed.  On R-MAT-22 the same engine ran the bucket-ordered copy of the
 // graph 32 ms faster than the original (support 86.5 -> 80.6 ms, peel 340.6
 // -> 315.1 ms): edges of similar-degree vertices sit together, so the peel's
-// random state and row reads fall on far fewer lines.
+// random state and row reads fall on far fewer lines.  Below 2^26 slots it
+// costs more than it saves (R-MAT-20 and 21: peel 5-6 ms slower), so the
+// tuning turns it on only for large skewed graphs.
 //   k_vertex_keys       (bucket << 32 | id) per vertex, for one radix pass
 //   k_vertex_order      new id and new degree per vertex
 //   k_relabel_rows      a warp per row of at most kRelabelWarpRow entries
