@@ -58,6 +58,8 @@ enum : uint32_t {
 
 enum : uint32_t { kPhaseScan0 = 0, kPhaseScan = 1, kPhaseProc = 2, kPhaseDone = 3 };
 
+constexpr uint32_t kVinfoHub = 0x80000000u;  // Union::vinfo: the longer row's vertex has a hub map
+
 struct Union {  // the prepared concatenated graph, as the peel sees it
   const uint32_t* off;             // working row offsets
   const unsigned long long* row;   // working rows: (id | edge id << 32)
@@ -75,6 +77,9 @@ struct Union {  // the prepared concatenated graph, as the peel sees it
   const unsigned long long* hpool; // row hash tables (nullptr = none): vertex v's at 4 * off0[v]
   const uint32_t* off0;            // the rows' original offsets (hash table positions)
   uint2* qh[2];                    // per queue entry: {hash table position, log2 capacity} or 0
+  const unsigned long long* vinfo; // per vertex, what a frontier edge's longer row offers (k_vinfo):
+                                   // kVinfoHub | hub map base, or {table position, log2 capacity},
+                                   // or 0; nullptr when there are neither hub maps nor tables
   uint32_t hash_min;               // rows of at least this degree have a hash table (0: none)
   uint32_t n;
   uint32_t m;
@@ -132,19 +137,20 @@ struct UnionRegs {
   const uint32_t* __restrict__ off0;
   uint2* qh0;
   uint2* qh1;
+  const unsigned long long* __restrict__ vinfo;
   uint32_t n;
   uint32_t hash_min;
   __device__ __forceinline__ explicit UnionRegs(const Union* p)
       : off(p->off), row(p->row), ocol(p->ocol), osrc(p->osrc), es(p->es),
         act0(p->act[0]), act1(p->act[1]), q0(p->q[0]), q1(p->q[1]),
         qd0(p->qd[0]), qd1(p->qd[1]), hub_slot(p->hub_slot), hub_map(p->hub_map), hub_base(p->hub_base),
-        mu(nullptr), hpool(p->hpool), off0(p->off0), qh0(p->qh[0]), qh1(p->qh[1]), n(p->n),
+        mu(nullptr), hpool(p->hpool), off0(p->off0), qh0(p->qh[0]), qh1(p->qh[1]), vinfo(p->vinfo), n(p->n),
         hash_min(p->hash_min) {}
   __device__ __forceinline__ UnionRegs(const Union* p, const PeelArrays& a)
       : off(p->off), row(p->row), ocol(a.ocol), osrc(a.osrc), es(a.es),
         act0(a.act0), act1(a.act1), q0(a.q0), q1(a.q1),
         qd0(a.qd0), qd1(a.qd1), hub_slot(a.hub_slot), hub_map(a.hub_map), hub_base(a.hub_base), mu(a.mu),
-        hpool(a.hpool), off0(a.off0), qh0(a.qh0), qh1(a.qh1), n(a.n), hash_min(a.hash_min) {}
+        hpool(a.hpool), off0(a.off0), qh0(a.qh0), qh1(a.qh1), vinfo(nullptr), n(a.n), hash_min(a.hash_min) {}
 };
 
 // Row hash tables: vertex v of original degree d >= hash_min (and no hub map)
@@ -1329,23 +1335,38 @@ struct WaveArgs {
 // *hq: the longer row's hash table {position, log2 capacity}, or {0, 0}.
 __device__ __forceinline__ uint4 edge_desc(const UnionRegs& U, uint32_t x, uint2* hq) {
   const uint32_t u = __ldg(U.osrc + x), v = __ldg(U.ocol + x);
+  // row bounds and both vertices' longer-row offers, all in one round of loads
   const uint32_t ub = __ldg(U.off + u), ue = __ldg(U.off + u + 1);
   const uint32_t vb = __ldg(U.off + v), ve = __ldg(U.off + v + 1);
+  const unsigned long long iu = U.vinfo ? __ldg(U.vinfo + u) : 0ull, iv = U.vinfo ? __ldg(U.vinfo + v) : 0ull;
   const bool u_short = ue - ub <= ve - vb;
+  const unsigned long long li = u_short ? iv : iu;
+  const uint32_t lo = (uint32_t)li, hi = (uint32_t)(li >> 32);
   *hq = make_uint2(0, 0);
-  if (U.hub_slot) {
-    const uint32_t hs = __ldg(U.hub_slot + (u_short ? v : u));
-    if (hs != kInvalid) {
-      const uint32_t base = __ldg(U.hub_base + hs);
-      return u_short ? make_uint4(ub, ue - ub, kHubDesc, base) : make_uint4(vb, ve - vb, kHubDesc, base);
-    }
-  }
-  if (U.hash_min) {
-    const uint32_t lv = u_short ? v : u;
-    const uint32_t b0 = __ldg(U.off0 + lv), d0 = __ldg(U.off0 + lv + 1) - b0;
-    if (d0 >= U.hash_min) *hq = make_uint2(4 * b0, hash_log2cap(d0));
-  }
+  if (hi & kVinfoHub)
+    return u_short ? make_uint4(ub, ue - ub, kHubDesc, lo) : make_uint4(vb, ve - vb, kHubDesc, lo);
+  if (hi) *hq = make_uint2(lo, hi);
   return u_short ? make_uint4(ub, ue - ub, vb, ve) : make_uint4(vb, ve - vb, ub, ue);
+}
+
+// What each vertex's row offers when it is a frontier edge's longer row: its
+// hub map (kVinfoHub | the map's base), else its hash table (log2 capacity <<
+// 32 | the table's position), else nothing.
+__global__ void __launch_bounds__(256) k_vinfo(uint32_t n, const uint32_t* __restrict__ hub_slot,
+                                               const uint32_t* __restrict__ hub_base,
+                                               const uint32_t* __restrict__ off0, uint32_t hash_min,
+                                               unsigned long long* __restrict__ vinfo) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    unsigned long long info = 0;
+    const uint32_t hs = hub_slot ? __ldg(hub_slot + v) : kInvalid;
+    if (hs != kInvalid) {
+      info = ((unsigned long long)kVinfoHub << 32) | __ldg(hub_base + hs);
+    } else if (hash_min) {
+      const uint32_t b0 = __ldg(off0 + v), d0 = __ldg(off0 + v + 1) - b0;
+      if (d0 >= hash_min) info = ((unsigned long long)hash_log2cap(d0) << 32) | (4u * b0);
+    }
+    vinfo[v] = info;
+  }
 }
 
 // PKT sub-level rule for one triangle (e, f, h) of frontier edge e at level l,

@@ -203,6 +203,7 @@ struct Counters {  // device scalars
 struct Layout {
   size_t off, nbr, row0, dplus, opos, ocol, osrc, es, act0, act1, q0, q1, qd0, qd1, out, stage0, stage1;
   size_t offA, offB, rowA, rowB;  // compaction ping-pong buffers (0 when compaction is off)
+  size_t vinfo;                   // per vertex: what its row offers as a longer row (hub map / hash table)
   size_t alive;                   // compaction: one bit per edge, set while it is unprocessed
   size_t big;                     // compaction: rows longer than kWarpRow (a block each)
   size_t hub_slot, hub_vertex, hub_base, hub_hist, hub_map;  // hub maps (hub_cap == 0: none)
@@ -259,6 +260,7 @@ Layout make_layout(uint64_t N, uint64_t W, uint32_t G, bool own_nbr, size_t out_
   if (max_n == 0) max_n = N;
   L.hub_cap = hub_capacity(max_n, W);
   L.hub_hist = take(4 * 34 + 8 * 34);  // vertices, then slots, per log2 degree (always: the tuning key)
+  L.vinfo = take(8ull * N);              // per vertex: its row's hub map or hash table (k_vinfo)
   if (L.hub_cap) {
     L.hub_pool = std::min<unsigned long long>(4ull * L.hub_cap * max_n, kHubBudgetBytes) / 4;
     L.hub_slot = take(4 * N);
@@ -1094,6 +1096,13 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     U.qh[0] = qh0;
     U.qh[1] = qh1;
     U.hash_min = hash_min;
+    U.vinfo = nullptr;
+    if (d_hub_slot || hash_min) {
+      unsigned long long* vinfo = at<unsigned long long>(E, L.vinfo);
+      k_vinfo<<<grid_for(N, 256, E.sm_count * 16), 256, 0, s>>>(N, d_hub_slot, d_hub_base, J.off, hash_min, vinfo);
+      J.launches += 1;
+      U.vinfo = vinfo;
+    }
     U.n = N;
     U.m = (uint32_t)m;
     U.width = (uint32_t)W;
@@ -2189,6 +2198,8 @@ struct LaneHook : ServeHook {
       CU(cudaMemcpyAsync(at<int2>(E, L.es) + m0, at<int2>(*P, PJ.L.es), 8 * mp, cudaMemcpyDeviceToDevice, s));
     }
     if (ctx.U.hub_slot && Np) CU(cudaMemsetAsync(at<uint32_t>(E, L.hub_slot) + N0, 0xFF, 4 * Np, s));
+    // joining rows offer neither hub maps nor tables
+    if (ctx.U.vinfo && Np) CU(cudaMemsetAsync(at<unsigned long long>(E, L.vinfo) + N0, 0, 8 * Np, s));
     Counters* cnt = at<Counters>(E, L.cnt);
     if (Np) k_big_rows_range<<<grid_for(Np, 256, E.sm_count * 8), 256, 0, s>>>(off, N0, N0 + (uint32_t)Np,
                                                                                  at<uint32_t>(E, L.big),
