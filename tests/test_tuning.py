@@ -38,7 +38,7 @@ def test_store_lookup_save_load(tmp_path):
     t, found = P.tuning_lookup(key)
     assert not found and t == P.PktTuning()
     mine = P.PktTuning(merge_ratio=4, hub_min_degree=512, sample_min=128, support_kernel=2, compact_pct=75,
-                       hash_min_degree=32, sup_hash_min=16)
+                       hash_min_degree=32, sup_hash_min=16, relabel=1)
     P.tuning_store(key, mine)
     assert P.tuning_lookup(key) == (mine, True)
     path = str(tmp_path / "tune.txt")
@@ -53,6 +53,8 @@ def test_store_lookup_save_load(tmp_path):
         P.tuning_store(key, P.PktTuning(hub_min_degree=100))
     with pytest.raises(P.PktError):
         P.tuning_store(key, P.PktTuning(sup_hash_min=2))
+    with pytest.raises(P.PktError):
+        P.tuning_store(key, P.PktTuning(relabel=2))
     P.tuning_clear()
 
 
