@@ -888,8 +888,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaMemcpyAsync(hist_slots, hub_hist_slots, 8 * 34, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     if (pass == 0) J.slot_self_loops = hc.self_loops;
+    // (single-graph calls only: a batch's budget does not count the relabelled copy)
     if (pass == 0 && hc.err == 0 && G == 1 && N > 1 && W > 0 && !J.support_only && !J.prep_only && !J.hook &&
-        resolve_tuning(tune_key(hist, hist_slots, W)).relabel) {
+        !J.budget && resolve_tuning(tune_key(hist, hist_slots, W)).relabel) {
       // a sound simple graph: orient its degree-ordered copy instead (when the
       // device has no room for the copy, the caller's ids are used as they are)
       int rc = relabel_graph(E, J, N, W, big, &cnt->big_count, s);
