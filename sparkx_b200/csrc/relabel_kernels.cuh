@@ -1,5 +1,6 @@
-// Vertex relabelling for locality (single graphs): vertices take new ids in
-// (floor(log2 degree), id) order and the CSR is rebuilt on them; the caller's
+// Vertex relabelling for locality: vertices take new ids in (floor(log2
+// degree), id) order, within their own graph's id range in a union, and the
+// CSR is rebuilt on them; the caller's
 // slot s maps to the new slot rmap[s].  Rows are sorted by id, and within a
 // degree bucket the new ids keep the old order, so each new row is the old
 // row stably partitioned by its neighbours' buckets: no sort of the slots is
@@ -9,7 +10,8 @@
 // random state and row reads fall on far fewer lines.  Below 2^26 slots it
 // costs more than it saves (R-MAT-20 and 21: peel 5-6 ms slower), so the
 // tuning turns it on only for large skewed graphs.
-//   k_vertex_keys       (bucket << 32 | id) per vertex, for one radix pass
+//   k_vertex_keys       ((member << 5 | bucket) << 32 | id) per vertex, for the
+//                       radix passes (one for a single graph)
 //   k_vertex_order      new id and new degree per vertex
 //   k_relabel_rows      a warp per row of at most kRelabelWarpRow entries
 //   k_relabel_rows_big  a block per longer row (the listed big rows)
@@ -27,12 +29,20 @@ constexpr uint32_t kRelabelWarpRow = 2048;  // longer rows: a block each (the or
 
 __device__ __forceinline__ uint32_t degree_bucket(uint32_t d) { return d > 1 ? 31u - __clz(d) : 0u; }
 
+// Keys ((member << 5 | bucket) << 32 | id): in a union of G graphs (members
+// by ascending first vertex `vb`) every vertex keeps to its member's id range.
 __global__ void __launch_bounds__(256) k_vertex_keys(const uint32_t* __restrict__ off, uint32_t n,
+                                                     const uint32_t* __restrict__ member_vb, uint32_t G,
                                                      unsigned long long* __restrict__ keys,
                                                      uint8_t* __restrict__ bucket) {
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
     const uint32_t b = degree_bucket(__ldg(off + u + 1) - __ldg(off + u));
-    keys[u] = ((unsigned long long)b << 32) | u;
+    uint32_t lo = 0, hi = G - 1;  // the last member whose first vertex is <= u
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(member_vb + mid) <= u) lo = mid; else hi = mid - 1;
+    }
+    keys[u] = ((unsigned long long)((lo << 5) | b) << 32) | u;
     bucket[u] = (uint8_t)b;
   }
 }

@@ -774,9 +774,10 @@ SortedBufs radix_sort(int sm_count, unsigned long long* ka, unsigned long long* 
   return {ka, pa};
 }
 
-// Rebuild a single graph's CSR on vertex ids in (floor(log2 degree), id)
-// order (relabel_kernels.cuh): J.off / J.nbr become the new rows, J.smap the
-// caller slot -> new slot map the finalize reads through.  `big` / `big_count`:
+// Rebuild a graph's (or a union's) CSR on vertex ids in (floor(log2 degree),
+// id) order within each member's id range (relabel_kernels.cuh): J.off / J.nbr
+// become the new rows, J.smap the caller slot -> new slot map the finalize
+// reads through.  `big` / `big_count`:
 // the rows longer than kWarpRow (listed by the orientation pass).  Everything
 // lives in the second workspace.
 static_assert(kRelabelWarpRow == kWarpRow, "the relabel's block rows are the orientation's big-row list");
@@ -793,7 +794,8 @@ int relabel_graph(Engine& E, UnionJob& J, uint32_t N, uint64_t W, const uint32_t
   const size_t o_off = take(4ull * (N + 1)), o_nbr = take(4 * W), o_rmap = take(4 * W), o_va = take(8ull * N),
                o_vb = take(8ull * N), o_newid = take(4ull * N), o_deg = take(4ull * N), o_bucket = take(N),
                o_hist = take(4ull * 256 * blocks_max), o_hstart = take(4ull * (256 * blocks_max + 1)),
-               o_tiles = take(4 * (scan_items / kScanTile + 4)), o_grand = take(4);
+               o_tiles = take(4 * (scan_items / kScanTile + 4)), o_grand = take(4),
+               o_mvb = take(4ull * J.members.size());
   int rc = ensure_ws2(E, p);
   if (rc) return rc;
   char* b = E.ws2;
@@ -805,12 +807,21 @@ int relabel_graph(Engine& E, UnionJob& J, uint32_t N, uint64_t W, const uint32_t
   uint8_t* bucket = (uint8_t*)(b + o_bucket);
   uint32_t* tiles = (uint32_t*)(b + o_tiles);
   uint32_t* grand = (uint32_t*)(b + o_grand);
-  // vertices: (bucket, id) order, one radix pass over the bucket (< 32)
-  k_vertex_keys<<<grid_for(N, 256, E.sm_count * 16), 256, 0, s>>>(J.off, N, (unsigned long long*)(b + o_va),
-                                                                   bucket);
+  // vertices: (member, bucket, id) order; radix passes over the member and
+  // bucket bits (one pass for a single graph)
+  const uint32_t G = (uint32_t)J.members.size();
+  std::vector<uint32_t> mvb(G);
+  for (uint32_t g = 0; g < G; ++g) mvb[g] = J.members[g].vb;
+  uint32_t* member_vb = (uint32_t*)(b + o_mvb);
+  CU(cudaMemcpyAsync(member_vb, mvb.data(), 4ull * G, cudaMemcpyHostToDevice, s));  // pageable: staged
+  const int kbits = 5 + (G > 1 ? 32 - __builtin_clz(G - 1) : 0);
+  std::vector<int> vshifts;
+  for (int bit = 0; bit < kbits; bit += 8) vshifts.push_back(32 + bit);
+  k_vertex_keys<<<grid_for(N, 256, E.sm_count * 16), 256, 0, s>>>(J.off, N, member_vb, G,
+                                                                   (unsigned long long*)(b + o_va), bucket);
   const SortedBufs vs = radix_sort(E.sm_count, (unsigned long long*)(b + o_va), (unsigned long long*)(b + o_vb),
-                                   nullptr, nullptr, N, std::vector<int>{32}, (uint32_t*)(b + o_hist),
-                                   (uint32_t*)(b + o_hstart), tiles, grand, s);
+                                   nullptr, nullptr, N, vshifts, (uint32_t*)(b + o_hist), (uint32_t*)(b + o_hstart),
+                                   tiles, grand, s);
   k_vertex_order<<<grid_for(N, 256, E.sm_count * 16), 256, 0, s>>>(vs.keys, J.off, N, newid, deg_r);
   exclusive_scan<uint32_t>(LoadU32{deg_r}, N, off_r, tiles, grand, s);
   // rows: each moved to its new place and stably partitioned by bucket
@@ -888,9 +899,9 @@ int run_union(Engine& E, UnionJob& J, const Opts& O, cudaStream_t s) {
     CU(cudaMemcpyAsync(hist_slots, hub_hist_slots, 8 * 34, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     if (pass == 0) J.slot_self_loops = hc.self_loops;
-    // (single-graph calls only: a batch's budget does not count the relabelled copy)
-    if (pass == 0 && hc.err == 0 && G == 1 && N > 1 && W > 0 && !J.support_only && !J.prep_only && !J.hook &&
-        !J.budget && resolve_tuning(tune_key(hist, hist_slots, W)).relabel) {
+    // (batched unions: the packer counted the relabelled copy in their budget)
+    if (pass == 0 && hc.err == 0 && N > 1 && W > 0 && !J.support_only && !J.prep_only && !J.hook &&
+        resolve_tuning(tune_key(hist, hist_slots, W)).relabel) {
       // a sound simple graph: orient its degree-ordered copy instead (when the
       // device has no room for the copy, the caller's ids are used as they are)
       int rc = relabel_graph(E, J, N, W, big, &cnt->big_count, s);
@@ -1797,11 +1808,13 @@ int run_batch_union(Engine& E, std::vector<HostMember>& hm, const Opts& O, int* 
 }
 
 // workspace of the peel's row hash tables for W slots (run_union's pool, the
-// two queue descriptor arrays and the list of rows built a block each)
+// two queue descriptor arrays and the list of rows built a block each), and
+// of the relabelled copy of N vertices' rows (relabel_graph, bounded above)
 size_t table_bytes(uint64_t W) {
   return align_up(32ull * W) + 2 * align_up(8ull * std::max<uint64_t>(W / 2, 1)) +
          align_up(4ull * (W / (kTableSmem / 2) + 2));
 }
+size_t relabel_bytes(uint64_t N, uint64_t W) { return 8 * W + 30 * N + (64ull << 20); }
 #ifndef SPARX_BATCH_FOR_TABLES
 #define SPARX_BATCH_FOR_TABLES 1  // size batched unions so the row hash tables fit
 #endif
@@ -1864,7 +1877,9 @@ int run_batch(const sparx_graph_view* graphs, uint64_t count, uint64_t budget, c
       // slots, and within the budget with them): on the mix the tables take
       // more off the peel than the extra unions' waves cost.  A graph too large
       // for that still runs, alone, without them.
-      const bool fits_tables = fits && (!kBatchForTables || (W2 < (1ull << 30) && bytes + table_bytes(W2) <= budget));
+      const bool fits_tables =
+          fits && (!kBatchForTables ||
+                   (W2 < (1ull << 30) && bytes + table_bytes(W2) + relabel_bytes(N2, W2) <= budget));
       if (!fits_tables && !wave.empty()) break;
       if (!fits) {  // a single graph over the budget
         if (status_out) status_out[h.index] = SPARX_E_OOM;

@@ -155,3 +155,9 @@ def test_relabel_gives_the_same_truss_in_caller_order():
         assert np.array_equal(got, want)
         plain, st0 = P.run_pkt(g.offsets, g.neighbours, O32)
         assert st.triangles == st0.triangles and st.k_max == st0.k_max
+    # a batched union: every member is relabelled within its own id range
+    pairs = [(g.offsets, g.neighbours) for g in graphs]
+    want = [O.pkt(g.offsets, g.neighbours, threads=4) for g in graphs]
+    res = _with_tuning(P.PktTuning(relabel=1), lambda: P.run_batch(pairs, O32))
+    for w, (truss, st, status) in zip(want, res):
+        assert status == 0 and np.array_equal(truss, w)
