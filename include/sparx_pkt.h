@@ -253,8 +253,9 @@ typedef struct sparx_tuning {
                                plus 16 B per edge) is over a batch's budget or cannot be allocated */
   uint32_t sup_hash_min;    /* support: oriented out-lists of at least this length (>= 4) get a hash
                                table probed instead of the sampled search; 0 = none (0) */
-  uint32_t relabel;         /* single-graph calls, graphs without parallel edges: rebuild the CSR on vertex ids in
-                               (floor(log2 degree), id) order before the decomposition, for locality;
+  uint32_t relabel;         /* graphs and batched unions without parallel edges: rebuild the CSR on vertex ids
+                               in (floor(log2 degree), id) order (a union's members each within their own
+                               id range) before the decomposition, for locality;
                                results are returned in the caller's slot order (0; 1 for keys of
                                2^26 slots or more with a quarter of them in rows of degree >= 256) */
 } sparx_tuning;

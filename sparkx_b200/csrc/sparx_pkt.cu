@@ -74,7 +74,7 @@ struct Tuning {
   uint32_t compact_pct = 85;       // rebuild the peel's rows when live entries fill <= this % of them
   uint32_t hash_min_degree = 128;  // rows of at least this degree get a hash table for the per-lane search (0: none)
   uint32_t sup_hash_min = 0;       // support: out-lists of at least this length are probed in a hash table (0: none)
-  uint32_t relabel = 0;            // single graphs: rebuild the CSR on degree-ordered vertex ids first (0/1)
+  uint32_t relabel = 0;            // rebuild the CSR on degree-ordered vertex ids first (0/1)
 };
 
 // Degree-distribution signature: log2 of the slot count, log2 bucket of the
