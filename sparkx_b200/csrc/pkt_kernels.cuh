@@ -25,8 +25,13 @@
 //                               without processed edges whenever the live
 //                               edges fill at most 85% of it (two ping-pong
 //                               buffers)
-//   hub maps                    single-graph launches: neighbour id -> edge id
-//                               for the highest-degree vertices
+//   hub maps                    neighbour id -> edge id for the highest-degree
+//                               vertices (each spans its own member's ids)
+//   row hash tables (u64)       open-addressed (id | edge id << 32) entries,
+//                               2^(1+ceil(log2 d)) of them at 4 * off[v] for
+//                               rows of degree >= the tuning's floor
+//   vinfo[n] (u64)              per vertex: hub base (kVinfoHub set) or the
+//                               table's (log2 size << 32 | position), 0: none
 #pragma once
 
 #include <cstdint>
